@@ -1,0 +1,45 @@
+"""Small test-only models that exercise operators the benchmark workloads do not
+(cos, neg, sub of two nodes, reverse-sub, nn.Linear with bias, slices, scalar gathers,
+division by a constant, concatenation of several rows)."""
+import torch
+
+F64 = torch.float64
+
+
+class MixedOps(torch.nn.Module):
+    def __init__(self, seed=7):
+        super().__init__()
+        g = torch.Generator().manual_seed(seed)
+        self.lin = torch.nn.Linear(6, 4).to(F64)
+        with torch.no_grad():
+            self.lin.weight.copy_(torch.randn(4, 6, generator=g, dtype=F64))
+            self.lin.bias.copy_(torch.randn(4, generator=g, dtype=F64))
+        self.register_buffer("c", torch.randn(4, generator=g, dtype=F64))
+        self.box = (-1.5, 1.5)
+
+    def forward(self, x):
+        y = self.lin(x)
+        z = (y ** 2 + torch.cos(x[:, 1:5]) - 2.0 * y + torch.square(y) + y / 4.0
+             - (3.0 - y) + x[:, 2:3] + torch.exp(-0.5 * y) + self.c * torch.sin(y))
+        w = torch.log(2.5 + x[:, 0:4] * x[:, 2:6]) - x[:, 3:7 - 3] * y
+        return torch.cat([z.sum(1, keepdim=True), (x[:, 0] * 5.0).unsqueeze(1),
+                          w.sum(1, keepdim=True), (x[:, 4] - x[:, 5] * x[:, 1]).unsqueeze(1)], 1)
+
+
+class SinWide(torch.nn.Module):
+    """sin/cos on wide and shifted intervals (non-S-shaped branch, table lookups)."""
+
+    def __init__(self, seed=11):
+        super().__init__()
+        g = torch.Generator().manual_seed(seed)
+        self.register_buffer("w", torch.rand(5, generator=g, dtype=F64) * 6 + 0.5)
+        self.register_buffer("s", torch.randn(5, generator=g, dtype=F64) * 3)
+        self.box = (-3.0, 3.0)
+
+    def forward(self, x):
+        a = torch.sin(self.w * x + self.s)
+        b = torch.cos(self.w * x - self.s)
+        return torch.cat([(a + b).sum(1, keepdim=True), (a * b).sum(1, keepdim=True)], 1)
+
+
+MODELS = {"mixed_ops": (MixedOps, 6), "sin_wide": (SinWide, 5)}

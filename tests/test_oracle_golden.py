@@ -1,0 +1,63 @@
+"""The CPU oracle against fixtures recorded from the reference implementation.
+
+The fixtures hold the reference's compute_bounds(method='CROWN') outputs and the
+intermediate bounds it kept. With those intermediates injected (tie_tol=0, the
+reference's float comparison) the oracle must reproduce lb / lA / lbias; its own
+intermediates must match the recorded ones. With its default deterministic McCormick
+tie-break it must stay sound against sampling and match the reference wherever no tie
+decides a plane."""
+import numpy as np
+import pytest
+
+from golden_cases import cases, load
+from oracle.crown import CrownOracle
+
+
+@pytest.mark.parametrize("case", cases())
+def test_oracle_matches_reference_with_injected_intermediates(case):
+    m, g, d, inject = load(case)
+    o = CrownOracle(g, tie_tol=0.0, inject=inject)
+    lb, _, lA, lbias = o.compute_bounds(d["x_L"], d["x_U"], d["C"])
+    scale = np.maximum(1.0, np.abs(d["lb"]))
+    assert np.all(np.abs(lb - d["lb"]) / scale < 1e-9)
+    assert np.abs(lA - d["lA"]).max() <= 1e-9 * max(1.0, np.abs(d["lA"]).max())
+    assert np.all(np.abs(lbias - d["lbias"]) / np.maximum(1.0, np.abs(d["lbias"])) < 1e-9)
+
+
+@pytest.mark.parametrize("case", cases())
+def test_oracle_intermediates_match_reference(case):
+    m, g, d, inject = load(case)
+    o = CrownOracle(g, tie_tol=0.0, inject=inject)
+    o.compute_bounds(d["x_L"], d["x_U"], d["C"])
+    for v, (lo, hi) in inject.items():
+        if v in o.computed:
+            clo, chi = o.computed[v]
+            assert np.abs(clo - lo).max() <= 1e-12 * max(1.0, np.abs(lo).max())
+            assert np.abs(chi - hi).max() <= 1e-12 * max(1.0, np.abs(hi).max())
+
+
+@pytest.mark.parametrize("case", cases())
+def test_oracle_pass_order_matches_reference(case):
+    m, g, d, inject = load(case)
+    o = CrownOracle(g)
+    o.compute_bounds(d["x_L"], d["x_U"], d["C"])
+    mine = [g[v].width for kind, v in o.log if kind == "crown"]
+    ref = [int(p.split(":")[1]) for p in d["passes"]][:-1]
+    assert mine == ref
+
+
+@pytest.mark.parametrize("case", cases())
+def test_oracle_default_is_sound_by_sampling(case):
+    m, g, d, inject = load(case)
+    o = CrownOracle(g)
+    lb, _, lA, lbias = o.compute_bounds(d["x_L"], d["x_U"], d["C"])
+    rng = np.random.default_rng(0)
+    B, n = d["x_L"].shape
+    P = 2000 if n < 1000 else 200
+    for b in range(B):
+        pts = d["x_L"][b] + (d["x_U"][b] - d["x_L"][b]) * rng.random((P, n))
+        y = g.forward_numpy(pts) @ d["C"][b].T
+        assert np.all(lb[b] <= y.min(0) + 1e-9 * np.maximum(1, np.abs(y.min(0))))
+        # the returned plane is a valid lower bound too
+        plane = pts @ lA[b].T + lbias[b]
+        assert np.all(plane <= y + 1e-9 * np.maximum(1, np.abs(y)))
