@@ -1,0 +1,62 @@
+"""ctypes binding of libgear_b200.so (the C ABI declared in include/gear_b200.h)."""
+import ctypes
+import os
+
+from . import build as _build
+
+_LIB = None
+c_i32p = ctypes.POINTER(ctypes.c_int32)
+c_dblp = ctypes.POINTER(ctypes.c_double)
+
+
+class GearError(RuntimeError):
+    pass
+
+
+def lib():
+    """Load the in-tree extension; raise if it is missing (there is no CPU fallback)."""
+    global _LIB
+    if _LIB is None:
+        path = _build.LIB
+        if not os.path.exists(path):
+            raise GearError(f"libgear_b200.so not built ({path}); run gear_b200.build.build()")
+        L = ctypes.CDLL(path)
+        L.gear_dag_create.argtypes = [c_i32p, ctypes.c_int64, c_i32p, ctypes.c_int64, c_i32p, ctypes.c_int64,
+                                      c_i32p, ctypes.c_int64, c_i32p, ctypes.c_int64, c_i32p, ctypes.c_int64,
+                                      c_dblp, ctypes.c_int64, ctypes.POINTER(ctypes.c_void_p)]
+        L.gear_dag_create.restype = ctypes.c_int
+        L.gear_dag_destroy.argtypes = [ctypes.c_void_p]
+        L.gear_dag_destroy.restype = ctypes.c_int
+        L.gear_crown_workspace_bytes.argtypes = [ctypes.c_void_p, ctypes.c_int64]
+        L.gear_crown_workspace_bytes.restype = ctypes.c_int64
+        L.gear_crown_lower.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
+        L.gear_crown_lower.restype = ctypes.c_int
+        L.gear_last_error.argtypes = []
+        L.gear_last_error.restype = ctypes.c_char_p
+        L.gear_last_launch_count.argtypes = []
+        L.gear_last_launch_count.restype = ctypes.c_int
+        _LIB = L
+    return _LIB
+
+
+def check(status, what):
+    if status != 0:
+        msg = lib().gear_last_error().decode(errors="replace")
+        if status == -2:
+            import torch
+            raise torch.OutOfMemoryError(f"{what}: {msg}")
+        raise GearError(f"{what} failed ({status}): {msg}")
+
+
+def ptr_i32(a):
+    return a.ctypes.data_as(c_i32p)
+
+
+def ptr_dbl(a):
+    return a.ctypes.data_as(c_dblp)
+
+
+EXPORTED = ("gear_dag_create", "gear_dag_destroy", "gear_crown_workspace_bytes", "gear_crown_lower",
+            "gear_last_launch_count", "gear_last_error")

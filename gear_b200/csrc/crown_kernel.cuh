@@ -1,0 +1,1003 @@
+// CROWN bound propagation over a batch of boxes: one persistent megakernel.
+// (Included by gear_capi.cu, the single translation unit of libgear_b200.so.)
+//
+// Each CTA takes boxes b = blockIdx.x, blockIdx.x + gridDim.x, ... and runs the whole
+// compiled schedule for that box: plain IBP of every node, relaxation planes, every
+// intermediate CROWN pass (lower and upper, C = I over the node width, then
+// compare-with-IBP), the final pass and its box concretisation. The A coefficients of a
+// pass live in shared memory as the statically-sparse entry lists the host compiler built
+// (gear_b200/program.py); intervals, planes and fold vectors live in a per-CTA scratch slot
+// in global memory (reused box after box, so it stays in L2).
+//
+// Reference semantics followed (paths relative to solver/auto_LiRPA):
+//   relaxations  operators/bivariate.py:38-247 (McCormick, coefficient-aware pick),
+//                operators/activations.py:186-210 (Sqr), operators/convex_concave.py:64-92
+//                (Log), :569-626 (Exp), operators/s_shaped.py:325-550 and
+//                operators/trigonometric.py:27-527 (Sin/Cos);
+//   backward     backward_bound.py:880-1206, operators/clampmult.py:31-77;
+//   IBP          interval_bound.py:156-254 and the operators' interval_propagate;
+//   concretise   concretize_bounds.py:160-321, concretize_func.py:553-569,
+//                fp_enclosure.py:34-98.
+// Compiled with -fmad=false: the elementwise formulas round like the reference's eager
+// float64 arithmetic (no contraction), which keeps the relaxation choices stable.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "gear_program.h"
+
+namespace gear {
+
+constexpr double PI = 3.141592653589793;
+constexpr double TWO_PI = 2 * PI;
+constexpr double HALF_PI = PI / 2;
+constexpr double THREE_HALF_PI = 3 * PI / 2;
+constexpr double EPS = 2.220446049250313e-16;   // float64 machine epsilon
+constexpr double UNIT = EPS / 2;
+constexpr double EPSILON = 1e-12;               // operators/base.py:32
+constexpr double TIE_TOL = 1e-12;               // McCormick tie tolerance (see program.py)
+constexpr double STEP_PRE = 0.01;
+constexpr int NT = 256;                         // threads per CTA
+constexpr int NWARP = NT / 32;
+
+// sin/cos table offsets (gear_b200/tables.py SIN_TABLE_ORDER)
+constexpr int T_DL = 0, T_DU = SIN_N_PRE, T_XLLD = 2 * SIN_N_PRE, T_XLLC = T_XLLD + SIN_N_TB,
+              T_XLUD = T_XLLC + SIN_N_TB, T_XLUC = T_XLUD + SIN_N_TB, T_XULD = T_XLUC + SIN_N_TB,
+              T_XULC = T_XULD + SIN_N_TB, T_XUUD = T_XULC + SIN_N_TB, T_XUUC = T_XUUD + SIN_N_TB;
+
+struct Work {
+  const double* xL;
+  const double* xU;
+  const double* C;       // (B, S, w_t) or null (identity)
+  double* lb;            // (B, S)
+  double* lA;            // (B, S, n) or null
+  double* lbias;         // (B, S) or null
+  double* scratch;       // per-slot scratch
+  int64_t slot_doubles;
+  int64_t B;
+  int* status;
+};
+
+// ------------------------------------------------------------------ small helpers
+__device__ __forceinline__ double rounding_error(double mag, double n) {
+  return mag * ((n + 16.0) * EPS * 4.0);
+}
+__device__ __forceinline__ double widen(double bound, double err, double sign) {
+  double out = isfinite(bound) ? bound + sign * err : bound;
+  return (isinf(err) && err > 0) ? sign * INFINITY : out;
+}
+__device__ __forceinline__ double finite_abs(double v) { return isfinite(v) ? fabs(v) : 0.0; }
+__device__ __forceinline__ double gamma_k(double k) { return (k + 1.0) * UNIT * (1.0 + 1e-6); }
+// NaN-propagating min / max (torch.minimum / np.minimum semantics)
+__device__ __forceinline__ double pmax(double a, double b) { return (isnan(a) || a > b) ? a : (isnan(b) ? b : (a > b ? a : b)); }
+__device__ __forceinline__ double pmin(double a, double b) { return (isnan(a) || a < b) ? a : (isnan(b) ? b : (a < b ? a : b)); }
+__device__ __forceinline__ double nan_lo(double v) { return isnan(v) ? -INFINITY : v; }
+__device__ __forceinline__ double nan_hi(double v) { return isnan(v) ? INFINITY : v; }
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ int warp_or(int v) { return __any_sync(0xffffffffu, v); }
+
+// ------------------------------------------------------------------ relaxations
+__device__ void relax_sqr(double l, double u, double* p) {
+  double uk = l + u;
+  double ub = -l * uk + l * l;
+  double mid = fmax(l, 0.0) - fmax(-u, 0.0);
+  double lk = 2 * mid;
+  double lb = -mid * lk + mid * mid;
+  p[0] = lk; p[1] = lb; p[2] = uk; p[3] = ub;
+}
+
+__device__ void relax_exp(double l, double u, double* p) {
+  double du = u - l;
+  double neg_expm1 = -expm1(l - u);
+  double m_par = u + log(fmax(neg_expm1, EPSILON)) - log(fmax(du, EPSILON));
+  double m_mid = (l + u) / 2;
+  double m = du > 1e-6 ? m_par : m_mid;
+  m = fmin(fmax(m, l), u);
+  double exp_l = exp(l), exp_m = exp(m), exp_u = exp(u);
+  double lower_k = isfinite(exp_m) ? exp_m : 0.0;
+  double lower_x0 = isfinite(m) ? m : 0.0;
+  double lower_b = -lower_x0 * lower_k + lower_k;
+  bool lsafe = isfinite(lower_k) && isfinite(lower_b);
+  p[0] = lsafe ? lower_k : 0.0;
+  p[1] = lsafe ? lower_b : 0.0;
+  double d = u - l;
+  double k;
+  if (d < 1) k = exp_l * (d > 0 ? expm1(fmin(d, 1.0)) / fmax(d, 1e-300) : 1.0);
+  else k = (exp_u - exp_l) / fmax(d, 1.0);
+  double upper_b = -l * k + exp_l;
+  bool usafe = isfinite(k) && isfinite(upper_b);
+  p[2] = usafe ? k : 0.0;
+  p[3] = usafe ? upper_b : INFINITY;
+}
+
+__device__ void relax_log(double l, double u, double* p) {
+  double rl = log(l), ru = log(u);
+  double du = u - l;
+  double ku = (ru - rl) / fmax(du, EPSILON);
+  p[0] = ku;
+  p[1] = -l * ku + rl;
+  double dlog = fmax(ru - rl, EPSILON);
+  double m_par = du / dlog;
+  double m_mid = (l + u) / 2;
+  double m = du > 1e-6 ? m_par : m_mid;
+  m = fmin(fmax(m, l), u);
+  double k = 1.0 / m;
+  p[2] = k;
+  p[3] = -m * k + log(m);
+}
+
+struct SinT {
+  const double* T;
+};
+
+__device__ __forceinline__ long trunc_l(double v) { return (long)v; }
+
+__device__ void sin_gen_d(const double* T, double lower, double upper, double* dl, double* du) {
+  const double sp = STEP_PRE;
+  double k = floor(upper / TWO_PI);
+  double uc = upper - k * TWO_PI;
+  double c1 = (uc >= 0 && uc <= HALF_PI) ? 1.0 : 0.0;
+  double ucn = fmin(fmax(uc, 0.0), HALF_PI);
+  long idx = max(0L, trunc_l(ucn / sp)) + 1;
+  double d_lower = (T[T_DL + idx] + k * 2 * PI) * c1;
+  double c2 = (uc >= PI && uc <= THREE_HALF_PI) ? 1.0 : 0.0;
+  ucn = fmin(fmax(uc, PI), THREE_HALF_PI);
+  idx = max(0L, trunc_l((PI - ucn) / -sp)) + 1;
+  double d_upper = (PI - T[T_DU + idx] + k * 2 * PI) * c2;
+  k = floor(lower / TWO_PI);
+  double lc = lower - k * TWO_PI;
+  double c3 = (lc >= THREE_HALF_PI && lc <= 2 * PI) ? 1.0 : 0.0;
+  double lcn = fmin(fmax(lc, THREE_HALF_PI), 2 * PI);
+  idx = max(0L, trunc_l((lcn - 2 * PI) / -sp)) + 1;
+  d_upper = d_upper + (T[T_DU + idx] + (k + 1) * 2 * PI) * c3;
+  double c4 = (lc >= HALF_PI && lc <= PI) ? 1.0 : 0.0;
+  lcn = fmin(fmax(lc, HALF_PI), 3 * PI);
+  idx = max(0L, trunc_l((PI - lcn) / sp)) + 1;
+  d_lower = d_lower + (PI - T[T_DL + idx] + k * 2 * PI) * c4;
+  *dl = d_lower;
+  *du = d_upper;
+}
+
+__device__ double sin_pick(double mid, double lower, double upper, double lb_cyc, double ub_cyc,
+                           double tl, double tr, double cl, double cr, double base) {
+  double unf_l = tl + cl + lb_cyc;
+  double l_ends = base + cl + lb_cyc;
+  double unf_r = tr + cr + ub_cyc;
+  double r_ends = base + cr + ub_cyc;
+  bool leftmost = (mid < unf_l) && (unf_l <= upper);
+  bool left_range = (mid >= unf_l) && (mid < l_ends);
+  bool inbetween = (mid >= l_ends) && (mid < r_ends);
+  bool rightmost = (mid >= unf_r) && (unf_r >= lower);
+  bool right_range = (!left_range) && ((mid >= r_ends) && (mid < unf_r));
+  double tp = (leftmost ? 1.0 : 0.0) * tl + (left_range ? 1.0 : 0.0) * (mid - cl - lb_cyc) +
+              (inbetween ? 1.0 : 0.0) * base + (rightmost ? 1.0 : 0.0) * tr +
+              (right_range ? 1.0 : 0.0) * (mid - cr - ub_cyc);
+  bool any = leftmost || left_range || inbetween || rightmost || right_range;
+  return any ? tp : tl;
+}
+
+__device__ void sin_bound_tb(const double* T, double lb, double ub, double* out) {
+  double lower = lb, upper = ub;
+  const double step = 2 * PI / (SIN_N_TB - 1);
+  double lb_cyc = floor(lb / (2 * PI)) * (2 * PI);
+  double lbm = fmin(fmax(lb - lb_cyc, 0.0), 2 * PI);
+  double ub_cyc = floor(ub / (2 * PI)) * (2 * PI);
+  double ubm = fmin(fmax(ub - ub_cyc, 0.0), 2 * PI);
+  long il = trunc_l(lbm / step);
+  long iu = min(trunc_l(ceil(ubm / step)), (long)(SIN_N_TB - 1));
+  double tll = T[T_XLLD + il], tlu = T[T_XLUD + il], trl = T[T_XULD + iu], tru = T[T_XUUD + iu];
+  double cll = T[T_XLLC + il], clu = T[T_XLUC + il], crl = T[T_XULC + iu], cru = T[T_XUUC + iu];
+  double mid = (lower + upper) / 2;
+  double tp_l = sin_pick(mid, lower, upper, lb_cyc, ub_cyc, tll, trl, cll, crl, 1.5 * PI);
+  double tp_u = sin_pick(mid, lower, upper, lb_cyc, ub_cyc, tlu, tru, clu, cru, 2.5 * PI);
+  double d_l = cos(tp_l);
+  double b_l = sin(tp_l) - d_l * (tp_l + (tp_l <= 1.5 * PI ? cll + lb_cyc : crl + ub_cyc));
+  double d_u = cos(tp_u);
+  double b_u = sin(tp_u) - d_u * (tp_u + (tp_u <= 2.5 * PI ? clu + lb_cyc : cru + ub_cyc));
+  out[0] = d_l; out[1] = b_l; out[2] = d_u; out[3] = b_u;
+}
+
+__device__ __forceinline__ double sin_n_crossing(double start, double end, double s) {
+  double cycles = floor((end - start) / (2 * PI));
+  double dist = floor((s - start) / (2 * PI));
+  double real_s = s - dist * 2 * PI;
+  double real_end = end - cycles * 2 * PI;
+  return (real_s >= start ? 1.0 : 0.0) * (real_s <= real_end ? 1.0 : 0.0) + cycles;
+}
+
+__device__ void sin_branch(const double* T, double lb, double ub, double* out) {
+  ub = fmax(ub, lb + 1e-8);
+  double sub = sin(ub), slb = sin(lb);
+  double mid = (sub + slb) / 2.;
+  double smid = sin((ub + lb) / 2);
+  double gap = smid - mid;
+  double slope = (sub - slb) / fmax(ub - lb, 1e-10);
+  double bias = slb - slope * lb;
+  double c = slope;
+  double cr1 = (c == -1 ? -PI / 2 : (c == 1 ? PI / 2 : asin(c))) - 0.5 * PI;
+  double cr2 = PI - cr1 - 2 * (0.5 * PI);
+  double crossings = sin_n_crossing(lb, ub, cr1) + sin_n_crossing(lb, ub, cr2);
+  bool use_line = crossings == 1;
+  double ul = (gap < 0 && use_line) ? 1.0 : 0.0;
+  double ll = (gap >= 0 && use_line) ? 1.0 : 0.0;
+  double tb[4];
+  sin_bound_tb(T, lb, ub, tb);
+  out[0] = ll * slope + (1 - ll) * tb[0];
+  out[1] = ll * bias + (1 - ll) * tb[1];
+  out[2] = ul * slope + (1 - ul) * tb[2];
+  out[3] = ul * bias + (1 - ul) * tb[3];
+}
+
+__device__ void relax_sin(const double* T, double l, double u, double* p) {
+  double twopi = 2 * PI;
+  double lbc = l - floor(l / twopi) * twopi;
+  double ubc = u - floor(u / twopi) * twopi;
+  bool ml1 = lbc >= 0 && lbc < PI / 2, ml2 = lbc >= PI / 2 && lbc < PI, ml3 = lbc >= PI && lbc < 3 * PI / 2,
+       ml4 = lbc >= 3 * PI / 2 && lbc < 2 * PI;
+  bool mu1 = ubc >= 0 && ubc < PI / 2, mu2 = ubc >= PI / 2 && ubc < PI, mu3 = ubc >= PI && ubc < 3 * PI / 2,
+       mu4 = ubc >= 3 * PI / 2 && ubc < 2 * PI;
+  bool sig = (u - l <= PI) && (((ml2 || ml3) && (mu2 || mu3)) || ((ml1 || ml4) && (mu1 || mu4)));
+  bool mneg = (ml3 || ml4) && ((mu3 || mu4) && sig);
+  bool mpos = (ml1 || ml2) && ((mu1 || mu2) && sig);
+  bool mboth = sig != (mneg || mpos);
+  bool cc = (-sin(l)) >= 0;
+  double lw = 0, lb = 0, uw = 0, ub = 0;
+#define ADD_LOWER(mask, k, x0, y0) if (mask) { lw = (k); lb = -(x0) * (k) + (y0); }
+#define ADD_UPPER(mask, k, x0, y0) if (mask) { uw = (k); ub = -(x0) * (k) + (y0); }
+  double y_l = sin(l), y_u = sin(u);
+  double width = u - l;
+  double k_direct = (y_u - y_l) / fmax(width, 1e-8);
+  if (width < 1e-8) k_direct = cos(l);
+  ADD_UPPER(mneg, k_direct, l, y_l);
+  ADD_LOWER(mpos, k_direct, l, y_l);
+  double d_lower, d_upper;
+  sin_gen_d(T, l, u, &d_lower, &d_upper);
+  bool mdl = (cc ? (k_direct < cos(l)) : (k_direct > cos(u))) && mboth;
+  bool mdu = (cc ? (k_direct < cos(u)) : (k_direct > cos(l))) && mboth;
+  double m = (l + u) / 2;
+  double y_m = sin(m), k_m = cos(m);
+  ADD_LOWER(mneg, k_m, m, y_m);
+  ADD_UPPER(mpos, k_m, m, y_m);
+  ADD_LOWER(mdl, k_direct, l, y_l);
+  ADD_LOWER(mboth != mdl, cos(d_lower), d_lower, sin(d_lower));
+  ADD_UPPER(mdu, k_direct, l, y_l);
+  ADD_UPPER(mboth != mdu, cos(d_upper), d_upper, sin(d_upper));
+  ADD_LOWER(sig && (y_l < y_u) && (d_lower >= m), k_m, m, y_m);
+  ADD_UPPER(sig && (y_l < y_u) && (d_upper < m), k_m, m, y_m);
+  ADD_LOWER(sig && (y_l >= y_u) && (d_lower < m), k_m, m, y_m);
+  ADD_UPPER(sig && (y_l >= y_u) && (d_upper >= m), k_m, m, y_m);
+#undef ADD_LOWER
+#undef ADD_UPPER
+  if (!sig) {
+    double br[4];
+    sin_branch(T, l, u, br);
+    lw = br[0]; lb = br[1]; uw = br[2]; ub = br[3];
+  }
+  double ro = 8 * EPS * (1 + fmax(fabs(l), fabs(u)));
+  p[0] = lw; p[1] = lb - ro; p[2] = uw; p[3] = ub + ro;
+}
+
+__device__ void relax_cos(const double* T, double l, double u, double* p) {
+  const double hp = 0.5 * PI;
+  relax_sin(T, l + hp, u + hp, p);
+  p[1] = p[1] + p[0] * hp;
+  p[3] = p[3] + p[2] * hp;
+}
+
+__device__ void relax_mul(double xl, double xu, double yl, double yu, double* p) {
+  auto amin = [&](double a, double b, double c) {
+    return a * (a >= 0 ? xl : xu) + b * (b >= 0 ? yl : yu) + c;
+  };
+  auto amax = [&](double a, double b, double c) {
+    return a * (a >= 0 ? xu : xl) + b * (b >= 0 ? yu : yl) + c;
+  };
+  double m1 = amin(yl, xl, -xl * yl), m2 = amin(yu, xu, -xu * yu);
+  double M1 = amax(yu, xl, -yu * xl), M2 = amax(yl, xu, -yl * xu);
+  double r_l = (m1 >= m2 - TIE_TOL * (fabs(m1) + fabs(m2))) ? 1.0 : 0.0;
+  double r_u = (M1 <= M2 + TIE_TOL * (fabs(M1) + fabs(M2))) ? 1.0 : 0.0;
+  p[0] = (yl - yu) * r_l + yu;
+  p[1] = (xl - xu) * r_l + xu;
+  p[2] = (yu * xu - yl * xl) * r_l - yu * xu;
+  p[3] = (yu - yl) * r_u + yl;
+  p[4] = (xl - xu) * r_u + xu;
+  p[5] = (yl * xu - yu * xl) * r_u - yl * xu;
+}
+
+// ------------------------------------------------------------------ per-box context
+struct Box {
+  const DevProgram* P;
+  double* lo;      // interval arena (arena_w)
+  double* hi;
+  double* mag;     // magnitude arena
+  double* planes;  // plane arena
+  double* fold;    // fold vectors
+  double* pres_lo; // pass results (maxw)
+  double* pres_hi;
+  const double* xL;  // this box's input box (n)
+  const double* xU;
+  int64_t b;
+};
+
+__device__ __forceinline__ const int32_t* node_rec(const DevProgram* P, int v) { return P->nodes + v * NODE_REC; }
+
+// interval sums over the inputs of a reducesum output j (increasing input order)
+__device__ void ibp_element(const Box& bx, const int32_t* nd, int j, double* olo, double* ohi) {
+  const DevProgram* P = bx.P;
+  const int kind = nd[N_KIND];
+  const double* lo = bx.lo;
+  const double* hi = bx.hi;
+  double l = 0, h = 0;
+  switch (kind) {
+    case NK_MUL: {
+      const int32_t* a = node_rec(P, nd[N_IN0]);
+      const int32_t* c = node_rec(P, nd[N_IN1]);
+      int i0 = P->ip[nd[N_MAP0] + j], i1 = P->ip[nd[N_MAP1] + j];
+      double xl = lo[a[N_CUR] + i0], xu = hi[a[N_CUR] + i0];
+      double yl = lo[c[N_CUR] + i1], yu = hi[c[N_CUR] + i1];
+      double r0 = xl * yl, r1 = xl * yu, r2 = xu * yl, r3 = xu * yu;
+      bool nan = isnan(r0) || isnan(r1) || isnan(r2) || isnan(r3);
+      l = nan ? -INFINITY : fmin(fmin(r0, r1), fmin(r2, r3));
+      h = nan ? INFINITY : fmax(fmax(r0, r1), fmax(r2, r3));
+      break;
+    }
+    case NK_MULC: {
+      const int32_t* a = node_rec(P, nd[N_IN0]);
+      int i0 = P->ip[nd[N_MAP0] + j];
+      double xl = lo[a[N_CUR] + i0], xu = hi[a[N_CUR] + i0];
+      double c = P->dp[nd[N_CVEC] + j];
+      l = c > 0 ? xl * c : (c < 0 ? xu * c : 0.0);
+      h = c > 0 ? xu * c : (c < 0 ? xl * c : 0.0);
+      break;
+    }
+    case NK_ADD: case NK_SUB: case NK_ADDC: case NK_SUBC: case NK_RSUBC: {
+      const int32_t* a = node_rec(P, nd[N_IN0]);
+      int i0 = P->ip[nd[N_MAP0] + j];
+      double xl = lo[a[N_CUR] + i0], xu = hi[a[N_CUR] + i0];
+      double yl, yu;
+      if (kind == NK_ADD || kind == NK_SUB) {
+        const int32_t* c = node_rec(P, nd[N_IN1]);
+        int i1 = P->ip[nd[N_MAP1] + j];
+        yl = lo[c[N_CUR] + i1]; yu = hi[c[N_CUR] + i1];
+      } else {
+        yl = yu = P->dp[nd[N_CVEC] + j];
+        if (kind == NK_RSUBC) { double tl = xl, tu = xu; xl = yl; xu = yu; yl = tl; yu = tu; }
+      }
+      if (kind == NK_ADD || kind == NK_ADDC) { l = xl + yl; h = xu + yu; }
+      else { l = xl - yu; h = xu - yl; }
+      l = widen(l, rounding_error(finite_abs(l), 1), -1);
+      h = widen(h, rounding_error(finite_abs(h), 1), 1);
+      break;
+    }
+    case NK_NEG: {
+      const int32_t* a = node_rec(P, nd[N_IN0]);
+      l = -hi[a[N_CUR] + j]; h = -lo[a[N_CUR] + j];
+      break;
+    }
+    case NK_SQR: case NK_EXP: case NK_LOG: case NK_SIN: case NK_COS: {
+      const int32_t* a = node_rec(P, nd[N_IN0]);
+      double xl = lo[a[N_CUR] + j], xu = hi[a[N_CUR] + j];
+      if (kind == NK_SQR) {
+        l = xu < 0 ? xu * xu : (xl > 0 ? xl * xl : 0.0);
+        h = pmax(xl * xl, xu * xu);
+      } else if (kind == NK_EXP) {
+        l = exp(xl); h = exp(xu);
+      } else if (kind == NK_LOG) {
+        if (xl <= 0) xl = 0.0;
+        l = log(xl); h = log(xu);
+      } else {
+        double maxp = kind == NK_SIN ? PI / 2 : 0.0;
+        double minp = kind == NK_SIN ? PI * 3 / 2 : PI;
+        double fl = kind == NK_SIN ? sin(xl) : cos(xl);
+        double fu = kind == NK_SIN ? sin(xu) : cos(xu);
+        auto crossing = [&](double ll, double uu, double point) {
+          double lc = (ll - point) / (2 * PI);
+          double uc = (uu - point) / (2 * PI);
+          double ro = 2 * EPS * (1 + fmax(fabs(lc), fabs(uc)));
+          return (uu - ll >= 2 * PI) || (floor(uc + ro) > floor(lc - ro));
+        };
+        h = crossing(xl, xu, maxp) ? 1.0 : pmax(fl, fu);
+        l = crossing(xl, xu, minp) ? -1.0 : pmin(fl, fu);
+      }
+      break;
+    }
+    case NK_REDUCESUM: {
+      const int32_t* a = node_rec(P, nd[N_IN0]);
+      const int32_t* inv = P->ip + nd[N_MAP1];
+      int w = nd[N_W];
+      int s0 = inv[j], s1 = inv[j + 1];
+      for (int k = s0; k < s1; ++k) {
+        int i = inv[w + 1 + k];
+        l += lo[a[N_CUR] + i];
+        h += hi[a[N_CUR] + i];
+      }
+      break;
+    }
+    case NK_MAP: {
+      const int32_t* a = node_rec(P, nd[N_IN0]);
+      int i = P->ip[nd[N_MAP0] + j];
+      l = lo[a[N_CUR] + i]; h = hi[a[N_CUR] + i];
+      break;
+    }
+    case NK_CONCAT: {
+      int pos = P->ip[nd[N_MAP0] + j];
+      const int32_t* ins = P->ip + nd[N_INS];
+      for (int k = 0; k < nd[N_NIN]; ++k) {
+        const int32_t* a = node_rec(P, ins[k]);
+        if (pos < a[N_W]) { l = lo[a[N_CUR] + pos]; h = hi[a[N_CUR] + pos]; break; }
+        pos -= a[N_W];
+      }
+      break;
+    }
+    default:
+      break;
+  }
+  *olo = nan_lo(l);
+  *ohi = nan_hi(h);
+}
+
+// Linear / MatMul interval (interval_bound + BoundLinear._bound_box): warp per output row.
+__device__ void ibp_linear(const Box& bx, const int32_t* nd, double* olo, double* ohi) {
+  const DevProgram* P = bx.P;
+  int w = nd[N_W], win = nd[N_WIN];
+  const double* W = P->dp + nd[N_W_OFF];
+  const double* bias = nd[N_B_OFF] >= 0 ? P->dp + nd[N_B_OFF] : nullptr;
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (nd[N_FOLD] >= 0) {
+    const double* f = bx.fold + nd[N_FOLD];
+    for (int j = threadIdx.x; j < w; j += NT) {
+      double bb = bias ? bias[j] : 0.0;
+      double l = f[j] - f[w + j], h = f[j] + f[w + j];
+      l = l + bb; h = h + bb;
+      double err = rounding_error(f[2 * w + j] + fabs(bb), win);
+      olo[j] = nan_lo(widen(l, err, -1));
+      ohi[j] = nan_hi(widen(h, err, 1));
+    }
+    return;
+  }
+  const int32_t* a = node_rec(P, nd[N_IN0]);
+  const double* ilo = bx.lo + a[N_CUR];
+  const double* ihi = bx.hi + a[N_CUR];
+  for (int j = warp; j < w; j += NWARP) {
+    const double* Wr = W + (int64_t)j * win;
+    double center = 0, dev = 0, mag = 0, slo = 0, shi = 0;
+    int nonfin = 0;
+    for (int i = lane; i < win; i += 32) {
+      double wv = Wr[i];
+      double l = ilo[i], h = ihi[i];
+      nonfin |= !(isfinite(l) && isfinite(h));
+      center += ((l + h) / 2) * wv;
+      dev += ((h - l) / 2) * fabs(wv);
+      mag += finite_abs(fmax(fabs(l), fabs(h))) * fabs(wv);
+      double pl = wv > 0 ? wv * l : (wv < 0 ? wv * h : 0.0);
+      double ph = wv > 0 ? wv * h : (wv < 0 ? wv * l : 0.0);
+      slo += isnan(pl) ? -INFINITY : pl;
+      shi += isnan(ph) ? INFINITY : ph;
+    }
+    center = warp_sum(center); dev = warp_sum(dev); mag = warp_sum(mag);
+    slo = warp_sum(slo); shi = warp_sum(shi);
+    nonfin = warp_or(nonfin);
+    if (lane == 0) {
+      double l = nonfin ? slo : center - dev;
+      double h = nonfin ? shi : center + dev;
+      double bb = bias ? bias[j] : 0.0;
+      l = l + bb; h = h + bb;
+      double err = rounding_error(mag + fabs(bb), win);
+      olo[j] = nan_lo(widen(l, err, -1));
+      ohi[j] = nan_hi(widen(h, err, 1));
+    }
+  }
+}
+
+__device__ void ibp_node(const Box& bx, int v, double* olo, double* ohi) {
+  const int32_t* nd = node_rec(bx.P, v);
+  int kind = nd[N_KIND];
+  if (kind == NK_LINEAR || kind == NK_MATMUL) {
+    ibp_linear(bx, nd, olo, ohi);
+    return;
+  }
+  int w = nd[N_W];
+  for (int j = threadIdx.x; j < w; j += NT) ibp_element(bx, nd, j, olo + j, ohi + j);
+}
+
+// fold vectors of a linear/matmul on the input: W x0, |W| eps, |W| max(|xL|, |xU|)
+__device__ void fold_node(const Box& bx, int v) {
+  const DevProgram* P = bx.P;
+  const int32_t* nd = node_rec(P, v);
+  int w = nd[N_W], win = nd[N_WIN];
+  const double* W = P->dp + nd[N_W_OFF];
+  double* f = bx.fold + nd[N_FOLD];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int j = warp; j < w; j += NWARP) {
+    const double* Wr = W + (int64_t)j * win;
+    double c = 0, r = 0, t = 0;
+    for (int i = lane; i < win; i += 32) {
+      double wv = Wr[i];
+      double l = bx.xL[i], h = bx.xU[i];
+      c += ((h + l) / 2.0) * wv;
+      r += ((h - l) / 2.0) * fabs(wv);
+      t += finite_abs(fmax(fabs(l), fabs(h))) * fabs(wv);
+    }
+    c = warp_sum(c); r = warp_sum(r); t = warp_sum(t);
+    if (lane == 0) { f[j] = c; f[w + j] = r; f[2 * w + j] = t; }
+  }
+}
+
+__device__ void relax_node(const Box& bx, int v) {
+  const DevProgram* P = bx.P;
+  const int32_t* nd = node_rec(P, v);
+  int kind = nd[N_KIND], w = nd[N_W];
+  double* pl = bx.planes + nd[N_PLANE];
+  const double* T = P->dp + P->hdr[H_SINOFF];
+  for (int j = threadIdx.x; j < w; j += NT) {
+    if (kind == NK_MUL) {
+      const int32_t* a = node_rec(P, nd[N_IN0]);
+      const int32_t* c = node_rec(P, nd[N_IN1]);
+      int i0 = P->ip[nd[N_MAP0] + j], i1 = P->ip[nd[N_MAP1] + j];
+      double xl = bx.lo[a[N_CUR] + i0], xu = bx.hi[a[N_CUR] + i0];
+      double yl = bx.lo[c[N_CUR] + i1], yu = bx.hi[c[N_CUR] + i1];
+      double* p = pl + 6 * j;
+      if (!(isfinite(xl) && isfinite(xu) && isfinite(yl) && isfinite(yu))) {
+        for (int k = 0; k < 6; ++k) p[k] = NAN;
+      } else {
+        relax_mul(xl, xu, yl, yu, p);
+      }
+    } else {
+      const int32_t* a = node_rec(P, nd[N_IN0]);
+      double l = bx.lo[a[N_CUR] + j], u = bx.hi[a[N_CUR] + j];
+      double* p = pl + 4 * j;
+      bool bad = !(isfinite(l) && isfinite(u));
+      if (kind == NK_LOG) bad = bad || !(l > 0);
+      if (bad) {
+        p[0] = p[1] = p[2] = p[3] = NAN;
+      } else if (kind == NK_SQR) relax_sqr(l, u, p);
+      else if (kind == NK_EXP) relax_exp(l, u, p);
+      else if (kind == NK_LOG) relax_log(l, u, p);
+      else if (kind == NK_SIN) relax_sin(T, l, u, p);
+      else if (kind == NK_COS) relax_cos(T, l, u, p);
+    }
+  }
+}
+
+// ------------------------------------------------------------------ CROWN pass
+// Row arrays in shared memory, per side: bias, bias magnitude, charge, base, dev, berr, undef.
+enum { R_BIAS = 0, R_BMAG, R_CHG, R_BASE, R_DEV, R_BERR, R_UNDEF, R_COUNT };
+
+struct PassCtx {
+  const int32_t* pr;
+  int S, sides;
+  double* rows;      // [side][R_COUNT][S]
+  double* buf;       // [side][smem]
+  int smem;
+  __device__ double* row(int side, int what) const { return rows + ((size_t)side * R_COUNT + what) * S; }
+  __device__ double* vals(int side, int off) const { return buf + (size_t)side * smem + off; }
+};
+
+// transformed coefficient for input `slot` of an elementwise op, and its bias term
+__device__ __forceinline__ double elem_coef(int kind, int slot, int side, double a, const double* pl,
+                                            double cval, double* bterm) {
+  *bterm = 0.0;
+  switch (kind) {
+    case NK_SQR: case NK_EXP: case NK_LOG: case NK_SIN: case NK_COS: {
+      // lower side: positive -> (lw, lb), negative -> (uw, ub); upper side: reversed
+      double wp = side == 0 ? pl[0] : pl[2], bp = side == 0 ? pl[1] : pl[3];
+      double wn = side == 0 ? pl[2] : pl[0], bn = side == 0 ? pl[3] : pl[1];
+      if (a > 0) { *bterm = a * bp; return wp * a; }
+      if (a < 0) { *bterm = a * bn; return wn * a; }
+      return 0.0;
+    }
+    case NK_MUL: {
+      // planes: al, bl, gl, au, bu, gu (alpha multiplies x, beta y)
+      const double* P_ = side == 0 ? pl : pl + 3;   // positive coefficients
+      const double* N_ = side == 0 ? pl + 3 : pl;   // negative coefficients
+      if (a > 0) { *bterm = a * P_[2]; return P_[slot] * a; }
+      if (a < 0) { *bterm = a * N_[2]; return N_[slot] * a; }
+      return 0.0;
+    }
+    case NK_MULC: return a * cval;
+    case NK_SUB: return slot == 0 ? a : -a;
+    case NK_RSUBC: return -a;
+    case NK_NEG: return -a;
+    default: return a;   // add, addc, subc, reducesum, map, concat
+  }
+}
+
+__device__ void run_pass(const Box& bx, int pid, double* sm, const Work& wk) {
+  const DevProgram* P = bx.P;
+  const int32_t* pr = P->passes + pid * PASS_REC;
+  PassCtx ctx;
+  ctx.pr = pr;
+  ctx.S = pr[P_S];
+  ctx.sides = pr[P_SIDES];
+  ctx.smem = pr[P_SMEM];
+  ctx.rows = sm;
+  ctx.buf = sm + (size_t)ctx.sides * R_COUNT * ctx.S;
+  const int S = ctx.S, sides = ctx.sides;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const bool onehot = pr[P_ONEHOT] != 0;
+  const int n = P->hdr[H_N];
+  const int t = pr[P_T];
+  const int32_t* tnd = node_rec(P, t);
+
+  for (int k = tid; k < sides * R_COUNT * S; k += NT) ctx.rows[k] = 0.0;
+  // initial A at t
+  {
+    const int32_t* trp = P->ip + pr[P_TRP];
+    int nnz_t = trp[S];
+    for (int side = 0; side < sides; ++side) {
+      double* V = ctx.vals(side, pr[P_TBUF]);
+      if (pr[P_INIT] == 0) {
+        for (int k = tid; k < nnz_t; k += NT) V[k] = 1.0;     // row s -> entry (s, s)
+      } else {
+        int wt = tnd[N_W];
+        const double* Cb = wk.C + (size_t)bx.b * S * wt;
+        for (int k = tid; k < nnz_t; k += NT) V[k] = Cb[k];  // dense rows, entry order = (s, c)
+      }
+    }
+  }
+  __syncthreads();
+
+  const int op0 = pr[P_OP0], nop = pr[P_NOP];
+  for (int oi = 0; oi < nop; ++oi) {
+    const int32_t* op = P->ops + (op0 + oi) * OP_REC;
+    const int kind = op[O_KIND], v = op[O_V], slot = op[O_SLOT];
+    const int32_t* vnd = node_rec(P, v);
+    const int32_t* vrp = P->ip + op[O_VRP];
+    const int32_t* vcols = P->ip + op[O_VCOLS];
+    const double* pl = vnd[N_PLANE] >= 0 ? bx.planes + vnd[N_PLANE] : nullptr;
+    const bool relax = (kind == NK_SQR || kind == NK_EXP || kind == NK_LOG || kind == NK_SIN || kind == NK_COS);
+    const int ppe = kind == NK_MUL ? 6 : 4;
+    const int u = op[O_U];
+    const int32_t* und = u >= 0 ? node_rec(P, u) : nullptr;
+
+    // ---- phase A: per-row bias / charges / undefined rows over v's entries
+    if (op[O_FIRST]) {
+      bool need = relax || kind == NK_MUL || kind == NK_MULC || kind == NK_ADD || kind == NK_SUB ||
+                  kind == NK_ADDC || kind == NK_SUBC || kind == NK_RSUBC ||
+                  ((kind == NK_LINEAR) && vnd[N_B_OFF] >= 0);
+      if (need) {
+        const double* cvec = vnd[N_CVEC] >= 0 ? P->dp + vnd[N_CVEC] : nullptr;
+        const int32_t* map0 = vnd[N_MAP0] >= 0 ? P->ip + vnd[N_MAP0] : nullptr;
+        const int32_t* map1 = vnd[N_MAP1] >= 0 ? P->ip + vnd[N_MAP1] : nullptr;
+        const int32_t* inex = vnd[N_INEXACT] >= 0 ? P->ip + vnd[N_INEXACT] : nullptr;
+        const double* m0 = bx.mag + node_rec(P, vnd[N_IN0])[N_CUR];
+        const double* m1 = (kind == NK_ADD || kind == NK_SUB) ? bx.mag + node_rec(P, vnd[N_IN1])[N_CUR] : nullptr;
+        const double* bvec = (kind == NK_LINEAR && vnd[N_B_OFF] >= 0) ? P->dp + vnd[N_B_OFF] : nullptr;
+        for (int side = 0; side < sides; ++side) {
+          const double* V = ctx.vals(side, op[O_VBUF]);
+          double* rb = ctx.row(side, R_BIAS);
+          double* rm = ctx.row(side, R_BMAG);
+          double* rc = ctx.row(side, R_CHG);
+          double* ru = ctx.row(side, R_UNDEF);
+          // one thread per row for one-hot passes, a warp per row otherwise
+          const int rstep = onehot ? NT : NWARP;
+          const int rfirst = onehot ? tid : warp;
+          const int estep = onehot ? 1 : 32;
+          const int eoff = onehot ? 0 : lane;
+          for (int s = rfirst; s < S; s += rstep) {
+            int e0 = vrp[s], e1 = vrp[s + 1];
+            if (e0 == e1) continue;
+            double sb = 0, sm_ = 0, sc = 0;
+            int und_ = 0;
+            for (int e = e0 + eoff; e < e1; e += estep) {
+              double a = V[e];
+              int c = vcols[e];
+              if (relax || kind == NK_MUL) {
+                const double* p = pl + ppe * c;
+                double bt;
+                double na = elem_coef(kind, 0, side, a, p, 0.0, &bt);
+                double bt2 = 0.0, nb = 0.0;
+                if (kind == NK_MUL) nb = elem_coef(kind, 1, side, a, p, 0.0, &bt2);
+                if (a != 0.0 && (!isfinite(bt) || !isfinite(na) || !isfinite(nb))) und_ = 1;
+                if (isfinite(bt)) { sb += bt; sm_ += fabs(bt); }
+              } else if (kind == NK_MULC) {
+                double cv = cvec[c];
+                if (inex[c] && a != 0.0) {
+                  double m = m0[map0[c]];
+                  sc += isinf(m) ? INFINITY : fabs(a * cv) * m;
+                }
+              } else if (kind == NK_LINEAR) {
+                sb += a * bvec[c];
+                sm_ += fabs(a) * fabs(bvec[c]);
+              } else {
+                // add / sub / addc / subc / rsubc: output rounding (interval_bound.py:71-77)
+                double mx = m0[map0[c]];
+                double my = m1 ? m1[map1[c]] : fabs(cvec[c]);
+                double e_ = rounding_error(mx + my, 2);
+                double fa = finite_abs(a);
+                sc += fa > 0 ? (isinf(e_) ? INFINITY : fa * e_) : 0.0;
+                if (kind == NK_ADDC || kind == NK_SUBC || kind == NK_RSUBC) {
+                  double cv = kind == NK_SUBC ? -cvec[c] : cvec[c];
+                  sb += a * cv;
+                  sm_ += fabs(a) * fabs(cv);
+                }
+              }
+            }
+            if (!onehot) { sb = warp_sum(sb); sm_ = warp_sum(sm_); sc = warp_sum(sc); und_ = warp_or(und_); }
+            if (onehot || lane == 0) {
+              rb[s] += sb; rm[s] += sm_;
+              rc[s] += (kind == NK_MULC) ? UNIT * sc : sc;
+              if (und_) ru[s] = 1.0;
+            }
+          }
+        }
+      }
+    }
+
+    // ---- phase B: first contribution into u -> zero its buffer
+    if (!op[O_FOLD] && !op[O_UMERGE]) {
+      int nnz_u = op[O_UNNZ];
+      for (int side = 0; side < sides; ++side) {
+        double* U = ctx.vals(side, op[O_UBUF]);
+        for (int k = tid; k < nnz_u; k += NT) U[k] = 0.0;
+      }
+    }
+    __syncthreads();
+
+    // ---- phase C: contributions into u
+    if (op[O_FOLD]) {
+      // linear/matmul on the input, one entry per row: exact fold into the concretisation
+      const double* f = bx.fold + vnd[N_FOLD];
+      int w = vnd[N_W];
+      double gk = gamma_k((double)op[O_WOUT]);
+      for (int side = 0; side < sides; ++side) {
+        const double* V = ctx.vals(side, op[O_VBUF]);
+        double* rbase = ctx.row(side, R_BASE);
+        double* rdev = ctx.row(side, R_DEV);
+        double* rberr = ctx.row(side, R_BERR);
+        double* rc = ctx.row(side, R_CHG);
+        for (int s = tid; s < S; s += NT) {
+          int e0 = vrp[s], e1 = vrp[s + 1];
+          if (e0 == e1) continue;
+          double a = V[e0];
+          int c = vcols[e0];
+          rbase[s] += a * f[c];
+          rdev[s] += fabs(a) * f[w + c];
+          rberr[s] += fabs(a) * f[2 * w + c];
+          rc[s] += gk * (fabs(a) * f[2 * w + c]);
+        }
+      }
+    } else if (op[O_DENSE]) {
+      // GEMV per row: A_u[s, :] += sum_e A_v[e] W[c_e, :]; charge gamma_k <|A_v||W|, m_u>
+      const int32_t* urp = P->ip + op[O_URP];
+      const double* W = P->dp + vnd[N_W_OFF];
+      int win = vnd[N_WIN];
+      const double* mu = bx.mag + und[N_CUR];
+      double gk = gamma_k((double)op[O_WOUT]);
+      for (int side = 0; side < sides; ++side) {
+        const double* V = ctx.vals(side, op[O_VBUF]);
+        double* U = ctx.vals(side, op[O_UBUF]);
+        double* rc = ctx.row(side, R_CHG);
+        for (int s = warp; s < S; s += NWARP) {
+          int e0 = vrp[s], e1 = vrp[s + 1];
+          if (e0 == e1) continue;
+          double* Ur = U + urp[s];
+          double part = 0;
+          for (int j = lane; j < win; j += 32) {
+            double acc = 0, aabs = 0;
+            for (int e = e0; e < e1; ++e) {
+              double a = V[e];
+              double wv = W[(int64_t)vcols[e] * win + j];
+              acc += a * wv;
+              aabs += fabs(a) * fabs(wv);
+            }
+            Ur[j] += acc;
+            double m = mu[j];
+            part += aabs * (isinf(m) ? 0.0 : m);
+          }
+          part = warp_sum(part);
+          if (lane == 0) rc[s] += gk * part;
+        }
+      }
+    } else {
+      // pull moves: target entry <- sum of transformed source entries
+      const int ntgt = op[O_NTGT];
+      const int32_t* tgt = P->ip + op[O_TGT];
+      const int32_t* sptr = P->ip + op[O_SPTR];
+      const int32_t* src = P->ip + op[O_SRC];
+      const double* cvec = (kind == NK_MULC) ? P->dp + vnd[N_CVEC] : nullptr;
+      for (int side = 0; side < sides; ++side) {
+        const double* V = ctx.vals(side, op[O_VBUF]);
+        double* U = ctx.vals(side, op[O_UBUF]);
+        for (int k = tid; k < ntgt; k += NT) {
+          double acc = 0;
+          for (int q = sptr[k]; q < sptr[k + 1]; ++q) {
+            int e = src[q];
+            double a = V[e];
+            int c = vcols[e];
+            double bt;
+            double na = elem_coef(kind, slot, side, a, pl ? pl + ppe * c : nullptr, cvec ? cvec[c] : 0.0, &bt);
+            if (!isfinite(na)) na = 0.0;
+            acc += na;
+          }
+          U[tgt[k]] += acc;
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---- phase D: merge charge u <|A_u|, m_u> (A_u = old + new)
+    if (!op[O_FOLD] && op[O_UMERGE]) {
+      const int32_t* urp = P->ip + op[O_URP];
+      const int32_t* ucols = P->ip + op[O_UCOLS];
+      const double* mu = bx.mag + und[N_CUR];
+      for (int side = 0; side < sides; ++side) {
+        const double* U = ctx.vals(side, op[O_UBUF]);
+        double* rc = ctx.row(side, R_CHG);
+        for (int s = warp; s < S; s += NWARP) {
+          int e0 = urp[s], e1 = urp[s + 1];
+          double part = 0;
+          int hit = 0;
+          for (int e = e0 + lane; e < e1; e += 32) {
+            double a = fabs(U[e]);
+            double m = mu[ucols[e]];
+            if (isinf(m)) { if (a > 0) hit = 1; }
+            else part += a * m;
+          }
+          part = warp_sum(part);
+          hit = warp_or(hit);
+          if (lane == 0 && e1 > e0) rc[s] += hit ? INFINITY : UNIT * part;
+        }
+      }
+      __syncthreads();
+    }
+  }
+
+  // ---- concretisation at the input and outputs
+  const bool fold = pr[P_NFOLD] != 0;
+  const int xnnz = pr[P_XNNZ];
+  const int32_t* xrp = (!fold && xnnz > 0) ? P->ip + pr[P_XRP] : nullptr;
+  const int32_t* xcols = (!fold && xnnz > 0) ? P->ip + pr[P_XCOLS] : nullptr;
+  if (xrp) {
+    for (int side = 0; side < sides; ++side) {
+      const double* V = ctx.vals(side, pr[P_XBUF]);
+      double* rbase = ctx.row(side, R_BASE);
+      double* rdev = ctx.row(side, R_DEV);
+      double* rberr = ctx.row(side, R_BERR);
+      for (int s = warp; s < S; s += NWARP) {
+        int e0 = xrp[s], e1 = xrp[s + 1];
+        double bs = 0, dv = 0, be = 0;
+        for (int e = e0 + lane; e < e1; e += 32) {
+          double a = V[e];
+          int c = xcols[e];
+          double l = bx.xL[c], h = bx.xU[c];
+          bs += a * ((h + l) / 2.0);
+          dv += fabs(a) * ((h - l) / 2.0);
+          be += finite_abs(a) * finite_abs(fmax(fabs(l), fabs(h)));
+        }
+        bs = warp_sum(bs); dv = warp_sum(dv); be = warp_sum(be);
+        if (lane == 0) { rbase[s] += bs; rdev[s] += dv; rberr[s] += be; }
+      }
+    }
+  }
+  __syncthreads();
+  const double nvisit = (double)max(pr[P_NVISIT], 1);
+  const bool final = pr[P_FINAL] != 0;
+  for (int side = 0; side < sides; ++side) {
+    double sign = side == 0 ? -1.0 : 1.0;
+    for (int s = tid; s < S; s += NT) {
+      double bias = ctx.row(side, R_BIAS)[s];
+      double b = widen(bias, rounding_error(ctx.row(side, R_BMAG)[s], nvisit + n), sign);
+      double root = ctx.row(side, R_BASE)[s] + sign * ctx.row(side, R_DEV)[s];
+      root = widen(root, rounding_error(ctx.row(side, R_BERR)[s], n), sign);
+      if (!isfinite(root)) root = sign * INFINITY;
+      double tot = b + root;
+      tot = widen(tot, rounding_error(finite_abs(tot), 1) + ctx.row(side, R_CHG)[s], sign);
+      bool undef = ctx.row(side, R_UNDEF)[s] != 0.0;
+      if (undef) tot = sign * INFINITY;
+      if (final) {
+        double lbv = tot;
+        if (undef) {
+          // interval fallback for a discarded row (backward_bound.py:826)
+          double fb = 0;
+          if (pr[P_INIT] == 0) fb = bx.lo[tnd[N_CUR] + s];
+          else {
+            int wt = tnd[N_W];
+            const double* Cb = wk.C + ((size_t)bx.b * S + s) * wt;
+            for (int c = 0; c < wt; ++c) {
+              double cv = Cb[c];
+              fb += cv > 0 ? cv * bx.lo[tnd[N_CUR] + c] : (cv < 0 ? cv * bx.hi[tnd[N_CUR] + c] : 0.0);
+            }
+          }
+          lbv = fmax(lbv, fb);
+        }
+        wk.lb[(size_t)bx.b * S + s] = lbv;
+        if (wk.lbias) wk.lbias[(size_t)bx.b * S + s] = undef ? -INFINITY : tot - root;
+      } else {
+        double* out = side == 0 ? bx.pres_lo : bx.pres_hi;
+        out[s] = tot;
+      }
+    }
+  }
+  if (final && wk.lA) {
+    // dense lA rows: zero, then the input's entries (rows of undefined bounds stay zero)
+    double* lA = wk.lA + (size_t)bx.b * S * n;
+    for (int k = tid; k < S * n; k += NT) lA[k] = 0.0;
+    __syncthreads();
+    if (xrp) {
+      const double* V = ctx.vals(0, pr[P_XBUF]);
+      for (int s = warp; s < S; s += NWARP) {
+        if (ctx.row(0, R_UNDEF)[s] != 0.0) continue;
+        for (int e = xrp[s] + lane; e < xrp[s + 1]; e += 32) lA[(size_t)s * n + xcols[e]] = V[e];
+      }
+    }
+  }
+  __syncthreads();
+}
+
+__device__ void compare_node(const Box& bx, int v, double* tmp_lo, double* tmp_hi) {
+  // IBP of v from its inputs' current intervals, intersected with the pass result
+  const int32_t* nd = node_rec(bx.P, v);
+  int w = nd[N_W];
+  ibp_node(bx, v, tmp_lo, tmp_hi);
+  __syncthreads();
+  for (int j = threadIdx.x; j < w; j += NT) {
+    double l = nan_lo(bx.pres_lo[j]), h = nan_hi(bx.pres_hi[j]);
+    bx.lo[nd[N_CUR] + j] = fmax(l, tmp_lo[j]);
+    bx.hi[nd[N_CUR] + j] = fmin(h, tmp_hi[j]);
+  }
+}
+
+__global__ void __launch_bounds__(NT) crown_megakernel(DevProgram P, Work wk) {
+  extern __shared__ double sm[];
+  const int32_t* hdr = P.hdr;
+  const int arena = hdr[H_ARENA], planes_w = hdr[H_PLANES], fold_w = hdr[H_FOLDW], maxw = hdr[H_MAXW];
+  const int n = hdr[H_N];
+  double* slot = wk.scratch + (size_t)blockIdx.x * wk.slot_doubles;
+  Box bx;
+  bx.P = &P;
+  bx.lo = slot;
+  bx.hi = slot + arena;
+  bx.mag = slot + 2 * (size_t)arena;
+  bx.planes = slot + 3 * (size_t)arena;
+  bx.fold = bx.planes + planes_w;
+  bx.pres_lo = bx.fold + fold_w;
+  bx.pres_hi = bx.pres_lo + maxw;
+  double* tmp_lo = bx.pres_hi + maxw;
+  double* tmp_hi = tmp_lo + maxw;
+  const int nsteps = hdr[H_NSTEPS];
+  for (int64_t b = blockIdx.x; b < wk.B; b += gridDim.x) {
+    bx.b = b;
+    bx.xL = wk.xL + (size_t)b * n;
+    bx.xU = wk.xU + (size_t)b * n;
+    for (int j = threadIdx.x; j < n; j += NT) { bx.lo[j] = bx.xL[j]; bx.hi[j] = bx.xU[j]; }
+    __syncthreads();
+    for (int si = 0; si < nsteps; ++si) {
+      const int32_t* st = P.steps + si * STEP_REC;
+      const int type = st[0], a = st[1];
+      switch (type) {
+        case ST_FOLD: fold_node(bx, a); break;
+        case ST_IBP: {
+          const int32_t* nd = node_rec(&P, a);
+          ibp_node(bx, a, tmp_lo, tmp_hi);
+          __syncthreads();
+          for (int j = threadIdx.x; j < nd[N_W]; j += NT) {
+            bx.lo[nd[N_CUR] + j] = tmp_lo[j];
+            bx.hi[nd[N_CUR] + j] = tmp_hi[j];
+          }
+          break;
+        }
+        case ST_MAG: {
+          const int32_t* nd = node_rec(&P, a);
+          for (int j = threadIdx.x; j < nd[N_W]; j += NT) {
+            double l = bx.lo[nd[N_CUR] + j], h = bx.hi[nd[N_CUR] + j];
+            bx.mag[nd[N_CUR] + j] = l > h ? INFINITY : fmax(-l, h);
+          }
+          break;
+        }
+        case ST_RELAX: relax_node(bx, a); break;
+        case ST_PASS: case ST_FINAL: run_pass(bx, a, sm, wk); break;
+        case ST_COMPARE: compare_node(bx, a, tmp_lo, tmp_hi); break;
+        default: break;
+      }
+      __syncthreads();
+    }
+  }
+}
+
+}  // namespace gear

@@ -1,0 +1,158 @@
+// C ABI of libgear_b200.so: program upload, workspace sizing, megakernel launch.
+// Declarations and the reference interfaces they replace: include/gear_b200.h.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <new>
+#include <string>
+
+#include "../../include/gear_b200.h"
+#include "crown_kernel.cuh"
+
+namespace {
+thread_local std::string g_err;
+thread_local int g_launches = 0;
+
+int fail(int code, const char* fmt, const char* detail = "") {
+  char buf[512];
+  snprintf(buf, sizeof(buf), fmt, detail);
+  g_err = buf;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+  int code = (e == cudaErrorMemoryAllocation) ? GEAR_E_NOMEM : GEAR_E_CUDA;
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  g_err = m;
+  return code;
+}
+}  // namespace
+
+struct gear_dag {
+  gear::DevProgram P;
+  void* dev = nullptr;
+  int32_t hdr[gear::HEADER_LEN];
+  int64_t slot_doubles = 0;
+  int smem_bytes = 0;
+  int device = 0;
+  int num_sms = 0;
+  int blocks_per_sm = 0;
+};
+
+extern "C" const char* gear_last_error(void) { return g_err.c_str(); }
+extern "C" int gear_last_launch_count(void) { return g_launches; }
+
+extern "C" int gear_dag_create(const int32_t* header, int64_t header_len, const int32_t* nodes,
+                               int64_t n_nodes_ints, const int32_t* steps, int64_t n_steps_ints,
+                               const int32_t* passes, int64_t n_passes_ints, const int32_t* ops,
+                               int64_t n_ops_ints, const int32_t* int_pool, int64_t n_int,
+                               const double* dbl_pool, int64_t n_dbl, gear_dag** out) {
+  if (!out || !header || header_len != gear::HEADER_LEN || !nodes || !steps)
+    return fail(GEAR_E_INVALID, "gear_dag_create: %s", "bad arguments");
+  using namespace gear;
+  if (n_nodes_ints != (int64_t)header[H_NNODES] * NODE_REC || n_steps_ints != (int64_t)header[H_NSTEPS] * STEP_REC ||
+      n_passes_ints != (int64_t)header[H_NPASSES] * PASS_REC || n_ops_ints != (int64_t)header[H_NOPS] * OP_REC)
+    return fail(GEAR_E_INVALID, "gear_dag_create: %s", "record counts do not match the header");
+  gear_dag* d = new (std::nothrow) gear_dag();
+  if (!d) return fail(GEAR_E_NOMEM, "gear_dag_create: %s", "host allocation");
+  memcpy(d->hdr, header, sizeof(d->hdr));
+  // one device block: doubles first (8-byte aligned), then int arrays
+  size_t nd = (size_t)n_dbl, ni = (size_t)(header_len + n_nodes_ints + n_steps_ints + n_passes_ints + n_ops_ints + n_int);
+  size_t bytes = nd * sizeof(double) + ni * sizeof(int32_t) + 64;
+  cudaError_t e = cudaGetDevice(&d->device);
+  if (e != cudaSuccess) { delete d; return cuda_fail(e, "cudaGetDevice"); }
+  e = cudaMalloc(&d->dev, bytes);
+  if (e != cudaSuccess) { delete d; return cuda_fail(e, "cudaMalloc(program)"); }
+  char* base = (char*)d->dev;
+  double* dp = (double*)base;
+  int32_t* ip = (int32_t*)(base + nd * sizeof(double));
+  size_t o = 0;
+  auto put = [&](const int32_t* src, int64_t cnt) -> const int32_t* {
+    int32_t* dst = ip + o;
+    if (cnt > 0) cudaMemcpy(dst, src, cnt * sizeof(int32_t), cudaMemcpyHostToDevice);
+    o += (size_t)cnt;
+    return dst;
+  };
+  d->P.hdr = put(header, header_len);
+  d->P.nodes = put(nodes, n_nodes_ints);
+  d->P.steps = put(steps, n_steps_ints);
+  d->P.passes = put(passes, n_passes_ints);
+  d->P.ops = put(ops, n_ops_ints);
+  d->P.ip = put(int_pool, n_int);
+  if (nd > 0) cudaMemcpy(dp, dbl_pool, nd * sizeof(double), cudaMemcpyHostToDevice);
+  d->P.dp = dp;
+  e = cudaGetLastError();
+  if (e != cudaSuccess) { cudaFree(d->dev); delete d; return cuda_fail(e, "upload"); }
+  // per-CTA scratch: lo, hi, mag arenas; planes; fold vectors; 4 node-wide temporaries
+  d->slot_doubles = 3 * (int64_t)header[H_ARENA] + header[H_PLANES] + header[H_FOLDW] + 4 * (int64_t)header[H_MAXW] + 8;
+  d->slot_doubles = (d->slot_doubles + 31) / 32 * 32;
+  d->smem_bytes = header[H_SMEM] * (int)sizeof(double);
+  cudaDeviceProp prop;
+  e = cudaGetDeviceProperties(&prop, d->device);
+  if (e != cudaSuccess) { cudaFree(d->dev); delete d; return cuda_fail(e, "cudaGetDeviceProperties"); }
+  if (d->smem_bytes > (int)prop.sharedMemPerBlockOptin) {
+    cudaFree(d->dev);
+    delete d;
+    return fail(GEAR_E_INVALID, "gear_dag_create: %s", "pass working set exceeds shared memory");
+  }
+  e = cudaFuncSetAttribute(gear::crown_megakernel, cudaFuncAttributeMaxDynamicSharedMemorySize, d->smem_bytes);
+  if (e != cudaSuccess) { cudaFree(d->dev); delete d; return cuda_fail(e, "cudaFuncSetAttribute"); }
+  d->num_sms = prop.multiProcessorCount;
+  int bps = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, gear::crown_megakernel, gear::NT, d->smem_bytes);
+  if (e != cudaSuccess || bps < 1) bps = 1;
+  d->blocks_per_sm = bps;
+  *out = d;
+  return GEAR_OK;
+}
+
+extern "C" int gear_dag_destroy(gear_dag* dag) {
+  if (!dag) return GEAR_OK;
+  if (dag->dev) cudaFree(dag->dev);
+  delete dag;
+  return GEAR_OK;
+}
+
+static int64_t slots_for(const gear_dag* d, int64_t batch) {
+  int64_t slots = (int64_t)d->num_sms * d->blocks_per_sm;
+  if (batch < slots) slots = batch;
+  return slots < 1 ? 1 : slots;
+}
+
+extern "C" int64_t gear_crown_workspace_bytes(const gear_dag* dag, int64_t batch) {
+  if (!dag || batch < 0) return -1;
+  return slots_for(dag, batch) * dag->slot_doubles * (int64_t)sizeof(double);
+}
+
+extern "C" int gear_crown_lower(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
+                                const double* C, double* lb, double* lA, double* lbias, void* workspace,
+                                int64_t workspace_bytes, void* stream) {
+  g_launches = 0;
+  if (!dag || !x_L || !x_U || !lb || batch < 0) return fail(GEAR_E_INVALID, "gear_crown_lower: %s", "bad arguments");
+  if (batch == 0) return GEAR_OK;
+  if (!workspace || workspace_bytes < gear_crown_workspace_bytes(dag, batch))
+    return fail(GEAR_E_WORKSPACE, "gear_crown_lower: %s", "workspace too small");
+  if (dag->hdr[gear::H_RETA] == 0 && lA) return fail(GEAR_E_INVALID, "gear_crown_lower: %s", "program built without A");
+  gear::Work wk;
+  wk.xL = x_L;
+  wk.xU = x_U;
+  wk.C = C;
+  wk.lb = lb;
+  wk.lA = lA;
+  wk.lbias = lbias;
+  wk.scratch = (double*)workspace;
+  wk.slot_doubles = dag->slot_doubles;
+  wk.B = batch;
+  wk.status = nullptr;
+  int64_t slots = slots_for(dag, batch);
+  // the kernel's dynamic shared-memory limit is per function: set it for this program
+  cudaError_t ea = cudaFuncSetAttribute(gear::crown_megakernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        dag->smem_bytes);
+  if (ea != cudaSuccess) return cuda_fail(ea, "cudaFuncSetAttribute");
+  gear::crown_megakernel<<<(unsigned)slots, gear::NT, dag->smem_bytes, (cudaStream_t)stream>>>(dag->P, wk);
+  g_launches = 1;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "crown_megakernel launch");
+  return GEAR_OK;
+}

@@ -1,0 +1,51 @@
+// Device-side layout of a compiled CROWN program (host side: gear_b200/program.py).
+// All records are int32; offsets index the int pool (ip) or the float64 pool (dp).
+#pragma once
+#include <stdint.h>
+
+namespace gear {
+
+enum NodeKind {
+  NK_INPUT = 0, NK_LINEAR = 1, NK_MATMUL = 2, NK_MUL = 3, NK_MULC = 4, NK_ADD = 5, NK_SUB = 6,
+  NK_ADDC = 7, NK_SUBC = 8, NK_RSUBC = 9, NK_NEG = 10, NK_SQR = 11, NK_EXP = 12, NK_LOG = 13,
+  NK_SIN = 14, NK_COS = 15, NK_POW = 16, NK_REDUCESUM = 17, NK_MAP = 18, NK_CONCAT = 19
+};
+
+enum NodeField {
+  N_KIND = 0, N_W, N_NIN, N_IN0, N_IN1, N_CUR, N_PLANE, N_CVEC, N_MAP0, N_MAP1, N_W_OFF, N_B_OFF,
+  N_WIN, N_INS, N_FOLD, N_INEXACT, NODE_REC
+};
+
+enum StepType { ST_IBP = 0, ST_MAG = 1, ST_RELAX = 2, ST_PASS = 3, ST_COMPARE = 4, ST_FOLD = 5, ST_FINAL = 6 };
+constexpr int STEP_REC = 4;
+
+enum PassField {
+  P_T = 0, P_S, P_SIDES, P_INIT, P_OP0, P_NOP, P_TBUF, P_XNNZ, P_XBUF, P_XRP, P_XCOLS, P_NFOLD,
+  P_SMEM, P_TRP, P_TCOLS, P_FINAL, P_NVISIT, P_MAXROW, P_ONEHOT, PASS_REC = 24
+};
+
+enum OpField {
+  O_KIND = 0, O_V, O_SLOT, O_FIRST, O_VBUF, O_VNNZ, O_VRP, O_VCOLS, O_U, O_UBUF, O_UNNZ, O_URP,
+  O_UCOLS, O_UMERGE, O_NTGT, O_TGT, O_SPTR, O_SRC, O_DENSE, O_FOLD, O_WOUT, OP_REC = 24
+};
+
+enum HeaderField {
+  H_NNODES = 0, H_NSTEPS, H_NPASSES, H_NOPS, H_N, H_S, H_T, H_ARENA, H_PLANES, H_FOLDW,
+  H_SMEM, H_MAXS, H_SINOFF, H_MAXW, H_RETA, H_R15, HEADER_LEN = 16
+};
+
+// Sin/cos table layout inside the float64 pool, from H_SINOFF (gear_b200/tables.py order).
+constexpr int SIN_N_PRE = 162;   // int(pi/2 / 0.01) + 5
+constexpr int SIN_N_TB = 1001;
+
+struct DevProgram {
+  const int32_t* hdr;
+  const int32_t* nodes;
+  const int32_t* steps;
+  const int32_t* passes;
+  const int32_t* ops;
+  const int32_t* ip;
+  const double* dp;
+};
+
+}  // namespace gear

@@ -1,0 +1,634 @@
+"""Host compiler: a traced ``Graph`` -> a flat device program for the CROWN megakernel.
+
+Two things are decided here, once per graph, on the host:
+
+1. **The schedule** -- which nodes get intermediate bounds, by IBP or by a CROWN pass, in
+   which order, and which transient IBP recomputations ``compare_with_IBP`` needs. It is a
+   symbolic replay of the reference's recursion (``auto_LiRPA/bound_general.py:1032-1222``
+   ``check_prior_bounds`` / ``compute_intermediate_bounds``, ``interval_bound.py:310-406``),
+   which depends only on the graph, never on box values.
+
+2. **Static A sparsity per pass** -- the backward BFS (``backward_bound.py:880-1206``) is
+   replayed symbolically and, for every node a pass visits, the set of (spec row, column)
+   entries of its A matrix that can be nonzero is computed. Rows of an identity
+   specification stay one-hot through elementwise chains, slices and gathers, so the
+   intermediate passes (C = I over the node width) cost O(width) instead of
+   O(width^2). Zero entries contribute exactly zero in the reference's dense arithmetic,
+   so skipping them changes no bound. Each pass op becomes a list of pull "moves"
+   (target entry <- source entries) that the kernel executes per box.
+
+   One further exact rewrite: when the only contribution to the input node in a
+   non-final pass comes from a Linear/MatMul on the input and every row reaches it with at
+   most one nonzero, the input's A row is ``a * W[c, :]`` and its box concretisation
+   ``a W[c] x0 -/+ |a| |W[c]| eps`` is read from per-box vectors ``W x0`` and ``|W| eps``
+   (``fold``) instead of materialising ``w_out x n`` coefficients.
+
+The output is a handful of int32 / float64 arrays (layout constants below mirror
+``csrc/gear_program.h``).
+"""
+from __future__ import annotations
+
+from collections import deque
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+
+from . import tables
+from .graph import Graph, MAP_KINDS
+
+# ---- node kinds (csrc/gear_program.h: enum NodeKind)
+NK = {"input": 0, "linear": 1, "matmul": 2, "mul": 3, "mulc": 4, "add": 5, "sub": 6, "addc": 7,
+      "subc": 8, "rsubc": 9, "neg": 10, "sqr": 11, "exp": 12, "log": 13, "sin": 14, "cos": 15,
+      "pow": 16, "reducesum": 17, "map": 18, "concat": 19}
+NODE_REC = 16
+# node record fields
+N_KIND, N_W, N_NIN, N_IN0, N_IN1, N_CUR, N_PLANE, N_CVEC, N_MAP0, N_MAP1, N_W_OFF, N_B_OFF, \
+    N_WIN, N_INS, N_FOLD, N_INEXACT = range(16)
+
+# ---- steps
+ST = {"ibp": 0, "mag": 1, "relax": 2, "pass": 3, "compare": 4, "fold": 5, "final": 6}
+STEP_REC = 4
+
+PASS_REC = 24
+(P_T, P_S, P_SIDES, P_INIT, P_OP0, P_NOP, P_TBUF, P_XNNZ, P_XBUF, P_XRP, P_XCOLS, P_NFOLD,
+ P_SMEM, P_TRP, P_TCOLS, P_FINAL, P_NVISIT, P_MAXROW, P_ONEHOT, P_R19, P_R20, P_R21, P_R22, P_R23) = range(24)
+
+OP_REC = 24
+(O_KIND, O_V, O_SLOT, O_FIRST, O_VBUF, O_VNNZ, O_VRP, O_VCOLS, O_U, O_UBUF, O_UNNZ, O_URP,
+ O_UCOLS, O_UMERGE, O_NTGT, O_TGT, O_SPTR, O_SRC, O_DENSE, O_FOLD, O_WOUT, O_R21, O_R22, O_R23) = range(24)
+
+PLANES_PER_ELEM = {"mul": 6, "sqr": 4, "exp": 4, "log": 4, "sin": 4, "cos": 4, "pow": 4}
+
+TIE_TOL = 1e-12
+
+
+class ProgramError(ValueError):
+    pass
+
+
+@dataclass
+class PassInfo:
+    t: int
+    S: int
+    sides: int
+    final: bool
+    init: int                 # 0 identity, 1 dense C
+    order: List[int] = field(default_factory=list)       # BFS visit order (excl. root)
+    patterns: Dict[int, List[np.ndarray]] = field(default_factory=dict)   # node -> per-row sorted cols
+
+
+class Pools:
+    def __init__(self):
+        self.ints: List[np.ndarray] = []
+        self.n_int = 0
+        self.dbl: List[np.ndarray] = []
+        self.n_dbl = 0
+
+    def add_int(self, a) -> int:
+        a = np.ascontiguousarray(np.asarray(a, dtype=np.int32).reshape(-1))
+        off = self.n_int
+        self.ints.append(a)
+        self.n_int += a.size
+        return off
+
+    def add_dbl(self, a) -> int:
+        a = np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1))
+        # 32-byte alignment of every vector (coalesced row reads of W)
+        pad = (-self.n_dbl) % 4
+        if pad:
+            self.dbl.append(np.zeros(pad))
+            self.n_dbl += pad
+        off = self.n_dbl
+        self.dbl.append(a)
+        self.n_dbl += a.size
+        return off
+
+    def int_array(self):
+        return np.concatenate(self.ints) if self.ints else np.zeros(0, np.int32)
+
+    def dbl_array(self):
+        return np.concatenate(self.dbl) if self.dbl else np.zeros(0, np.float64)
+
+
+class Program:
+    """Compiled device program for one graph and one final specification shape."""
+
+    def __init__(self, graph: Graph, spec_rows: Optional[int] = None, dense_c: bool = False,
+                 return_a: bool = True, smem_limit: int = 200 * 1024):
+        self.g = graph
+        self.n = graph[0].width
+        t = graph.output
+        self.t = t
+        self.S = graph[t].width if spec_rows is None else int(spec_rows)
+        self.dense_c = bool(dense_c)
+        self.return_a = return_a
+        self.smem_limit = smem_limit
+        self.pools = Pools()
+        self.steps: List[Tuple[int, int, int, int]] = []
+        self.passes: List[PassInfo] = []
+        self.pass_recs: List[np.ndarray] = []
+        self.op_recs: List[np.ndarray] = []
+        self.log: List[tuple] = []
+        self._layout_nodes()
+        self._schedule()
+        self._emit_nodes()
+        self._finish()
+
+    # ================================================================= node layout
+    def _layout_nodes(self):
+        g = self.g
+        self.cur_off = {}
+        off = 0
+        for nd in g.nodes:
+            self.cur_off[nd.id] = off
+            off += nd.width
+        self.arena_w = off            # doubles per box per (lo | hi | mag) arena
+        self.plane_off = {}
+        off = 0
+        for nd in g.nodes:
+            if nd.kind in PLANES_PER_ELEM:
+                if nd.kind == "pow":
+                    raise ProgramError("pow with exponent other than 2 is not supported by the GPU engine")
+                self.plane_off[nd.id] = off
+                off += nd.width * PLANES_PER_ELEM[nd.kind]
+        self.plane_w = off
+        # linear/matmul directly on the input: per-box fold vectors W x0, |W| eps, |W| max|x|
+        self.fold_off = {}
+        off = 0
+        for nd in g.nodes:
+            if nd.kind in ("linear", "matmul") and nd.inputs[0] == 0:
+                self.fold_off[nd.id] = off
+                off += 3 * nd.width
+        self.fold_w = off
+        self.maxw = max(nd.width for nd in g.nodes)
+
+    # ================================================================= schedule
+    def _ancestors(self, t):
+        seen, stack = set(), [t]
+        while stack:
+            v = stack.pop()
+            if v in seen:
+                continue
+            seen.add(v)
+            stack += self.g[v].inputs
+        return seen
+
+    def _schedule(self):
+        g = self.g
+        self.anc = self._ancestors(self.t)
+        self.stored = {0}
+        self.prior_checked = set()
+        # fold vectors first (they only depend on the input box)
+        for v in sorted(self.fold_off):
+            self.steps.append((ST["fold"], v, 0, 0))
+        # plain IBP of every node: magnitudes of nodes without stored bounds
+        for nd in g.nodes[1:]:
+            self.steps.append((ST["ibp"], nd.id, 0, 0))
+        for nd in g.nodes:
+            self.steps.append((ST["mag"], nd.id, 0, 0))
+        self.relaxed = set()
+        self._check_prior(self.t, final=True)
+        # interval of the final node for the undefined-row fallback
+        self._transient_ibp(self.t, set())
+        self.steps.append((ST["ibp"], self.t, 0, 0))
+        self._ensure_relax_for_pass(self.t)
+        pid = self._add_pass(self.t, self.S, sides=1, final=True, init=1 if self.dense_c else 0)
+        self.steps.append((ST["final"], pid, 0, 0))
+        self.log.append(("final", self.t))
+
+    def _check_prior(self, v, final=False):
+        g = self.g
+        n = g[v]
+        if v in self.prior_checked or v not in self.anc or n.kind == "input":
+            return
+        if final and n.kind == "concat" and not self.dense_c:
+            # identity C: every concatenated input is used (bound_general.py:1036-1052)
+            for p in n.inputs:
+                self._check_prior(p)
+        else:
+            for p in n.inputs:
+                self._check_prior(p)
+        for i, p in enumerate(n.inputs):
+            if i in n.requires_input_bounds or g[p].has_constraint:
+                self._compute_intermediate(p)
+        self.prior_checked.add(v)
+
+    def _store_ibp(self, v):
+        g = self.g
+        for p in g[v].inputs:
+            if p not in self.stored:
+                self._store_ibp(p)
+        self.steps.append((ST["ibp"], v, 0, 0))
+        self.steps.append((ST["mag"], v, 0, 0))
+        self.stored.add(v)
+        self.log.append(("ibp", v))
+
+    def _transient_ibp(self, v, done):
+        """IBP of v's non-stored ancestors from stored bounds (not stored)."""
+        g = self.g
+        for p in g[v].inputs:
+            if p not in self.stored and p not in done:
+                self._transient_ibp(p, done)
+                self.steps.append((ST["ibp"], p, 0, 0))
+                done.add(p)
+
+    def _compute_intermediate(self, v):
+        g = self.g
+        if v in self.stored:
+            return
+        n = g[v]
+        if n.kind == "reshape" and n.inputs[0] in self.stored:
+            self.steps.append((ST["ibp"], v, 0, 0))
+            self.steps.append((ST["mag"], v, 0, 0))
+            self.stored.add(v)
+            self.log.append(("ibp", v))
+            return
+        chain, cur, ok = [], v, True
+        while cur not in self.stored:
+            if not g[cur].ibp_intermediate:
+                ok = False
+                break
+            chain.append(cur)
+            cur = g[cur].inputs[0]
+        if ok:
+            for c in reversed(chain):
+                self._store_ibp(c)
+            return
+        if n.kind == "linear" and n.inputs[0] == 0:
+            self._store_ibp(v)
+            return
+        self._ensure_relax_for_pass(v)
+        pid = self._add_pass(v, n.width, sides=2, final=False, init=0)
+        self.steps.append((ST["pass"], pid, 0, 0))
+        self._transient_ibp(v, set())
+        self.steps.append((ST["compare"], v, pid, 0))
+        self.steps.append((ST["mag"], v, 0, 0))
+        self.stored.add(v)
+        self.log.append(("crown", v))
+
+    def _ensure_relax_for_pass(self, t):
+        """Relaxation planes of every relaxing node the pass visits (their inputs are stored)."""
+        for v in sorted(self._ancestors(t)):
+            nd = self.g[v]
+            if nd.kind in PLANES_PER_ELEM and v not in self.relaxed:
+                for p in nd.inputs:
+                    if p not in self.stored:
+                        raise ProgramError(f"relaxation of node {v} before its input {p} has bounds")
+                self.steps.append((ST["relax"], v, 0, 0))
+                self.relaxed.add(v)
+
+    # ================================================================= passes
+    def _bfs(self, t):
+        g = self.g
+        deg, added, q = {}, {t}, deque([t])
+        while q:
+            l = q.popleft()
+            for p in g[l].inputs:
+                deg[p] = deg.get(p, 0) + 1
+                if p not in added:
+                    q.append(p)
+                    added.add(p)
+        order, queue = [], deque([t])
+        while queue:
+            l = queue.popleft()
+            if l == 0:
+                continue
+            for p in g[l].inputs:
+                deg[p] -= 1
+                if deg[p] == 0:
+                    queue.append(p)
+            order.append(l)
+        return order
+
+    def _contrib(self, n, slot, rows_cols):
+        """Columns of input `slot` reached from each row's columns of node n."""
+        g = self.g
+        k, a = n.kind, n.attrs
+        p = n.inputs[slot]
+        w_in = g[p].width
+        out = []
+        if k in ("linear", "matmul"):
+            full = np.arange(w_in, dtype=np.int64)
+            return [full if len(c) else c for c in rows_cols]
+        if k in ("neg", "sqr", "exp", "log", "sin", "cos", "pow"):
+            return rows_cols
+        if k in ("mulc", "addc", "subc", "rsubc"):
+            m = a["map0"]
+        elif k in ("mul", "add", "sub"):
+            m = a["map0"] if slot == 0 else a["map1"]
+        elif k in MAP_KINDS:
+            m = a["map"]
+        elif k == "reducesum":
+            rmap = a["rmap"]
+            inv = {}
+            for i, o in enumerate(rmap):
+                inv.setdefault(int(o), []).append(i)
+            for c in rows_cols:
+                s = sorted(set(i for o in c for i in inv.get(int(o), [])))
+                out.append(np.array(s, dtype=np.int64))
+            return out
+        elif k == "concat":
+            off = sum(g[q].width for q in n.inputs[:slot])
+            cm = a["cmap"] - off
+            for c in rows_cols:
+                e = cm[c]
+                out.append(np.unique(e[(e >= 0) & (e < w_in)]))
+            return out
+        else:
+            raise ProgramError(k)
+        return [np.unique(m[c]) for c in rows_cols]
+
+    def _add_pass(self, t, S, sides, final, init):
+        g = self.g
+        order = self._bfs(t)
+        pi = PassInfo(t=t, S=S, sides=sides, final=final, init=init, order=order)
+        wt = g[t].width
+        if init == 0:
+            if S != wt:
+                raise ProgramError("an identity specification needs one row per output element")
+            pi.patterns[t] = [np.array([s], dtype=np.int64) for s in range(S)]
+        else:
+            pi.patterns[t] = [np.arange(wt, dtype=np.int64) for _ in range(S)]
+        # symbolic propagation
+        for v in order:
+            n = g[v]
+            pv = pi.patterns.get(v)
+            if pv is None:
+                continue
+            for slot, p in enumerate(n.inputs):
+                c = self._contrib(n, slot, pv)
+                if p not in pi.patterns:
+                    pi.patterns[p] = [np.array(x, dtype=np.int64) for x in c]
+                else:
+                    pi.patterns[p] = [np.union1d(a_, b_) for a_, b_ in zip(pi.patterns[p], c)]
+        self.passes.append(pi)
+        return len(self.passes) - 1
+
+    # ================================================================= emission
+    def _emit_nodes(self):
+        g = self.g
+        P = self.pools
+        recs = np.full((len(g), NODE_REC), -1, dtype=np.int32)
+        for nd in g.nodes:
+            r = recs[nd.id]
+            k = nd.kind if nd.kind not in MAP_KINDS else "map"
+            r[N_KIND] = NK[k]
+            r[N_W] = nd.width
+            r[N_NIN] = len(nd.inputs)
+            r[N_IN0] = nd.inputs[0] if nd.inputs else -1
+            r[N_IN1] = nd.inputs[1] if len(nd.inputs) > 1 else -1
+            r[N_CUR] = self.cur_off[nd.id]
+            r[N_PLANE] = self.plane_off.get(nd.id, -1)
+            r[N_FOLD] = self.fold_off.get(nd.id, -1)
+            a = nd.attrs
+            if k in ("mulc", "addc", "subc", "rsubc"):
+                r[N_CVEC] = P.add_dbl(a["c"])
+                r[N_MAP0] = P.add_int(a["map0"])
+                if k == "mulc":
+                    c = a["c"]
+                    exact = (c == 0) | (np.abs(np.frexp(c)[0]) == 0.5)
+                    r[N_INEXACT] = P.add_int((~exact).astype(np.int32))
+            elif k in ("mul", "add", "sub"):
+                r[N_MAP0] = P.add_int(a["map0"])
+                r[N_MAP1] = P.add_int(a["map1"])
+            elif k == "map":
+                r[N_MAP0] = P.add_int(a["map"])
+            elif k == "reducesum":
+                r[N_MAP0] = P.add_int(a["rmap"])
+                r[N_WIN] = g[nd.inputs[0]].width
+                # inverse map for the interval sums: ptr (w_out + 1) then input ids
+                order = np.argsort(a["rmap"], kind="stable")
+                cnt = np.bincount(a["rmap"], minlength=nd.width)
+                ptr = np.concatenate([[0], np.cumsum(cnt)])
+                r[N_MAP1] = P.add_int(np.concatenate([ptr, order]))
+            elif k == "concat":
+                r[N_MAP0] = P.add_int(a["cmap"])
+                r[N_INS] = P.add_int(nd.inputs)
+                r[N_WIN] = sum(g[q].width for q in nd.inputs)
+            elif k in ("linear", "matmul"):
+                W = a["W"] if k == "linear" else a["W"].T      # (out, in)
+                r[N_W_OFF] = P.add_dbl(np.ascontiguousarray(W))
+                r[N_WIN] = W.shape[1]
+                if k == "linear" and a.get("b") is not None:
+                    r[N_B_OFF] = P.add_dbl(a["b"])
+        self.node_recs = recs
+        # sin/cos tables
+        tb = tables.build()
+        self.sin_off = P.add_dbl(np.concatenate([tb[k] for k in tables.SIN_TABLE_ORDER]))
+        self.sin_lens = [len(tb[k]) for k in tables.SIN_TABLE_ORDER]
+
+    def _finish(self):
+        self.max_smem = 0
+        self.max_S = 1
+        for pid, pi in enumerate(self.passes):
+            self._emit_pass(pid, pi)
+        self.node_arr = self.node_recs.reshape(-1)
+        self.step_arr = np.array(self.steps, dtype=np.int32).reshape(-1)
+        self.pass_arr = np.stack(self.pass_recs).reshape(-1) if self.pass_recs else np.zeros(0, np.int32)
+        self.op_arr = np.stack(self.op_recs).reshape(-1) if self.op_recs else np.zeros(0, np.int32)
+        self.int_pool = self.pools.int_array()
+        self.dbl_pool = self.pools.dbl_array()
+        self.header = np.array([len(self.g), len(self.steps), len(self.passes), len(self.op_recs),
+                                self.n, self.S, self.t, self.arena_w, self.plane_w, self.fold_w,
+                                self.max_smem, self.max_S, self.sin_off, self.maxw,
+                                1 if self.return_a else 0, 0], dtype=np.int32)
+
+    def _emit_pass(self, pid, pi: PassInfo):
+        g = self.g
+        P = self.pools
+        S = pi.S
+        pats = pi.patterns
+        # entry tables per node
+        rowptr, cols, nnz, lookup = {}, {}, {}, {}
+        for v, pr in pats.items():
+            lens = np.array([len(c) for c in pr], dtype=np.int64)
+            rp = np.concatenate([[0], np.cumsum(lens)])
+            cc = np.concatenate(pr) if len(pr) else np.zeros(0, np.int64)
+            rowptr[v], cols[v], nnz[v] = rp, cc, int(rp[-1])
+        # fold decision: root contributions only from linear/matmul-on-input ops with
+        # at most one entry per row, in a non-final pass
+        contributors = [v for v in pi.order if 0 in g[v].inputs and v in pats]
+        fold = (not pi.final and len(contributors) > 0 and
+                all(g[v].kind in ("linear", "matmul") and v in self.fold_off and
+                    np.diff(rowptr[v]).max(initial=0) <= 1 for v in contributors))
+        # liveness-based buffer allocation (doubles per side)
+        first_use = {pi.t: -1}
+        last_use = {}
+        for i, v in enumerate(pi.order):
+            last_use[v] = i
+            for p in g[v].inputs:
+                if p not in first_use:
+                    first_use[p] = i
+        if not fold:
+            last_use[0] = len(pi.order)
+        free, bufoff, top = [], {}, 0
+
+        def alloc(v):
+            nonlocal top
+            size = max(nnz.get(v, 0), 1)
+            size = (size + 3) // 4 * 4
+            for k, (o, s_) in enumerate(free):
+                if s_ >= size:
+                    free.pop(k)
+                    if s_ > size:
+                        free.append((o + size, s_ - size))
+                    return o
+            o = top
+            top += size
+            return o
+
+        def release(v):
+            free.append((bufoff[v], (max(nnz.get(v, 0), 1) + 3) // 4 * 4))
+
+        bufoff[pi.t] = alloc(pi.t)
+        op_begin = len(self.op_recs)
+        merged_before = {pi.t}
+        for i, v in enumerate(pi.order):
+            n = g[v]
+            if v not in pats:
+                continue
+            for slot, p in enumerate(n.inputs):
+                if p == 0 and fold:
+                    continue
+                if p not in bufoff and p in pats:
+                    bufoff[p] = alloc(p)
+            k = n.kind
+            for slot, p in enumerate(n.inputs):
+                r = np.full(OP_REC, -1, dtype=np.int32)
+                kk = k if k not in MAP_KINDS else "map"
+                r[O_KIND] = NK[kk]
+                r[O_V] = v
+                r[O_SLOT] = slot
+                r[O_FIRST] = 1 if slot == 0 else 0
+                r[O_VBUF] = bufoff[v]
+                r[O_VNNZ] = nnz[v]
+                r[O_VRP] = P.add_int(rowptr[v])
+                r[O_VCOLS] = P.add_int(cols[v])
+                r[O_U] = p
+                r[O_WOUT] = n.width
+                r[O_DENSE] = 1 if k in ("linear", "matmul") else 0
+                r[O_FOLD] = 1 if (p == 0 and fold) else 0
+                if r[O_FOLD] == 1:
+                    r[O_UBUF] = -1
+                    r[O_UNNZ] = 0
+                    r[O_UMERGE] = 0
+                    self.op_recs.append(r)
+                    continue
+                r[O_UBUF] = bufoff[p]
+                r[O_UNNZ] = nnz[p]
+                r[O_URP] = P.add_int(rowptr[p])
+                r[O_UCOLS] = P.add_int(cols[p])
+                r[O_UMERGE] = 1 if p in merged_before else 0
+                merged_before.add(p)
+                if r[O_DENSE] == 0:
+                    tgt, sptr, src = self._moves(n, slot, rowptr, cols, v, p)
+                    r[O_NTGT] = len(tgt)
+                    r[O_TGT] = P.add_int(tgt)
+                    r[O_SPTR] = P.add_int(sptr)
+                    r[O_SRC] = P.add_int(src)
+                else:
+                    r[O_NTGT] = 0
+                self.op_recs.append(r)
+            if last_use.get(v, -2) == i and v != 0:
+                release(v)
+        smem = top
+        x_nnz = 0 if fold else nnz.get(0, 0)
+        rec = np.full(PASS_REC, -1, dtype=np.int32)
+        rec[P_T] = pi.t
+        rec[P_S] = S
+        rec[P_SIDES] = pi.sides
+        rec[P_INIT] = pi.init
+        rec[P_OP0] = op_begin
+        rec[P_NOP] = len(self.op_recs) - op_begin
+        rec[P_TBUF] = bufoff[pi.t]
+        rec[P_XNNZ] = x_nnz
+        rec[P_XBUF] = bufoff.get(0, -1) if not fold else -1
+        if not fold and 0 in pats:
+            rec[P_XRP] = P.add_int(rowptr[0])
+            rec[P_XCOLS] = P.add_int(cols[0])
+        rec[P_NFOLD] = 1 if fold else 0
+        rec[P_SMEM] = smem
+        rec[P_TRP] = P.add_int(rowptr[pi.t])
+        rec[P_TCOLS] = P.add_int(cols[pi.t])
+        rec[P_FINAL] = 1 if pi.final else 0
+        rec[P_NVISIT] = len([v for v in pi.order if v in pats])
+        rec[P_MAXROW] = int(max(np.diff(rowptr[v]).max(initial=0) for v in pats if not (v == 0 and fold)))
+        rec[P_ONEHOT] = 1 if rec[P_MAXROW] <= 1 else 0
+        self.pass_recs.append(rec)
+        # kernel shared memory: per side 7 row arrays (S) + the entry buffers
+        self.max_smem = max(self.max_smem, pi.sides * (7 * S + smem))
+        self.max_S = max(self.max_S, S)
+        pi.bufoff = bufoff
+        pi.fold = fold
+        pi.nnz = nnz
+
+    def _moves(self, n, slot, rowptr, cols, v, p):
+        """Pull lists: for each target entry of input p, the source entries of v."""
+        g = self.g
+        k, a = n.kind, n.attrs
+        S = len(rowptr[v]) - 1
+        rp_u, cols_u = rowptr[p], cols[p]
+        w_in = g[p].width
+        tgt_l, src_l = [], []
+        if k == "reducesum":
+            rmap = a["rmap"]
+            for s in range(S):
+                vc = cols[v][rowptr[v][s]:rowptr[v][s + 1]]
+                if len(vc) == 0:
+                    continue
+                pos_v = {int(c): rowptr[v][s] + j for j, c in enumerate(vc)}
+                for j in range(rp_u[s], rp_u[s + 1]):
+                    o = int(rmap[cols_u[j]])
+                    if o in pos_v:
+                        tgt_l.append(j)
+                        src_l.append([pos_v[o]])
+        else:
+            if k in ("neg", "sqr", "exp", "log", "sin", "cos", "pow"):
+                m = None
+            elif k in ("mulc", "addc", "subc", "rsubc"):
+                m = a["map0"]
+            elif k in ("mul", "add", "sub"):
+                m = a["map0"] if slot == 0 else a["map1"]
+            elif k in MAP_KINDS:
+                m = a["map"]
+            elif k == "concat":
+                off = sum(g[q].width for q in n.inputs[:slot])
+                m = a["cmap"] - off
+            else:
+                raise ProgramError(k)
+            for s in range(S):
+                lo, hi = rowptr[v][s], rowptr[v][s + 1]
+                if lo == hi:
+                    continue
+                vc = cols[v][lo:hi]
+                tc = vc if m is None else m[vc]
+                if k == "concat":
+                    keep = (tc >= 0) & (tc < w_in)
+                else:
+                    keep = np.ones(len(tc), bool)
+                uc = cols_u[rp_u[s]:rp_u[s + 1]]
+                idx = np.searchsorted(uc, tc[keep])
+                tj = rp_u[s] + idx
+                srcs = (lo + np.nonzero(keep)[0])
+                order = np.argsort(tj, kind="stable")
+                tj, srcs = tj[order], srcs[order]
+                uniq, start = np.unique(tj, return_index=True)
+                ends = list(start[1:]) + [len(tj)]
+                for uu, st_, en in zip(uniq, start, ends):
+                    tgt_l.append(int(uu))
+                    src_l.append(list(srcs[st_:en]))
+        tgt = np.array(tgt_l, dtype=np.int64)
+        sptr = np.concatenate([[0], np.cumsum([len(x) for x in src_l])]) if src_l else np.zeros(1, np.int64)
+        src = np.concatenate([np.array(x, dtype=np.int64) for x in src_l]) if src_l else np.zeros(0, np.int64)
+        return tgt, sptr, src
+
+    # ================================================================= info
+    def describe(self) -> str:
+        lines = [f"nodes={len(self.g)} steps={len(self.steps)} passes={len(self.passes)} ops={len(self.op_recs)} "
+                 f"arena={self.arena_w} planes={self.plane_w} fold={self.fold_w} smem_doubles={self.max_smem}"]
+        for pid, pi in enumerate(self.passes):
+            r = self.pass_recs[pid]
+            lines.append(f"  pass {pid}: t={pi.t}({self.g[pi.t].kind}) S={pi.S} sides={pi.sides} final={pi.final} "
+                         f"fold={pi.fold} visits={r[P_NVISIT]} smem={r[P_SMEM]} x_nnz={r[P_XNNZ]} maxrow={r[P_MAXROW]}")
+        return "\n".join(lines)

@@ -1,0 +1,78 @@
+/* gear_b200: C ABI of the B200 (sm_100a) CROWN bound-propagation engine.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and returns an int
+ * status: 0 on success, a negative GEAR_E* code on failure, with a message available from
+ * gear_last_error() (thread-local). No exception crosses the ABI.
+ *
+ * Memory: the caller owns every buffer it passes (x_L, x_U, C, outputs, workspace) and
+ * they must be device memory on the current device; the library never frees them.
+ * A gear_dag handle owns the device copy of its compiled program and is released by
+ * gear_dag_destroy. Calls on one handle from several host threads must be serialised by
+ * the caller; calls on one stream run in stream order.
+ *
+ * Reference interfaces replaced (paths in the reference project):
+ *   gear_dag_create   <- BoundedModule(model, x0, bound_opts)           solver/auto_LiRPA/bound_general.py:87
+ *                        (the DAG arrives compiled by gear_b200/program.py from the same
+ *                        node program; the gear_program seam is bound_general.py:817-829)
+ *   gear_crown_lower  <- BoundedModule.compute_bounds(x=(BoundedTensor(x0,
+ *                        PerturbationLpNorm(x_L, x_U)),), C, method='CROWN',
+ *                        bound_upper=False, return_A=True, needed_A_dict)  bound_general.py:1275
+ *                        as called by get_lower_bound_naive (complete_verifier/input_split/bounding.py:317)
+ */
+#ifndef GEAR_B200_H
+#define GEAR_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GEAR_OK 0
+#define GEAR_E_INVALID (-1)     /* bad argument or malformed program */
+#define GEAR_E_NOMEM (-2)       /* device allocation failed (maps to torch.OutOfMemoryError) */
+#define GEAR_E_TIMEOUT (-3)     /* a bounded device wait expired */
+#define GEAR_E_CUDA (-4)        /* a CUDA runtime error */
+#define GEAR_E_WORKSPACE (-5)   /* workspace smaller than gear_crown_workspace_bytes */
+
+typedef struct gear_dag gear_dag;
+
+/* Upload a compiled program (gear_b200/program.py Program: header, node, step, pass and
+ * op records, int pool, float64 pool) to the current device. */
+int gear_dag_create(const int32_t* header, int64_t header_len,
+                    const int32_t* nodes, int64_t n_nodes_ints,
+                    const int32_t* steps, int64_t n_steps_ints,
+                    const int32_t* passes, int64_t n_passes_ints,
+                    const int32_t* ops, int64_t n_ops_ints,
+                    const int32_t* int_pool, int64_t n_int,
+                    const double* dbl_pool, int64_t n_dbl,
+                    gear_dag** out);
+
+int gear_dag_destroy(gear_dag* dag);
+
+/* Bytes of device workspace gear_crown_lower needs for a batch of `batch` boxes
+ * (bounded by the number of resident CTAs, not by the batch). */
+int64_t gear_crown_workspace_bytes(const gear_dag* dag, int64_t batch);
+
+/* CROWN lower bounds of the DAG's output over `batch` boxes.
+ *   x_L, x_U  (batch, n) float64      box of every subdomain
+ *   C         (batch, S, w_out) float64, or NULL for the identity specification
+ *   lb        (batch, S) float64      lower bound of every specification row
+ *   lA        (batch, S, n) float64 or NULL   A of the bound w.r.t. the input
+ *   lbias     (batch, S) float64 or NULL      bias of that plane (lb minus the
+ *                                            concretised A term)
+ * `stream` is a cudaStream_t (NULL: the legacy default stream). Asynchronous. */
+int gear_crown_lower(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
+                     const double* C, double* lb, double* lA, double* lbias,
+                     void* workspace, int64_t workspace_bytes, void* stream);
+
+/* Number of kernel launches the last gear_crown_lower on this thread issued. */
+int gear_last_launch_count(void);
+
+const char* gear_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GEAR_B200_H */

@@ -250,7 +250,8 @@ class SinRelax:
         # get_intersection(lb, ub, slope, theta = pi/2)
         c = slope
         with np.errstate(invalid="ignore"):
-            cr1 = np.where(c == -1, -PI / 2, np.where(c == 1, PI / 2, np.arcsin(np.clip(c, -1, 1)))) - 0.5 * PI
+            # BoundSin.arcsin: |c| > 1 (a rounded secant slope) gives NaN, no crossing
+            cr1 = np.where(c == -1, -PI / 2, np.where(c == 1, PI / 2, np.arcsin(c))) - 0.5 * PI
         cr2 = PI - cr1 - 2 * 0.5 * PI
         crossings = self._n_crossing(lb, ub, cr1) + self._n_crossing(lb, ub, cr2)
         use_line = crossings == 1
