@@ -501,6 +501,26 @@ __device__ void ibp_node(const Box& bx, int v, double* olo, double* ohi) {
     ibp_linear(bx, nd, olo, ohi);
     return;
   }
+  if (kind == NK_REDUCESUM) {
+    // a warp per output: lanes over the summed inputs
+    const DevProgram* P = bx.P;
+    const int32_t* a = node_rec(P, nd[N_IN0]);
+    const int32_t* inv = P->ip + nd[N_MAP1];
+    const int w = nd[N_W];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int j = warp; j < w; j += NWARP) {
+      double l = 0, h = 0;
+      for (int k = inv[j] + lane; k < inv[j + 1]; k += 32) {
+        int i = inv[w + 1 + k];
+        l += bx.lo[a[N_CUR] + i];
+        h += bx.hi[a[N_CUR] + i];
+      }
+      l = warp_sum(l);
+      h = warp_sum(h);
+      if (lane == 0) { olo[j] = nan_lo(l); ohi[j] = nan_hi(h); }
+    }
+    return;
+  }
   int w = nd[N_W];
   for (int j = threadIdx.x; j < w; j += NT) ibp_element(bx, nd, j, olo + j, ohi + j);
 }
@@ -564,6 +584,12 @@ __device__ void relax_node(const Box& bx, int v) {
   }
 }
 
+#ifdef GEAR_STEP_PROFILE
+// cycles spent per schedule step / pass op, summed over CTAs (measurement builds only)
+__device__ unsigned long long g_step_cycles[8192];
+__device__ unsigned long long g_op_cycles[8192];
+#endif
+
 // ------------------------------------------------------------------ CROWN pass
 // Row arrays in shared memory, per side: bias, bias magnitude, charge, base, dev, berr, undef.
 enum { R_BIAS = 0, R_BMAG, R_CHG, R_BASE, R_DEV, R_BERR, R_UNDEF, R_COUNT };
@@ -572,11 +598,31 @@ struct PassCtx {
   const int32_t* pr;
   int S, sides;
   double* rows;      // [side][R_COUNT][S]
+  double* red;       // RED_SLOTS reduction slots
   double* buf;       // [side][smem]
+  double* la;        // this box's lA block (S x n) when the input's A lives there
+  int32_t* stage_ops;
   int smem;
   __device__ double* row(int side, int what) const { return rows + ((size_t)side * R_COUNT + what) * S; }
-  __device__ double* vals(int side, int off) const { return buf + (size_t)side * smem + off; }
+  __device__ double* vals(int side, int off) const {
+    return off == ROOT_IN_LA ? la : buf + (size_t)side * smem + off;
+  }
 };
+
+// Work split over rows: one thread per row for short rows, one warp per row otherwise.
+struct RowSplit {
+  int first, step, eoff, estep;
+  bool warp;
+};
+__device__ __forceinline__ RowSplit row_split(int maxrow) {
+  RowSplit r;
+  r.warp = maxrow > ROW_THREAD_MAX;
+  r.first = r.warp ? (int)(threadIdx.x >> 5) : (int)threadIdx.x;
+  r.step = r.warp ? NWARP : NT;
+  r.eoff = r.warp ? (int)(threadIdx.x & 31) : 0;
+  r.estep = r.warp ? 32 : 1;
+  return r;
+}
 
 // transformed coefficient for input `slot` of an elementwise op, and its bias term
 __device__ __forceinline__ double elem_coef(int kind, int slot, int side, double a, const double* pl,
@@ -607,7 +653,7 @@ __device__ __forceinline__ double elem_coef(int kind, int slot, int side, double
   }
 }
 
-__device__ void run_pass(const Box& bx, int pid, double* sm, const Work& wk) {
+__device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops, const Work& wk) {
   const DevProgram* P = bx.P;
   const int32_t* pr = P->passes + pid * PASS_REC;
   PassCtx ctx;
@@ -616,10 +662,13 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, const Work& wk) {
   ctx.sides = pr[P_SIDES];
   ctx.smem = pr[P_SMEM];
   ctx.rows = sm;
-  ctx.buf = sm + (size_t)ctx.sides * R_COUNT * ctx.S;
+  ctx.red = sm + (size_t)ctx.sides * R_COUNT * ctx.S;
+  ctx.buf = ctx.red + RED_SLOTS;
+  const bool xdense = pr[P_XDENSE] != 0;
+  ctx.la = xdense ? wk.lA + (size_t)bx.b * ctx.S * P->hdr[H_N] : nullptr;
+  ctx.stage_ops = stage_ops;
   const int S = ctx.S, sides = ctx.sides;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const bool onehot = pr[P_ONEHOT] != 0;
   const int n = P->hdr[H_N];
   const int t = pr[P_T];
   const int32_t* tnd = node_rec(P, t);
@@ -643,8 +692,16 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, const Work& wk) {
   __syncthreads();
 
   const int op0 = pr[P_OP0], nop = pr[P_NOP];
+  // this pass's op records in shared memory (decoded once per box instead of per access)
+  int32_t* sops = ctx.stage_ops;
+  for (int k = tid; k < nop * OP_REC; k += NT) sops[k] = __ldg(P->ops + (size_t)op0 * OP_REC + k);
+  __syncthreads();
+#ifdef GEAR_STEP_PROFILE
+  long long t_op = clock64();
+  extern __device__ unsigned long long g_op_cycles[];
+#endif
   for (int oi = 0; oi < nop; ++oi) {
-    const int32_t* op = P->ops + (op0 + oi) * OP_REC;
+    const int32_t* op = sops + oi * OP_REC;
     const int kind = op[O_KIND], v = op[O_V], slot = op[O_SLOT];
     const int32_t* vnd = node_rec(P, v);
     const int32_t* vrp = P->ip + op[O_VRP];
@@ -654,199 +711,232 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, const Work& wk) {
     const int ppe = kind == NK_MUL ? 6 : 4;
     const int u = op[O_U];
     const int32_t* und = u >= 0 ? node_rec(P, u) : nullptr;
+    const bool first = op[O_FIRST] != 0;
+    const bool zero_u = !op[O_FOLD] && !op[O_UMERGE];
+    const bool u_la = op[O_UBUF] == ROOT_IN_LA;
+    const int uk = op[O_UK];
+    const double gmerge = uk >= 2 ? gamma_k((double)uk) : 0.0;
+    const double* mu = und ? bx.mag + und[N_CUR] : nullptr;
+    const int32_t* urp = (!op[O_FOLD]) ? P->ip + op[O_URP] : nullptr;
+    const int32_t* ucols = (!op[O_FOLD]) ? P->ip + op[O_UCOLS] : nullptr;
+    const bool need_a = first && (relax || kind == NK_MUL || kind == NK_MULC || kind == NK_ADD || kind == NK_SUB ||
+                                  kind == NK_ADDC || kind == NK_SUBC || kind == NK_RSUBC ||
+                                  ((kind == NK_LINEAR) && vnd[N_B_OFF] >= 0));
+    const double* cvec = vnd[N_CVEC] >= 0 ? P->dp + vnd[N_CVEC] : nullptr;
+    const int32_t* map0 = vnd[N_MAP0] >= 0 ? P->ip + vnd[N_MAP0] : nullptr;
+    const int32_t* map1 = vnd[N_MAP1] >= 0 ? P->ip + vnd[N_MAP1] : nullptr;
+    const int32_t* inex = vnd[N_INEXACT] >= 0 ? P->ip + vnd[N_INEXACT] : nullptr;
+    const double* m0 = bx.mag + node_rec(P, vnd[N_IN0])[N_CUR];
+    const double* m1 = (kind == NK_ADD || kind == NK_SUB) ? bx.mag + node_rec(P, vnd[N_IN1])[N_CUR] : nullptr;
+    const double* bvec = (kind == NK_LINEAR && vnd[N_B_OFF] >= 0) ? P->dp + vnd[N_B_OFF] : nullptr;
+    const bool dense = op[O_DENSE] != 0 && !op[O_FOLD];
 
-    // ---- phase A: per-row bias / charges / undefined rows over v's entries
-    if (op[O_FIRST]) {
-      bool need = relax || kind == NK_MUL || kind == NK_MULC || kind == NK_ADD || kind == NK_SUB ||
-                  kind == NK_ADDC || kind == NK_SUBC || kind == NK_RSUBC ||
-                  ((kind == NK_LINEAR) && vnd[N_B_OFF] >= 0);
-      if (need) {
-        const double* cvec = vnd[N_CVEC] >= 0 ? P->dp + vnd[N_CVEC] : nullptr;
-        const int32_t* map0 = vnd[N_MAP0] >= 0 ? P->ip + vnd[N_MAP0] : nullptr;
-        const int32_t* map1 = vnd[N_MAP1] >= 0 ? P->ip + vnd[N_MAP1] : nullptr;
-        const int32_t* inex = vnd[N_INEXACT] >= 0 ? P->ip + vnd[N_INEXACT] : nullptr;
-        const double* m0 = bx.mag + node_rec(P, vnd[N_IN0])[N_CUR];
-        const double* m1 = (kind == NK_ADD || kind == NK_SUB) ? bx.mag + node_rec(P, vnd[N_IN1])[N_CUR] : nullptr;
-        const double* bvec = (kind == NK_LINEAR && vnd[N_B_OFF] >= 0) ? P->dp + vnd[N_B_OFF] : nullptr;
-        for (int side = 0; side < sides; ++side) {
-          const double* V = ctx.vals(side, op[O_VBUF]);
-          double* rb = ctx.row(side, R_BIAS);
-          double* rm = ctx.row(side, R_BMAG);
-          double* rc = ctx.row(side, R_CHG);
-          double* ru = ctx.row(side, R_UNDEF);
-          // one thread per row for one-hot passes, a warp per row otherwise
-          const int rstep = onehot ? NT : NWARP;
-          const int rfirst = onehot ? tid : warp;
-          const int estep = onehot ? 1 : 32;
-          const int eoff = onehot ? 0 : lane;
-          for (int s = rfirst; s < S; s += rstep) {
-            int e0 = vrp[s], e1 = vrp[s + 1];
-            if (e0 == e1) continue;
-            double sb = 0, sm_ = 0, sc = 0;
-            int und_ = 0;
-            for (int e = e0 + eoff; e < e1; e += estep) {
-              double a = V[e];
-              int c = vcols[e];
-              if (relax || kind == NK_MUL) {
-                const double* p = pl + ppe * c;
-                double bt;
-                double na = elem_coef(kind, 0, side, a, p, 0.0, &bt);
-                double bt2 = 0.0, nb = 0.0;
-                if (kind == NK_MUL) nb = elem_coef(kind, 1, side, a, p, 0.0, &bt2);
-                if (a != 0.0 && (!isfinite(bt) || !isfinite(na) || !isfinite(nb))) und_ = 1;
-                if (isfinite(bt)) { sb += bt; sm_ += fabs(bt); }
-              } else if (kind == NK_MULC) {
-                double cv = cvec[c];
-                if (inex[c] && a != 0.0) {
-                  double m = m0[map0[c]];
-                  sc += isinf(m) ? INFINITY : fabs(a * cv) * m;
-                }
-              } else if (kind == NK_LINEAR) {
-                sb += a * bvec[c];
-                sm_ += fabs(a) * fabs(bvec[c]);
-              } else {
-                // add / sub / addc / subc / rsubc: output rounding (interval_bound.py:71-77)
-                double mx = m0[map0[c]];
-                double my = m1 ? m1[map1[c]] : fabs(cvec[c]);
-                double e_ = rounding_error(mx + my, 2);
-                double fa = finite_abs(a);
-                sc += fa > 0 ? (isinf(e_) ? INFINITY : fa * e_) : 0.0;
-                if (kind == NK_ADDC || kind == NK_SUBC || kind == NK_RSUBC) {
-                  double cv = kind == NK_SUBC ? -cvec[c] : cvec[c];
-                  sb += a * cv;
-                  sm_ += fabs(a) * fabs(cv);
-                }
-              }
-            }
-            if (!onehot) { sb = warp_sum(sb); sm_ = warp_sum(sm_); sc = warp_sum(sc); und_ = warp_or(und_); }
-            if (onehot || lane == 0) {
-              rb[s] += sb; rm[s] += sm_;
-              rc[s] += (kind == NK_MULC) ? UNIT * sc : sc;
-              if (und_) ru[s] = 1.0;
-            }
-          }
-        }
-      }
-    }
-
-    // ---- phase B: first contribution into u -> zero its buffer
-    if (!op[O_FOLD] && !op[O_UMERGE]) {
-      int nnz_u = op[O_UNNZ];
-      for (int side = 0; side < sides; ++side) {
-        double* U = ctx.vals(side, op[O_UBUF]);
-        for (int k = tid; k < nnz_u; k += NT) U[k] = 0.0;
-      }
-    }
-    __syncthreads();
-
-    // ---- phase C: contributions into u
-    if (op[O_FOLD]) {
-      // linear/matmul on the input, one entry per row: exact fold into the concretisation
-      const double* f = bx.fold + vnd[N_FOLD];
-      int w = vnd[N_W];
-      double gk = gamma_k((double)op[O_WOUT]);
+    // ---- per-row work of a non-GEMV op: bias/charges over v's row, zero u's row on its first
+    //      contribution, pull the row's moves (or fold it into the concretisation)
+    auto row_body = [&](int s, int eoff, int estep, bool wide) {
+      const int e0 = vrp[s], e1 = vrp[s + 1];
       for (int side = 0; side < sides; ++side) {
         const double* V = ctx.vals(side, op[O_VBUF]);
-        double* rbase = ctx.row(side, R_BASE);
-        double* rdev = ctx.row(side, R_DEV);
-        double* rberr = ctx.row(side, R_BERR);
-        double* rc = ctx.row(side, R_CHG);
-        for (int s = tid; s < S; s += NT) {
-          int e0 = vrp[s], e1 = vrp[s + 1];
-          if (e0 == e1) continue;
-          double a = V[e0];
-          int c = vcols[e0];
-          rbase[s] += a * f[c];
-          rdev[s] += fabs(a) * f[w + c];
-          rberr[s] += fabs(a) * f[2 * w + c];
-          rc[s] += gk * (fabs(a) * f[2 * w + c]);
-        }
-      }
-    } else if (op[O_DENSE]) {
-      // GEMV per row: A_u[s, :] += sum_e A_v[e] W[c_e, :]; charge gamma_k <|A_v||W|, m_u>
-      const int32_t* urp = P->ip + op[O_URP];
-      const double* W = P->dp + vnd[N_W_OFF];
-      int win = vnd[N_WIN];
-      const double* mu = bx.mag + und[N_CUR];
-      double gk = gamma_k((double)op[O_WOUT]);
-      for (int side = 0; side < sides; ++side) {
-        const double* V = ctx.vals(side, op[O_VBUF]);
-        double* U = ctx.vals(side, op[O_UBUF]);
-        double* rc = ctx.row(side, R_CHG);
-        for (int s = warp; s < S; s += NWARP) {
-          int e0 = vrp[s], e1 = vrp[s + 1];
-          if (e0 == e1) continue;
-          double* Ur = U + urp[s];
-          double part = 0;
-          for (int j = lane; j < win; j += 32) {
-            double acc = 0, aabs = 0;
-            for (int e = e0; e < e1; ++e) {
-              double a = V[e];
-              double wv = W[(int64_t)vcols[e] * win + j];
-              acc += a * wv;
-              aabs += fabs(a) * fabs(wv);
-            }
-            Ur[j] += acc;
-            double m = mu[j];
-            part += aabs * (isinf(m) ? 0.0 : m);
-          }
-          part = warp_sum(part);
-          if (lane == 0) rc[s] += gk * part;
-        }
-      }
-    } else {
-      // pull moves: target entry <- sum of transformed source entries
-      const int ntgt = op[O_NTGT];
-      const int32_t* tgt = P->ip + op[O_TGT];
-      const int32_t* sptr = P->ip + op[O_SPTR];
-      const int32_t* src = P->ip + op[O_SRC];
-      const double* cvec = (kind == NK_MULC) ? P->dp + vnd[N_CVEC] : nullptr;
-      for (int side = 0; side < sides; ++side) {
-        const double* V = ctx.vals(side, op[O_VBUF]);
-        double* U = ctx.vals(side, op[O_UBUF]);
-        for (int k = tid; k < ntgt; k += NT) {
-          double acc = 0;
-          for (int q = sptr[k]; q < sptr[k + 1]; ++q) {
-            int e = src[q];
+        if (need_a && e0 < e1) {
+          double sb = 0, sm_ = 0, sc = 0;
+          int und_ = 0;
+          for (int e = e0 + eoff; e < e1; e += estep) {
             double a = V[e];
             int c = vcols[e];
+            if (relax || kind == NK_MUL) {
+              const double* p = pl + ppe * c;
+              double bt;
+              double na = elem_coef(kind, 0, side, a, p, 0.0, &bt);
+              double bt2 = 0.0, nb = 0.0;
+              if (kind == NK_MUL) nb = elem_coef(kind, 1, side, a, p, 0.0, &bt2);
+              if (a != 0.0 && (!isfinite(bt) || !isfinite(na) || !isfinite(nb))) und_ = 1;
+              if (isfinite(bt)) { sb += bt; sm_ += fabs(bt); }
+            } else if (kind == NK_MULC) {
+              double cv = cvec[c];
+              if (inex[c] && a != 0.0) {
+                double m = m0[map0[c]];
+                sc += isinf(m) ? INFINITY : UNIT * (fabs(a * cv) * m);
+              }
+            } else if (kind == NK_LINEAR) {
+              // bias of a folded Linear: A_v . b
+              sb += a * bvec[c];
+              sm_ += fabs(a) * fabs(bvec[c]);
+            } else {
+              // add / sub / addc / subc / rsubc: output rounding (interval_bound.py:71-77)
+              double mx = m0[map0[c]];
+              double my = m1 ? m1[map1[c]] : fabs(cvec[c]);
+              double e_ = rounding_error(mx + my, 2);
+              double fa = finite_abs(a);
+              sc += fa > 0 ? (isinf(e_) ? INFINITY : fa * e_) : 0.0;
+              if (kind == NK_ADDC || kind == NK_SUBC || kind == NK_RSUBC) {
+                double cv = kind == NK_SUBC ? -cvec[c] : cvec[c];
+                sb += a * cv;
+                sm_ += fabs(a) * fabs(cv);
+              }
+            }
+          }
+          if (wide) { sb = warp_sum(sb); sm_ = warp_sum(sm_); sc = warp_sum(sc); und_ = warp_or(und_); }
+          if (!wide || lane == 0) {
+            ctx.row(side, R_BIAS)[s] += sb;
+            ctx.row(side, R_BMAG)[s] += sm_;
+            ctx.row(side, R_CHG)[s] += sc;
+            if (und_) ctx.row(side, R_UNDEF)[s] = 1.0;
+          }
+        }
+        if (op[O_FOLD]) {
+          // linear/matmul on the input, one entry per row: exact fold into the concretisation
+          if (e0 < e1 && (!wide || lane == 0)) {
+            const double* f = bx.fold + vnd[N_FOLD];
+            const int w = vnd[N_W];
+            const double gk = gamma_k((double)op[O_WOUT]);
+            double a = V[e0];
+            int c = vcols[e0];
+            ctx.row(side, R_BASE)[s] += a * f[c];
+            ctx.row(side, R_DEV)[s] += fabs(a) * f[w + c];
+            ctx.row(side, R_BERR)[s] += fabs(a) * f[2 * w + c];
+            ctx.row(side, R_CHG)[s] += gk * (fabs(a) * f[2 * w + c]);
+          }
+          continue;
+        }
+        double* U = ctx.vals(side, op[O_UBUF]);
+        if (zero_u) {
+          if (u_la) for (int j = eoff; j < n; j += estep) U[(size_t)s * n + j] = 0.0;
+          else for (int j = urp[s] + eoff; j < urp[s + 1]; j += estep) U[j] = 0.0;
+          if (wide) __syncwarp();
+        }
+        const int32_t* tptr = P->ip + op[O_TPTR];
+        const int k0 = tptr[s], k1 = tptr[s + 1];
+        if (k0 == k1) continue;
+        const int32_t* tgt = P->ip + op[O_TGT];
+        const int32_t* sptr = P->ip + op[O_SPTR];
+        const int32_t* src = P->ip + op[O_SRC];
+        double pmerge = 0;
+        const bool single = op[O_SINGLE] != 0;
+        for (int k = k0 + eoff; k < k1; k += estep) {
+          double acc = 0;
+          const int q0 = single ? k : __ldg(sptr + k), q1 = single ? k + 1 : __ldg(sptr + k + 1);
+          for (int q = q0; q < q1; ++q) {
+            int e = __ldg(src + q);
+            double a = V[e];
+            int c = __ldg(vcols + e);
             double bt;
-            double na = elem_coef(kind, slot, side, a, pl ? pl + ppe * c : nullptr, cvec ? cvec[c] : 0.0, &bt);
+            double na = elem_coef(kind, slot, side, a, pl ? pl + ppe * c : nullptr, cvec ? __ldg(cvec + c) : 0.0, &bt);
             if (!isfinite(na)) na = 0.0;
             acc += na;
           }
-          U[tgt[k]] += acc;
+          int ti = tgt[k];
+          U[ti] += acc;
+          if (uk >= 2 && acc != 0.0) {
+            int col = u_la ? ti - s * n : ucols[ti];
+            double m = mu[col];
+            pmerge += isinf(m) ? INFINITY : fabs(acc) * m;
+          }
+        }
+        if (uk >= 2) {
+          if (wide) pmerge = warp_sum(pmerge);
+          if (!wide || lane == 0) ctx.row(side, R_CHG)[s] += gmerge * pmerge;
+        }
+      }
+    };
+
+    if (!dense) {
+      const int32_t* shortr = P->ip + op[O_SHORT];
+      const int32_t* longr = P->ip + op[O_LONG];
+      const int nshort = op[O_NSHORT], nlong = op[O_NLONG];
+      for (int i = tid; i < nshort; i += NT) row_body(shortr[i], 0, 1, false);
+      for (int i = warp; i < nlong; i += NWARP) row_body(longr[i], lane, 32, true);
+    } else {
+      // ---- GEMV: A_u[s, :] (+)= sum_e A_v[e] W[c_e, :]; charges gamma_w <|A_v||W|, m_u> and merges
+      const bool block_rows = op[O_VROWS] < NWARP;   // few rows: the whole CTA on each row
+      const int s0 = block_rows ? 0 : warp, sstep = block_rows ? 1 : NWARP;
+      const int eoff = block_rows ? tid : lane, estep = block_rows ? NT : 32;
+      const double* W = P->dp + vnd[N_W_OFF];
+      const int win = vnd[N_WIN];
+      const double gk = gamma_k((double)op[O_WOUT]);
+      for (int s = s0; s < S; s += sstep) {
+        const int e0 = vrp[s], e1 = vrp[s + 1];
+        for (int side = 0; side < sides; ++side) {
+          const double* V = ctx.vals(side, op[O_VBUF]);
+          double* U = ctx.vals(side, op[O_UBUF]);
+          double* Ur = u_la ? U + (size_t)s * n : U + urp[s];
+          const int urow = u_la ? n : urp[s + 1] - urp[s];
+          if (need_a && e0 < e1) {
+            // Linear bias A_v . b
+            double sb = 0, sm_ = 0;
+            for (int e = e0 + eoff; e < e1; e += estep) {
+              double a = V[e];
+              sb += a * bvec[vcols[e]];
+              sm_ += fabs(a) * fabs(bvec[vcols[e]]);
+            }
+            sb = warp_sum(sb); sm_ = warp_sum(sm_);
+            if (block_rows) {
+              if (lane == 0) { ctx.red[warp] = sb; ctx.red[NWARP + warp] = sm_; }
+              __syncthreads();
+              if (tid == 0) {
+                double tb = 0, tm = 0;
+                for (int w_ = 0; w_ < NWARP; ++w_) { tb += ctx.red[w_]; tm += ctx.red[NWARP + w_]; }
+                ctx.row(side, R_BIAS)[s] += tb;
+                ctx.row(side, R_BMAG)[s] += tm;
+              }
+              __syncthreads();
+            } else if (lane == 0) {
+              ctx.row(side, R_BIAS)[s] += sb;
+              ctx.row(side, R_BMAG)[s] += sm_;
+            }
+          }
+          if (e0 == e1) {
+            if (zero_u) for (int j = eoff; j < urow; j += estep) Ur[j] = 0.0;
+            continue;
+          }
+          double part = 0, pmerge = 0;
+          for (int j = eoff; j < win; j += estep) {
+            double acc0 = 0, acc1 = 0, ab0 = 0, ab1 = 0;
+            int e = e0;
+            for (; e + 1 < e1; e += 2) {
+              double a0 = V[e], a1 = V[e + 1];
+              double w0 = W[(int64_t)vcols[e] * win + j], w1 = W[(int64_t)vcols[e + 1] * win + j];
+              acc0 += a0 * w0; acc1 += a1 * w1;
+              ab0 += fabs(a0) * fabs(w0); ab1 += fabs(a1) * fabs(w1);
+            }
+            if (e < e1) {
+              double a0 = V[e], w0 = W[(int64_t)vcols[e] * win + j];
+              acc0 += a0 * w0; ab0 += fabs(a0) * fabs(w0);
+            }
+            double acc = acc0 + acc1;
+            Ur[j] = zero_u ? acc : Ur[j] + acc;
+            double m = mu[j];
+            double mf = isinf(m) ? 0.0 : m;
+            part += (ab0 + ab1) * mf;
+            pmerge += fabs(acc) * mf;
+          }
+          double tot_ = gk * warp_sum(part) + gmerge * warp_sum(pmerge);
+          if (block_rows) {
+            if (lane == 0) ctx.red[warp] = tot_;
+            __syncthreads();
+            if (tid == 0) {
+              double t_ = 0;
+              for (int w_ = 0; w_ < NWARP; ++w_) t_ += ctx.red[w_];
+              ctx.row(side, R_CHG)[s] += t_;
+            }
+            __syncthreads();
+          } else if (lane == 0) {
+            ctx.row(side, R_CHG)[s] += tot_;
+          }
         }
       }
     }
     __syncthreads();
-
-    // ---- phase D: merge charge u <|A_u|, m_u> (A_u = old + new)
-    if (!op[O_FOLD] && op[O_UMERGE]) {
-      const int32_t* urp = P->ip + op[O_URP];
-      const int32_t* ucols = P->ip + op[O_UCOLS];
-      const double* mu = bx.mag + und[N_CUR];
-      for (int side = 0; side < sides; ++side) {
-        const double* U = ctx.vals(side, op[O_UBUF]);
-        double* rc = ctx.row(side, R_CHG);
-        for (int s = warp; s < S; s += NWARP) {
-          int e0 = urp[s], e1 = urp[s + 1];
-          double part = 0;
-          int hit = 0;
-          for (int e = e0 + lane; e < e1; e += 32) {
-            double a = fabs(U[e]);
-            double m = mu[ucols[e]];
-            if (isinf(m)) { if (a > 0) hit = 1; }
-            else part += a * m;
-          }
-          part = warp_sum(part);
-          hit = warp_or(hit);
-          if (lane == 0 && e1 > e0) rc[s] += hit ? INFINITY : UNIT * part;
-        }
-      }
-      __syncthreads();
+#ifdef GEAR_STEP_PROFILE
+    if (tid == 0) {
+      long long t1 = clock64();
+      atomicAdd(&g_op_cycles[op0 + oi], (unsigned long long)(t1 - t_op));
+      t_op = t1;
     }
+#endif
   }
+#ifdef GEAR_STEP_PROFILE
+  if (tid == 0) t_op = clock64();
+#endif
 
   // ---- concretisation at the input and outputs
   const bool fold = pr[P_NFOLD] != 0;
@@ -854,28 +944,32 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, const Work& wk) {
   const int32_t* xrp = (!fold && xnnz > 0) ? P->ip + pr[P_XRP] : nullptr;
   const int32_t* xcols = (!fold && xnnz > 0) ? P->ip + pr[P_XCOLS] : nullptr;
   if (xrp) {
+    const RowSplit rs = row_split(pr[P_XMAXROW]);
     for (int side = 0; side < sides; ++side) {
       const double* V = ctx.vals(side, pr[P_XBUF]);
       double* rbase = ctx.row(side, R_BASE);
       double* rdev = ctx.row(side, R_DEV);
       double* rberr = ctx.row(side, R_BERR);
-      for (int s = warp; s < S; s += NWARP) {
+      for (int s = rs.first; s < S; s += rs.step) {
         int e0 = xrp[s], e1 = xrp[s + 1];
         double bs = 0, dv = 0, be = 0;
-        for (int e = e0 + lane; e < e1; e += 32) {
-          double a = V[e];
+        for (int e = e0 + rs.eoff; e < e1; e += rs.estep) {
           int c = xcols[e];
+          double a = xdense ? V[(size_t)s * n + c] : V[e];
           double l = bx.xL[c], h = bx.xU[c];
           bs += a * ((h + l) / 2.0);
           dv += fabs(a) * ((h - l) / 2.0);
           be += finite_abs(a) * finite_abs(fmax(fabs(l), fabs(h)));
         }
-        bs = warp_sum(bs); dv = warp_sum(dv); be = warp_sum(be);
-        if (lane == 0) { rbase[s] += bs; rdev[s] += dv; rberr[s] += be; }
+        if (rs.warp) { bs = warp_sum(bs); dv = warp_sum(dv); be = warp_sum(be); }
+        if (!rs.warp || lane == 0) { rbase[s] += bs; rdev[s] += dv; rberr[s] += be; }
       }
     }
   }
   __syncthreads();
+#ifdef GEAR_STEP_PROFILE
+  if (tid == 0) atomicAdd(&g_op_cycles[8190], (unsigned long long)(clock64() - t_op));
+#endif
   const double nvisit = (double)max(pr[P_NVISIT], 1);
   const bool final = pr[P_FINAL] != 0;
   for (int side = 0; side < sides; ++side) {
@@ -914,7 +1008,13 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, const Work& wk) {
       }
     }
   }
-  if (final && wk.lA) {
+  if (final && wk.lA && xdense) {
+    // the input's A was accumulated in place; rows of undefined bounds become zero
+    for (int s = warp; s < S; s += NWARP) {
+      if (ctx.row(0, R_UNDEF)[s] == 0.0) continue;
+      for (int c = lane; c < n; c += 32) ctx.la[(size_t)s * n + c] = 0.0;
+    }
+  } else if (final && wk.lA) {
     // dense lA rows: zero, then the input's entries (rows of undefined bounds stay zero)
     double* lA = wk.lA + (size_t)bx.b * S * n;
     for (int k = tid; k < S * n; k += NT) lA[k] = 0.0;
@@ -930,7 +1030,9 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, const Work& wk) {
   __syncthreads();
 }
 
-__device__ void compare_node(const Box& bx, int v, double* tmp_lo, double* tmp_hi) {
+__device__ __forceinline__ double magnitude(double l, double h) { return l > h ? INFINITY : fmax(-l, h); }
+
+__device__ void compare_node(const Box& bx, int v, double* tmp_lo, double* tmp_hi, bool with_mag) {
   // IBP of v from its inputs' current intervals, intersected with the pass result
   const int32_t* nd = node_rec(bx.P, v);
   int w = nd[N_W];
@@ -938,14 +1040,25 @@ __device__ void compare_node(const Box& bx, int v, double* tmp_lo, double* tmp_h
   __syncthreads();
   for (int j = threadIdx.x; j < w; j += NT) {
     double l = nan_lo(bx.pres_lo[j]), h = nan_hi(bx.pres_hi[j]);
-    bx.lo[nd[N_CUR] + j] = fmax(l, tmp_lo[j]);
-    bx.hi[nd[N_CUR] + j] = fmin(h, tmp_hi[j]);
+    double lo_ = fmax(l, tmp_lo[j]), hi_ = fmin(h, tmp_hi[j]);
+    bx.lo[nd[N_CUR] + j] = lo_;
+    bx.hi[nd[N_CUR] + j] = hi_;
+    if (with_mag) bx.mag[nd[N_CUR] + j] = magnitude(lo_, hi_);
   }
 }
 
-__global__ void __launch_bounds__(NT) crown_megakernel(DevProgram P, Work wk) {
+
+__global__ void __launch_bounds__(NT, 3) crown_megakernel(DevProgram Pg, Work wk) {
   extern __shared__ double sm[];
-  const int32_t* hdr = P.hdr;
+  const int32_t* hdr = Pg.hdr;
+  // shared memory: [pass working set | node table | op records of the running pass]
+  const int pass_doubles = hdr[H_SMEM] - ((hdr[H_NNODES] * NODE_REC + hdr[H_MAXOPS] * OP_REC + 1) / 2 + 2);
+  int32_t* snodes = reinterpret_cast<int32_t*>(sm + pass_doubles);
+  int32_t* sops = snodes + hdr[H_NNODES] * NODE_REC;
+  for (int k = threadIdx.x; k < hdr[H_NNODES] * NODE_REC; k += NT) snodes[k] = __ldg(Pg.nodes + k);
+  __syncthreads();
+  DevProgram P = Pg;
+  P.nodes = snodes;
   const int arena = hdr[H_ARENA], planes_w = hdr[H_PLANES], fold_w = hdr[H_FOLDW], maxw = hdr[H_MAXW];
   const int n = hdr[H_N];
   double* slot = wk.scratch + (size_t)blockIdx.x * wk.slot_doubles;
@@ -968,6 +1081,9 @@ __global__ void __launch_bounds__(NT) crown_megakernel(DevProgram P, Work wk) {
     for (int j = threadIdx.x; j < n; j += NT) { bx.lo[j] = bx.xL[j]; bx.hi[j] = bx.xU[j]; }
     __syncthreads();
     for (int si = 0; si < nsteps; ++si) {
+#ifdef GEAR_STEP_PROFILE
+      long long t_step = clock64();
+#endif
       const int32_t* st = P.steps + si * STEP_REC;
       const int type = st[0], a = st[1];
       switch (type) {
@@ -976,26 +1092,30 @@ __global__ void __launch_bounds__(NT) crown_megakernel(DevProgram P, Work wk) {
           const int32_t* nd = node_rec(&P, a);
           ibp_node(bx, a, tmp_lo, tmp_hi);
           __syncthreads();
+          const bool with_mag = st[2] != 0;
           for (int j = threadIdx.x; j < nd[N_W]; j += NT) {
             bx.lo[nd[N_CUR] + j] = tmp_lo[j];
             bx.hi[nd[N_CUR] + j] = tmp_hi[j];
+            if (with_mag) bx.mag[nd[N_CUR] + j] = magnitude(tmp_lo[j], tmp_hi[j]);
           }
           break;
         }
         case ST_MAG: {
           const int32_t* nd = node_rec(&P, a);
           for (int j = threadIdx.x; j < nd[N_W]; j += NT) {
-            double l = bx.lo[nd[N_CUR] + j], h = bx.hi[nd[N_CUR] + j];
-            bx.mag[nd[N_CUR] + j] = l > h ? INFINITY : fmax(-l, h);
+            bx.mag[nd[N_CUR] + j] = magnitude(bx.lo[nd[N_CUR] + j], bx.hi[nd[N_CUR] + j]);
           }
           break;
         }
         case ST_RELAX: relax_node(bx, a); break;
-        case ST_PASS: case ST_FINAL: run_pass(bx, a, sm, wk); break;
-        case ST_COMPARE: compare_node(bx, a, tmp_lo, tmp_hi); break;
+        case ST_PASS: case ST_FINAL: run_pass(bx, a, sm, sops, wk); break;
+        case ST_COMPARE: compare_node(bx, a, tmp_lo, tmp_hi, st[3] != 0); break;
         default: break;
       }
       __syncthreads();
+#ifdef GEAR_STEP_PROFILE
+      if (threadIdx.x == 0 && si < 8192) atomicAdd(&g_step_cycles[si], (unsigned long long)(clock64() - t_step));
+#endif
     }
   }
 }

@@ -134,6 +134,8 @@ extern "C" int gear_crown_lower(const gear_dag* dag, const double* x_L, const do
   if (!workspace || workspace_bytes < gear_crown_workspace_bytes(dag, batch))
     return fail(GEAR_E_WORKSPACE, "gear_crown_lower: %s", "workspace too small");
   if (dag->hdr[gear::H_RETA] == 0 && lA) return fail(GEAR_E_INVALID, "gear_crown_lower: %s", "program built without A");
+  if (dag->hdr[gear::H_RETA] != 0 && !lA)
+    return fail(GEAR_E_INVALID, "gear_crown_lower: %s", "this program accumulates A in the lA output: lA is required");
   gear::Work wk;
   wk.xL = x_L;
   wk.xU = x_U;
@@ -156,3 +158,20 @@ extern "C" int gear_crown_lower(const gear_dag* dag, const double* x_L, const do
   if (e != cudaSuccess) return cuda_fail(e, "crown_megakernel launch");
   return GEAR_OK;
 }
+
+#ifdef GEAR_STEP_PROFILE
+extern "C" int gear_profile_read(unsigned long long* out, int n) {
+  cudaError_t e = cudaMemcpyFromSymbol(out, gear::g_step_cycles, sizeof(unsigned long long) * n);
+  return e == cudaSuccess ? 0 : -4;
+}
+extern "C" int gear_profile_reset(void) {
+  static unsigned long long zeros[8192];
+  cudaError_t e = cudaMemcpyToSymbol(gear::g_step_cycles, zeros, sizeof(zeros));
+  if (e == cudaSuccess) e = cudaMemcpyToSymbol(gear::g_op_cycles, zeros, sizeof(zeros));
+  return e == cudaSuccess ? 0 : -4;
+}
+extern "C" int gear_profile_read_ops(unsigned long long* out, int n) {
+  cudaError_t e = cudaMemcpyFromSymbol(out, gear::g_op_cycles, sizeof(unsigned long long) * n);
+  return e == cudaSuccess ? 0 : -4;
+}
+#endif

@@ -21,17 +21,25 @@ constexpr int STEP_REC = 4;
 
 enum PassField {
   P_T = 0, P_S, P_SIDES, P_INIT, P_OP0, P_NOP, P_TBUF, P_XNNZ, P_XBUF, P_XRP, P_XCOLS, P_NFOLD,
-  P_SMEM, P_TRP, P_TCOLS, P_FINAL, P_NVISIT, P_MAXROW, P_ONEHOT, PASS_REC = 24
+  P_SMEM, P_TRP, P_TCOLS, P_FINAL, P_NVISIT, P_MAXROW, P_ONEHOT, P_XMAXROW, P_XDENSE, P_TMAXROW,
+  PASS_REC = 24
 };
 
 enum OpField {
   O_KIND = 0, O_V, O_SLOT, O_FIRST, O_VBUF, O_VNNZ, O_VRP, O_VCOLS, O_U, O_UBUF, O_UNNZ, O_URP,
-  O_UCOLS, O_UMERGE, O_NTGT, O_TGT, O_SPTR, O_SRC, O_DENSE, O_FOLD, O_WOUT, OP_REC = 24
+  O_UCOLS, O_UMERGE, O_NTGT, O_TGT, O_SPTR, O_SRC, O_DENSE, O_FOLD, O_WOUT, O_VMAXROW, O_UMAXROW, O_VROWS,
+  O_TPTR, O_UK, O_TMAXROW, O_SHORT, O_NSHORT, O_LONG, O_NLONG, O_SINGLE, OP_REC = 32
 };
+// buffer offset marker: the input's A of a final pass accumulates in the lA output (row s at s * n)
+constexpr int ROOT_IN_LA = -2;
+// rows with at most this many entries are handled by one thread, longer rows by a warp
+constexpr int ROW_THREAD_MAX = 4;
+// shared-memory reduction slots reserved after the row arrays
+constexpr int RED_SLOTS = 32;
 
 enum HeaderField {
   H_NNODES = 0, H_NSTEPS, H_NPASSES, H_NOPS, H_N, H_S, H_T, H_ARENA, H_PLANES, H_FOLDW,
-  H_SMEM, H_MAXS, H_SINOFF, H_MAXW, H_RETA, H_R15, HEADER_LEN = 16
+  H_SMEM, H_MAXS, H_SINOFF, H_MAXW, H_RETA, H_MAXOPS, HEADER_LEN = 16
 };
 
 // Sin/cos table layout inside the float64 pool, from H_SINOFF (gear_b200/tables.py order).

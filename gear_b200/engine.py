@@ -70,7 +70,7 @@ class CrownEngine:
             C = C.to(torch.float64).contiguous()
         if out is None:
             lb = torch.empty(B, self.S, dtype=torch.float64, device=dev)
-            lA = torch.empty(B, self.S, self.n, dtype=torch.float64, device=dev) if return_A else None
+            lA = torch.empty(B, self.S, self.n, dtype=torch.float64, device=dev)
             lbias = torch.empty(B, self.S, dtype=torch.float64, device=dev)
         else:
             lb, lA, lbias = out
@@ -78,7 +78,7 @@ class CrownEngine:
         stream = torch.cuda.current_stream(dev).cuda_stream
         st = _lib.lib().gear_crown_lower(self.handle, x_L.data_ptr(), x_U.data_ptr(), B,
                                          C.data_ptr() if self.dense_c else None,
-                                         lb.data_ptr(), lA.data_ptr() if lA is not None else None,
+                                         lb.data_ptr(), lA.data_ptr(),
                                          lbias.data_ptr(), ws.data_ptr(), ws.numel(), stream)
         _lib.check(st, "gear_crown_lower")
-        return lb, lA, lbias
+        return lb, (lA if return_A else None), lbias

@@ -52,11 +52,14 @@ STEP_REC = 4
 
 PASS_REC = 24
 (P_T, P_S, P_SIDES, P_INIT, P_OP0, P_NOP, P_TBUF, P_XNNZ, P_XBUF, P_XRP, P_XCOLS, P_NFOLD,
- P_SMEM, P_TRP, P_TCOLS, P_FINAL, P_NVISIT, P_MAXROW, P_ONEHOT, P_R19, P_R20, P_R21, P_R22, P_R23) = range(24)
+ P_SMEM, P_TRP, P_TCOLS, P_FINAL, P_NVISIT, P_MAXROW, P_ONEHOT, P_XMAXROW, P_XDENSE, P_TMAXROW, P_R22, P_R23) = range(24)
 
-OP_REC = 24
+OP_REC = 32
 (O_KIND, O_V, O_SLOT, O_FIRST, O_VBUF, O_VNNZ, O_VRP, O_VCOLS, O_U, O_UBUF, O_UNNZ, O_URP,
- O_UCOLS, O_UMERGE, O_NTGT, O_TGT, O_SPTR, O_SRC, O_DENSE, O_FOLD, O_WOUT, O_R21, O_R22, O_R23) = range(24)
+ O_UCOLS, O_UMERGE, O_NTGT, O_TGT, O_SPTR, O_SRC, O_DENSE, O_FOLD, O_WOUT, O_VMAXROW, O_UMAXROW, O_VROWS,
+ O_TPTR, O_UK, O_TMAXROW, O_SHORT, O_NSHORT, O_LONG, O_NLONG, O_SINGLE) = range(32)
+ROW_THREAD_MAX = 4   # rows with at most this much work run on one thread, longer rows on a warp
+ROOT_IN_LA = -2     # buffer marker: the input's A of a final pass accumulates in the lA output
 
 PLANES_PER_ELEM = {"mul": 6, "sqr": 4, "exp": 4, "log": 4, "sin": 4, "cos": 4, "pow": 4}
 
@@ -183,10 +186,9 @@ class Program:
         for v in sorted(self.fold_off):
             self.steps.append((ST["fold"], v, 0, 0))
         # plain IBP of every node: magnitudes of nodes without stored bounds
+        self.steps.append((ST["mag"], 0, 0, 0))
         for nd in g.nodes[1:]:
-            self.steps.append((ST["ibp"], nd.id, 0, 0))
-        for nd in g.nodes:
-            self.steps.append((ST["mag"], nd.id, 0, 0))
+            self.steps.append((ST["ibp"], nd.id, 1, 0))      # b = 1: also write the magnitude
         self.relaxed = set()
         self._check_prior(self.t, final=True)
         # interval of the final node for the undefined-row fallback
@@ -219,8 +221,7 @@ class Program:
         for p in g[v].inputs:
             if p not in self.stored:
                 self._store_ibp(p)
-        self.steps.append((ST["ibp"], v, 0, 0))
-        self.steps.append((ST["mag"], v, 0, 0))
+        self.steps.append((ST["ibp"], v, 1, 0))
         self.stored.add(v)
         self.log.append(("ibp", v))
 
@@ -239,8 +240,7 @@ class Program:
             return
         n = g[v]
         if n.kind == "reshape" and n.inputs[0] in self.stored:
-            self.steps.append((ST["ibp"], v, 0, 0))
-            self.steps.append((ST["mag"], v, 0, 0))
+            self.steps.append((ST["ibp"], v, 1, 0))
             self.stored.add(v)
             self.log.append(("ibp", v))
             return
@@ -262,8 +262,7 @@ class Program:
         pid = self._add_pass(v, n.width, sides=2, final=False, init=0)
         self.steps.append((ST["pass"], pid, 0, 0))
         self._transient_ibp(v, set())
-        self.steps.append((ST["compare"], v, pid, 0))
-        self.steps.append((ST["mag"], v, 0, 0))
+        self.steps.append((ST["compare"], v, pid, 1))      # c = 1: also write the magnitude
         self.stored.add(v)
         self.log.append(("crown", v))
 
@@ -429,10 +428,14 @@ class Program:
         self.op_arr = np.stack(self.op_recs).reshape(-1) if self.op_recs else np.zeros(0, np.int32)
         self.int_pool = self.pools.int_array()
         self.dbl_pool = self.pools.dbl_array()
+        max_ops = max((int(r[P_NOP]) for r in self.pass_recs), default=0)
+        # shared memory: pass working set + staged node table + staged op records (in doubles)
+        stage = (len(self.g) * NODE_REC + max_ops * OP_REC + 1) // 2 + 2
+        self.smem_total = self.max_smem + stage
         self.header = np.array([len(self.g), len(self.steps), len(self.passes), len(self.op_recs),
                                 self.n, self.S, self.t, self.arena_w, self.plane_w, self.fold_w,
-                                self.max_smem, self.max_S, self.sin_off, self.maxw,
-                                1 if self.return_a else 0, 0], dtype=np.int32)
+                                self.smem_total, self.max_S, self.sin_off, self.maxw,
+                                1 if self.return_a else 0, max_ops], dtype=np.int32)
 
     def _emit_pass(self, pid, pi: PassInfo):
         g = self.g
@@ -449,7 +452,7 @@ class Program:
         # fold decision: root contributions only from linear/matmul-on-input ops with
         # at most one entry per row, in a non-final pass
         contributors = [v for v in pi.order if 0 in g[v].inputs and v in pats]
-        fold = (not pi.final and len(contributors) > 0 and
+        fold = (not pi.final and len(contributors) == 1 and
                 all(g[v].kind in ("linear", "matmul") and v in self.fold_off and
                     np.diff(rowptr[v]).max(initial=0) <= 1 for v in contributors))
         # liveness-based buffer allocation (doubles per side)
@@ -460,6 +463,7 @@ class Program:
             for p in g[v].inputs:
                 if p not in first_use:
                     first_use[p] = i
+        xdense = pi.final and self.return_a and not fold and 0 in pats
         if not fold:
             last_use[0] = len(pi.order)
         free, bufoff, top = [], {}, 0
@@ -483,6 +487,17 @@ class Program:
 
         bufoff[pi.t] = alloc(pi.t)
         op_begin = len(self.op_recs)
+        pat_off = {}
+
+        def pattern(v_):
+            if v_ not in pat_off:
+                pat_off[v_] = (P.add_int(rowptr[v_]), P.add_int(cols[v_]))
+            return pat_off[v_]
+        kcount = {}
+        for v in pi.order:
+            if v in pats:
+                for p in g[v].inputs:
+                    kcount[p] = kcount.get(p, 0) + 1
         merged_before = {pi.t}
         for i, v in enumerate(pi.order):
             n = g[v]
@@ -490,6 +505,9 @@ class Program:
                 continue
             for slot, p in enumerate(n.inputs):
                 if p == 0 and fold:
+                    continue
+                if p == 0 and xdense:
+                    bufoff[0] = ROOT_IN_LA
                     continue
                 if p not in bufoff and p in pats:
                     bufoff[p] = alloc(p)
@@ -503,34 +521,67 @@ class Program:
                 r[O_FIRST] = 1 if slot == 0 else 0
                 r[O_VBUF] = bufoff[v]
                 r[O_VNNZ] = nnz[v]
-                r[O_VRP] = P.add_int(rowptr[v])
-                r[O_VCOLS] = P.add_int(cols[v])
+                r[O_VRP], r[O_VCOLS] = pattern(v)
                 r[O_U] = p
                 r[O_WOUT] = n.width
                 r[O_DENSE] = 1 if k in ("linear", "matmul") else 0
                 r[O_FOLD] = 1 if (p == 0 and fold) else 0
+                r[O_VMAXROW] = int(np.diff(rowptr[v]).max(initial=0))
+                r[O_VROWS] = int((np.diff(rowptr[v]) > 0).sum())
                 if r[O_FOLD] == 1:
                     r[O_UBUF] = -1
                     r[O_UNNZ] = 0
                     r[O_UMERGE] = 0
+                    rows = np.nonzero(np.diff(rowptr[v]) > 0)[0]
+                    r[O_SHORT] = P.add_int(rows)
+                    r[O_NSHORT] = len(rows)
+                    r[O_LONG] = P.add_int(np.zeros(0, np.int64))
+                    r[O_NLONG] = 0
                     self.op_recs.append(r)
                     continue
                 r[O_UBUF] = bufoff[p]
                 r[O_UNNZ] = nnz[p]
-                r[O_URP] = P.add_int(rowptr[p])
-                r[O_UCOLS] = P.add_int(cols[p])
+                r[O_URP], r[O_UCOLS] = pattern(p)
                 r[O_UMERGE] = 1 if p in merged_before else 0
                 merged_before.add(p)
+                r[O_UK] = kcount.get(p, 1)
+                r[O_VMAXROW] = int(np.diff(rowptr[v]).max(initial=0))
+                r[O_UMAXROW] = int(np.diff(rowptr[p]).max(initial=0))
+                r[O_VROWS] = int((np.diff(rowptr[v]) > 0).sum())
                 if r[O_DENSE] == 0:
                     tgt, sptr, src = self._moves(n, slot, rowptr, cols, v, p)
+                    rows_of = np.repeat(np.arange(S), np.diff(rowptr[p]))
+                    trow = rows_of[tgt] if len(tgt) else np.zeros(0, np.int64)
+                    tptr = np.searchsorted(trow, np.arange(S + 1), side="left")
+                    r[O_TPTR] = P.add_int(tptr)
+                    r[O_TMAXROW] = int(np.diff(tptr).max(initial=0))
+                    if p == 0 and xdense:
+                        # entry (s, c) of the input's A lives at lA[s * n + c]
+                        tgt = trow * self.n + cols[0][tgt]
                     r[O_NTGT] = len(tgt)
                     r[O_TGT] = P.add_int(tgt)
                     r[O_SPTR] = P.add_int(sptr)
                     r[O_SRC] = P.add_int(src)
+                    # every target pulls exactly one source: src[k] is target k's source
+                    r[O_SINGLE] = 1 if (len(src) == len(tgt)) else 0
                 else:
                     r[O_NTGT] = 0
+                # rows this op works on, split by length: short rows one thread, long rows one warp
+                vlen = np.diff(rowptr[v])
+                ulen = np.diff(rowptr[p]) if r[O_UMERGE] == 0 else np.zeros(S, np.int64)
+                if p == 0 and xdense and r[O_UMERGE] == 0:
+                    ulen = np.full(S, self.n, np.int64)
+                tlen = np.diff(tptr) if r[O_DENSE] == 0 else np.zeros(S, np.int64)
+                work = np.maximum(np.maximum(vlen, ulen), tlen)
+                rows = np.nonzero(work > 0)[0]
+                short = rows[work[rows] <= ROW_THREAD_MAX]
+                long_ = rows[work[rows] > ROW_THREAD_MAX]
+                r[O_SHORT] = P.add_int(short)
+                r[O_NSHORT] = len(short)
+                r[O_LONG] = P.add_int(long_)
+                r[O_NLONG] = len(long_)
                 self.op_recs.append(r)
-            if last_use.get(v, -2) == i and v != 0:
+            if last_use.get(v, -2) == i and v != 0 and bufoff.get(v, 0) >= 0:
                 release(v)
         smem = top
         x_nnz = 0 if fold else nnz.get(0, 0)
@@ -545,19 +596,20 @@ class Program:
         rec[P_XNNZ] = x_nnz
         rec[P_XBUF] = bufoff.get(0, -1) if not fold else -1
         if not fold and 0 in pats:
-            rec[P_XRP] = P.add_int(rowptr[0])
-            rec[P_XCOLS] = P.add_int(cols[0])
+            rec[P_XRP], rec[P_XCOLS] = pattern(0)
         rec[P_NFOLD] = 1 if fold else 0
         rec[P_SMEM] = smem
-        rec[P_TRP] = P.add_int(rowptr[pi.t])
-        rec[P_TCOLS] = P.add_int(cols[pi.t])
+        rec[P_TRP], rec[P_TCOLS] = pattern(pi.t)
         rec[P_FINAL] = 1 if pi.final else 0
         rec[P_NVISIT] = len([v for v in pi.order if v in pats])
         rec[P_MAXROW] = int(max(np.diff(rowptr[v]).max(initial=0) for v in pats if not (v == 0 and fold)))
         rec[P_ONEHOT] = 1 if rec[P_MAXROW] <= 1 else 0
+        rec[P_XMAXROW] = int(np.diff(rowptr[0]).max(initial=0)) if (0 in pats and not fold) else 0
+        rec[P_XDENSE] = 1 if xdense else 0
+        rec[P_TMAXROW] = int(np.diff(rowptr[pi.t]).max(initial=0))
         self.pass_recs.append(rec)
         # kernel shared memory: per side 7 row arrays (S) + the entry buffers
-        self.max_smem = max(self.max_smem, pi.sides * (7 * S + smem))
+        self.max_smem = max(self.max_smem, pi.sides * (7 * S + smem) + 32)
         self.max_S = max(self.max_S, S)
         pi.bufoff = bufoff
         pi.fold = fold

@@ -58,7 +58,8 @@ int64_t gear_crown_workspace_bytes(const gear_dag* dag, int64_t batch);
  *   x_L, x_U  (batch, n) float64      box of every subdomain
  *   C         (batch, S, w_out) float64, or NULL for the identity specification
  *   lb        (batch, S) float64      lower bound of every specification row
- *   lA        (batch, S, n) float64 or NULL   A of the bound w.r.t. the input
+ *   lA        (batch, S, n) float64   A of the bound w.r.t. the input (required: the
+ *                                     final pass accumulates A in this buffer)
  *   lbias     (batch, S) float64 or NULL      bias of that plane (lb minus the
  *                                            concretised A term)
  * `stream` is a cudaStream_t (NULL: the legacy default stream). Asynchronous. */

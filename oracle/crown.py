@@ -567,6 +567,21 @@ class CrownOracle:
         bias_mag = [np.zeros((S, B)), np.zeros((S, B))]
         err = [np.zeros((S, B)), np.zeros((S, B))]
         undef = [np.zeros((S, B), bool), np.zeros((S, B), bool)]
+        # contributions into each node in this pass (merge-rounding factor K_p)
+        reach, K = {t}, {}
+        q2, deg2 = deque([t]), dict(deg)
+        while q2:
+            l = q2.popleft()
+            if l == 0:
+                continue
+            for p in g[l].inputs:
+                deg2[p] -= 1
+                if deg2[p] == 0:
+                    q2.append(p)
+            if l in reach:
+                for p in g[l].inputs:
+                    reach.add(p)
+                    K[p] = K.get(p, 0) + 1
         queue = deque([t])
         nvisit = 0
         while queue:
@@ -593,13 +608,11 @@ class CrownOracle:
                     if p not in A:
                         A[p] = [None, None]
                     old = A[p][side]
-                    if old is None:
-                        A[p][side] = new
-                    else:
-                        s = old + new
-                        # merge charge: u <|old + new|, m_p>
-                        err[side] += U * abs_dot(np.abs(s).transpose(0, 1, 2), self.magnitude(p)[None])
-                        A[p][side] = s
+                    if K.get(p, 0) >= 2:
+                        # merge rounding: the K_p additions into A_p err by at most
+                        # gamma(K_p) sum_i |contribution_i| (charged per contribution)
+                        err[side] += gamma(K[p]) * abs_dot(np.abs(new), self.magnitude(p)[None])
+                    A[p][side] = new if old is None else old + new
         # concretisation at the input
         xL, xU = self.xL, self.xU
         x0 = (xU + xL) / 2.0
