@@ -37,6 +37,21 @@ def lib():
         L.gear_last_error.restype = ctypes.c_char_p
         L.gear_last_launch_count.argtypes = []
         L.gear_last_launch_count.restype = ctypes.c_int
+        vp, i64, i32, dbl = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_double
+        L.gear_bab_workspace_bytes.argtypes = [i64]
+        L.gear_bab_workspace_bytes.restype = i64
+        L.gear_bab_prune.argtypes = [vp, vp, i64, i32, vp, vp, vp, vp, vp, i64, vp]
+        L.gear_bab_prune.restype = i32
+        L.gear_bab_branch.argtypes = [vp, vp, vp, vp, vp, i64, i32, i32, vp, dbl, dbl, vp, vp, i64, vp]
+        L.gear_bab_branch.restype = i32
+        L.gear_bab_split.argtypes = [vp, vp, vp, i64, i32, vp, vp, vp, vp, i32, vp, vp, vp, vp]
+        L.gear_bab_split.restype = i32
+        L.gear_queue_order.argtypes = [vp, vp, vp, i64, vp, i64, vp]
+        L.gear_queue_order.restype = i32
+        L.gear_gather_rows.argtypes = [vp, vp, i64, i64, vp, vp]
+        L.gear_gather_rows.restype = i32
+        L.gear_scatter_rows.argtypes = [vp, vp, i64, i64, vp, vp]
+        L.gear_scatter_rows.restype = i32
         _LIB = L
     return _LIB
 
@@ -59,4 +74,5 @@ def ptr_dbl(a):
 
 
 EXPORTED = ("gear_dag_create", "gear_dag_destroy", "gear_crown_workspace_bytes", "gear_crown_lower",
-            "gear_last_launch_count", "gear_last_error")
+            "gear_last_launch_count", "gear_last_error", "gear_bab_workspace_bytes", "gear_bab_prune",
+            "gear_bab_branch", "gear_bab_split", "gear_queue_order", "gear_gather_rows", "gear_scatter_rows")

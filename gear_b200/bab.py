@@ -1,0 +1,239 @@
+"""Input-space branch and bound on the GPU: select / bound / prune / branch / split.
+
+One iteration mirrors the reference's reordered loop (``complete_verifier/input_split/
+batch_branch_and_bound.py:275-652`` with ``reorder_bab``) restricted to the hot path:
+
+  select   the domains with the smallest objective key (queue sorted by the objective
+           row's lower bound, descending, ties by insertion id; the batch is the tail)
+           -- ``branching_domains.py:831-962, 1171``
+  bound    CROWN ``compute_bounds`` over the batch (the GPU megakernel)
+           -- ``bounding.py:124``
+  prune    ``get_remaining_index`` in solving mode -- ``branching_domains.py:412-558``
+  branch   SB score with sb_sum, top-1, width guard -- ``branching_heuristics.py:25-202``
+  split    midpoint bisection, children [upper halves; lower halves] -- ``split.py:26-122``
+  keys     children keyed by max(parent lb, parent plane minimum over the child box)
+           -- ``batch_branch_and_bound.py:189-225``
+
+Every step is a kernel of libgear_b200.so on device-resident data; the host only reads the
+number of surviving domains once per iteration. The global dual bound D is the minimum
+objective key over the open domains, capped by the smallest threshold of the domains
+discarded by the objective row (``batch_branch_and_bound.py:628-636``).
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import torch
+
+from . import _lib
+from .engine import CrownEngine
+from .graph import Graph
+
+
+def _p(t):
+    return None if t is None else t.data_ptr()
+
+
+@dataclass
+class BaBStats:
+    iterations: int = 0
+    bounded: int = 0
+    pruned: int = 0
+    history: List[dict] = field(default_factory=list)
+
+
+class DomainQueue:
+    """Device-resident pool of open subdomains (structure of arrays over slots)."""
+
+    def __init__(self, n: int, S: int, capacity: int, device):
+        self.n, self.S, self.device = n, S, device
+        self.cap = 0
+        self.lo = self.hi = self.key = self.thr = self.ids = None
+        self.free: List[torch.Tensor] = []
+        self.active = torch.empty(0, dtype=torch.int32, device=device)
+        self.next_id = 0
+        self._grow(max(capacity, 1))
+
+    def _grow(self, cap):
+        dev = self.device
+        new = dict(lo=torch.empty(cap, self.n, dtype=torch.float64, device=dev),
+                   hi=torch.empty(cap, self.n, dtype=torch.float64, device=dev),
+                   key=torch.full((cap, self.S), math.inf, dtype=torch.float64, device=dev),
+                   thr=torch.empty(cap, self.S, dtype=torch.float64, device=dev),
+                   ids=torch.zeros(cap, dtype=torch.int64, device=dev))
+        if self.cap:
+            for k in new:
+                new[k][:self.cap] = getattr(self, k)
+        for k, v in new.items():
+            setattr(self, k, v)
+        self.free_slots = torch.cat([getattr(self, "free_slots", torch.empty(0, dtype=torch.int32, device=dev)),
+                                     torch.arange(self.cap, cap, dtype=torch.int32, device=dev)])
+        self.cap = cap
+
+    def __len__(self):
+        return int(self.active.numel())
+
+    def push(self, lo, hi, key, thr):
+        m = lo.shape[0]
+        if m == 0:
+            return
+        if self.free_slots.numel() < m:
+            self._grow(max(2 * self.cap, self.cap + m))
+        slots = self.free_slots[-m:]
+        self.free_slots = self.free_slots[:-m]
+        L = _lib.lib()
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        for src, dst, w in ((lo, self.lo, self.n), (hi, self.hi, self.n), (key, self.key, self.S),
+                            (thr, self.thr, self.S)):
+            _lib.check(L.gear_scatter_rows(_p(src.contiguous()), _p(slots), m, w, _p(dst), stream), "gear_scatter_rows")
+        self.ids[slots.long()] = torch.arange(self.next_id, self.next_id + m, device=self.device)
+        self.next_id += m
+        self.active = torch.cat([self.active, slots])
+
+    def pop(self, batch: int):
+        """Sort by (objective key desc, id asc) and take the last `batch` domains."""
+        N = len(self)
+        b = min(batch, N)
+        n2 = 1 << max(0, (N - 1).bit_length())
+        order = torch.empty(max(n2, 1), dtype=torch.int32, device=self.device)
+        key0 = self.key[:, 0].contiguous()
+        L = _lib.lib()
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        _lib.check(L.gear_queue_order(_p(key0), _p(self.ids), _p(self.active), N, _p(order), order.numel(), stream),
+                   "gear_queue_order")
+        order = order[:N]
+        slots = order[N - b:].contiguous()
+        self.active = order[:N - b].contiguous()
+        out = []
+        for src, w in ((self.lo, self.n), (self.hi, self.n), (self.key, self.S), (self.thr, self.S)):
+            dst = torch.empty(b, w, dtype=torch.float64, device=self.device)
+            _lib.check(L.gear_gather_rows(_p(src), _p(slots), b, w, _p(dst), stream), "gear_gather_rows")
+            out.append(dst)
+        self.free_slots = torch.cat([self.free_slots, slots])
+        return out
+
+    def min_key(self) -> float:
+        if len(self) == 0:
+            return math.inf
+        return float(self.key[self.active.long(), 0].min())
+
+
+class BaB:
+    """Branch and bound to a relative gap on one NLP instance (x in [lo, hi]).
+
+    The model maps x (B, n) to y (B, 1 + m): row 0 the objective, rows 1..m constraints
+    g_k(x) <= rhs_k (rhs given already relaxed by the instance's feasibility tolerance)."""
+
+    def __init__(self, graph: Graph, lo: torch.Tensor, hi: torch.Tensor, rhs: Optional[torch.Tensor] = None,
+                 device="cuda", batch: int = 4096, sb_coeff_thresh: float = 1e-3,
+                 sb_min_width_ratio: float = 1e-3, model: Optional[torch.nn.Module] = None):
+        self.device = torch.device(device)
+        self.graph = graph
+        self.engine = CrownEngine(graph)
+        self.n = self.engine.n
+        self.S = self.engine.S
+        self.batch = batch
+        self.coeff_thresh = sb_coeff_thresh
+        self.min_width_ratio = sb_min_width_ratio
+        self.model = model
+        lo = lo.reshape(1, -1).to(self.device, torch.float64)
+        hi = hi.reshape(1, -1).to(self.device, torch.float64)
+        self.root_width = (hi - lo).reshape(-1).contiguous()
+        self.rhs = (torch.zeros(self.S - 1, dtype=torch.float64) if rhs is None else rhs.to(torch.float64)).to(self.device)
+        self.incumbent = math.inf
+        self.x_best = None
+        self.queue = DomainQueue(self.n, self.S, 4 * batch, self.device)
+        key = torch.full((1, self.S), -math.inf, dtype=torch.float64, device=self.device)
+        self.queue.push(lo, hi, key, self._thresholds(1))
+        self.disc_min = torch.full((1,), math.inf, dtype=torch.float64, device=self.device)
+        self.stats = BaBStats()
+        self._ws = torch.empty(1, dtype=torch.uint8, device=self.device)
+
+    def _thresholds(self, m):
+        t = torch.empty(m, self.S, dtype=torch.float64, device=self.device)
+        t[:, 0] = self.incumbent
+        t[:, 1:] = self.rhs
+        return t
+
+    def _ws_bytes(self, nbytes):
+        if self._ws.numel() < nbytes:
+            self._ws = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+        return self._ws
+
+    def update_incumbent(self, x: torch.Tensor):
+        """Primal points: evaluate the model (float64) and keep the best feasible objective."""
+        if self.model is None or x.numel() == 0:
+            return
+        with torch.no_grad():
+            y = self.model(x.to(self.device, torch.float64))
+        feas = (y[:, 1:] <= self.rhs).all(1) if y.shape[1] > 1 else torch.ones(y.shape[0], dtype=torch.bool,
+                                                                                device=self.device)
+        if bool(feas.any()):
+            obj = torch.where(feas, y[:, 0], torch.full_like(y[:, 0], math.inf))
+            i = int(torch.argmin(obj))
+            v = float(obj[i])
+            if v < self.incumbent:
+                self.incumbent = v
+                self.x_best = x[i].detach().clone()
+
+    def dual_bound(self) -> float:
+        d = self.queue.min_key()
+        return min(d, float(self.disc_min))
+
+    def gap(self) -> float:
+        P, D = self.incumbent, self.dual_bound()
+        if not math.isfinite(P):
+            return math.inf
+        if not math.isfinite(D):
+            return 0.0 if D > 0 else math.inf
+        return (P - D) / max(1.0, abs(P), abs(D))
+
+    def step(self):
+        """One iteration; returns the number of domains bounded."""
+        q = self.queue
+        if len(q) == 0:
+            return 0
+        lo, hi, key, thr = q.pop(self.batch)
+        B = lo.shape[0]
+        thr[:, 0] = self.incumbent          # thresholds follow the current incumbent
+        self.update_incumbent((lo + hi) / 2)
+        thr[:, 0] = self.incumbent
+        lb, lA, lbias = self.engine.lower(lo, hi)
+        L = _lib.lib()
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        keep = torch.empty(B, dtype=torch.uint8, device=self.device)
+        kept = torch.empty(B, dtype=torch.int32, device=self.device)
+        nk = torch.zeros(1, dtype=torch.int32, device=self.device)
+        ws = self._ws_bytes(int(L.gear_bab_workspace_bytes(B)))
+        _lib.check(L.gear_bab_prune(_p(lb), _p(thr), B, self.S, _p(keep), _p(kept), _p(nk), _p(self.disc_min),
+                                    _p(ws), ws.numel(), stream), "gear_bab_prune")
+        split_idx = torch.empty(B, dtype=torch.int32, device=self.device)
+        _lib.check(L.gear_bab_branch(_p(lA), _p(lo), _p(hi), _p(lb), _p(thr), B, self.S, self.n,
+                                     _p(self.root_width), self.coeff_thresh, self.min_width_ratio, _p(split_idx),
+                                     _p(ws), ws.numel(), stream), "gear_bab_branch")
+        K = int(nk.item())                   # the one host read per iteration
+        self.stats.iterations += 1
+        self.stats.bounded += B
+        self.stats.pruned += B - K
+        if K > 0:
+            clo = torch.empty(2 * K, self.n, dtype=torch.float64, device=self.device)
+            chi = torch.empty_like(clo)
+            ckey = torch.empty(2 * K, self.S, dtype=torch.float64, device=self.device)
+            _lib.check(L.gear_bab_split(_p(lo), _p(hi), _p(kept), K, self.n, _p(split_idx), _p(lb), _p(lA),
+                                        _p(lbias), self.S, _p(clo), _p(chi), _p(ckey), stream), "gear_bab_split")
+            q.push(clo, chi, ckey, torch.cat([thr[kept[:K].long()]] * 2))
+        return B
+
+    def run(self, rel_gap: float = 1e-4, max_iterations: int = 10000, time_limit: float = 60.0):
+        t0 = time.perf_counter()
+        while len(self.queue) and self.stats.iterations < max_iterations:
+            self.step()
+            g = self.gap()
+            self.stats.history.append(dict(it=self.stats.iterations, P=self.incumbent, D=self.dual_bound(),
+                                           gap=g, open=len(self.queue)))
+            if g <= rel_gap or time.perf_counter() - t0 > time_limit:
+                break
+        return self.incumbent, self.dual_bound(), self.gap()

@@ -10,6 +10,7 @@
 
 #include "../../include/gear_b200.h"
 #include "crown_kernel.cuh"
+#include "bab_kernels.cuh"
 
 namespace {
 thread_local std::string g_err;
@@ -157,6 +158,128 @@ extern "C" int gear_crown_lower(const gear_dag* dag, const double* x_L, const do
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "crown_megakernel launch");
   return GEAR_OK;
+}
+
+// ------------------------------------------------------------------ branch and bound
+namespace {
+__global__ void u64_from_double(const double* v, unsigned long long* u) { *u = gear::bab::ordered_bits(*v); }
+__global__ void double_from_u64(const unsigned long long* u, double* v) { *v = gear::bab::from_ordered_bits(*u); }
+inline unsigned grid_for(int64_t work) { return (unsigned)((work + gear::bab::BT - 1) / gear::bab::BT); }
+}  // namespace
+
+extern "C" int64_t gear_bab_workspace_bytes(int64_t batch) {
+  int64_t nblocks = (batch + gear::bab::BT - 1) / gear::bab::BT;
+  return 64 + (nblocks + 64) * (int64_t)sizeof(int32_t);
+}
+
+extern "C" int gear_bab_prune(const double* lb, const double* thr, int64_t batch, int S, uint8_t* keep, int32_t* kept,
+                              int32_t* n_kept, double* disc_min, void* workspace, int64_t ws_bytes, void* stream) {
+  using namespace gear::bab;
+  if (!lb || !thr || !keep || !kept || !n_kept || !disc_min || batch < 0 || S < 1)
+    return fail(GEAR_E_INVALID, "gear_bab_prune: %s", "bad arguments");
+  if (!workspace || ws_bytes < gear_bab_workspace_bytes(batch))
+    return fail(GEAR_E_WORKSPACE, "gear_bab_prune: %s", "workspace too small");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (batch == 0) { cudaMemsetAsync(n_kept, 0, sizeof(int32_t), st); return GEAR_OK; }
+  int64_t nblocks = (batch + BT - 1) / BT;
+  if (nblocks > (int64_t)BT * 1024) return fail(GEAR_E_INVALID, "gear_bab_prune: %s", "batch too large");
+  unsigned long long* u = (unsigned long long*)workspace;
+  int32_t* counts = (int32_t*)((char*)workspace + 64);
+  u64_from_double<<<1, 1, 0, st>>>(disc_min, u);
+  prune_kernel<<<(unsigned)nblocks, BT, 0, st>>>(lb, thr, batch, S, keep, u);
+  double_from_u64<<<1, 1, 0, st>>>(u, disc_min);
+  count_kernel<<<(unsigned)nblocks, BT, 0, st>>>(keep, batch, counts);
+  scan_counts_kernel<<<1, BT, 0, st>>>(counts, (int)nblocks, n_kept);
+  compact_kernel<<<(unsigned)nblocks, BT, 0, st>>>(keep, batch, counts, kept);
+  g_launches = 6;
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_bab_prune");
+}
+
+extern "C" int gear_bab_branch(const double* lA, const double* lo, const double* hi, const double* lb,
+                               const double* thr, int64_t batch, int S, int n, const double* root_width,
+                               double coeff_thresh, double min_width_ratio, int32_t* split_idx, void* workspace,
+                               int64_t ws_bytes, void* stream) {
+  using namespace gear::bab;
+  if (!lA || !lo || !hi || !lb || !thr || !split_idx || batch < 0 || S < 1 || n < 1)
+    return fail(GEAR_E_INVALID, "gear_bab_branch: %s", "bad arguments");
+  if (!workspace || ws_bytes < 64) return fail(GEAR_E_WORKSPACE, "gear_bab_branch: %s", "workspace too small");
+  if (batch == 0) return GEAR_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  int* flag = (int*)workspace;
+  cudaMemsetAsync(flag, 0, sizeof(int), st);
+  int64_t nA = batch * (int64_t)S * n, nS = batch * (int64_t)S;
+  unsigned g = grid_for(nA < (int64_t)1 << 26 ? nA : (int64_t)1 << 26);
+  nonfinite_kernel<<<g, BT, 0, st>>>(lA, nA, lb, thr, nS, flag);
+  branch_kernel<<<grid_for(batch * 32), BT, 0, st>>>(lA, lo, hi, batch, S, n, root_width, coeff_thresh,
+                                                        min_width_ratio, flag, split_idx);
+  g_launches = 2;
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_bab_branch");
+}
+
+extern "C" int gear_bab_split(const double* lo, const double* hi, const int32_t* kept, int64_t n_kept, int n,
+                              const int32_t* split_idx, const double* lb, const double* lA, const double* lbias,
+                              int S, double* child_lo, double* child_hi, double* child_key, void* stream) {
+  using namespace gear::bab;
+  if (!lo || !hi || !kept || !split_idx || !child_lo || !child_hi || n_kept < 0 || n < 1)
+    return fail(GEAR_E_INVALID, "gear_bab_split: %s", "bad arguments");
+  if (n_kept == 0) return GEAR_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  split_kernel<<<grid_for(2 * n_kept * n), BT, 0, st>>>(lo, hi, kept, n_kept, n, split_idx, child_lo, child_hi);
+  g_launches = 1;
+  if (child_key) {
+    if (!lb || !lA || !lbias || S < 1) return fail(GEAR_E_INVALID, "gear_bab_split: %s", "keys need lb, lA, lbias");
+    child_keys_kernel<<<grid_for(2 * n_kept * 32), BT, 0, st>>>(lb, lA, lbias, child_lo, child_hi, kept, n_kept, S,
+                                                                   n, child_key);
+    g_launches = 2;
+  }
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_bab_split");
+}
+
+extern "C" int gear_queue_order(const double* key, const int64_t* id, const int32_t* slots, int64_t count,
+                                int32_t* order, int64_t order_len, void* stream) {
+  using namespace gear::bab;
+  if (!key || !id || !slots || !order || count < 0) return fail(GEAR_E_INVALID, "gear_queue_order: %s", "bad arguments");
+  int64_t n2 = 1;
+  while (n2 < count) n2 <<= 1;
+  if (order_len < n2) return fail(GEAR_E_WORKSPACE, "gear_queue_order: %s", "order buffer shorter than the next power of two");
+  if (count == 0) return GEAR_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaMemsetAsync(order, 0xff, n2 * sizeof(int32_t), st);             // padding = -1
+  cudaMemcpyAsync(order, slots, count * sizeof(int32_t), cudaMemcpyDeviceToDevice, st);
+  int launches = 0;
+  for (int64_t k = 2; k <= n2; k <<= 1)
+    for (int64_t j = k >> 1; j > 0; j >>= 1) {
+      bitonic_step<<<grid_for(n2), BT, 0, st>>>(order, key, id, n2, count, (int)j, (int)k);
+      ++launches;
+    }
+  g_launches = launches;
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_queue_order");
+}
+
+extern "C" int gear_gather_rows(const double* src, const int32_t* rows, int64_t count, int64_t width, double* dst,
+                                void* stream) {
+  if (!src || !rows || !dst || count < 0 || width < 1) return fail(GEAR_E_INVALID, "gear_gather_rows: %s", "bad arguments");
+  if (count == 0) return GEAR_OK;
+  gear::bab::gather_rows_kernel<<<grid_for(count * width), gear::bab::BT, 0, (cudaStream_t)stream>>>(src, rows, count,
+                                                                                                    width, dst);
+  g_launches = 1;
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_gather_rows");
+}
+
+extern "C" int gear_scatter_rows(const double* src, const int32_t* rows, int64_t count, int64_t width, double* dst,
+                                 void* stream) {
+  if (!src || !rows || !dst || count < 0 || width < 1) return fail(GEAR_E_INVALID, "gear_scatter_rows: %s", "bad arguments");
+  if (count == 0) return GEAR_OK;
+  gear::bab::scatter_rows_kernel<<<grid_for(count * width), gear::bab::BT, 0, (cudaStream_t)stream>>>(src, rows, count,
+                                                                                                     width, dst);
+  g_launches = 1;
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_scatter_rows");
 }
 
 #ifdef GEAR_STEP_PROFILE
