@@ -38,6 +38,10 @@ def lib():
         L.gear_last_launch_count.argtypes = []
         L.gear_last_launch_count.restype = ctypes.c_int
         vp, i64, i32, dbl = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_double
+        L.gear_crown_lower_static.argtypes = [vp, vp, vp, i64, vp, vp, vp, vp, vp]
+        L.gear_crown_lower_static.restype = i32
+        L.gear_crown_static_scratch_bytes.argtypes = []
+        L.gear_crown_static_scratch_bytes.restype = i64
         L.gear_bab_workspace_bytes.argtypes = [i64]
         L.gear_bab_workspace_bytes.restype = i64
         L.gear_bab_prune.argtypes = [vp, vp, i64, i32, vp, vp, vp, vp, vp, i64, vp]
@@ -75,4 +79,5 @@ def ptr_dbl(a):
 
 EXPORTED = ("gear_dag_create", "gear_dag_destroy", "gear_crown_workspace_bytes", "gear_crown_lower",
             "gear_last_launch_count", "gear_last_error", "gear_bab_workspace_bytes", "gear_bab_prune",
-            "gear_bab_branch", "gear_bab_split", "gear_queue_order", "gear_gather_rows", "gear_scatter_rows")
+            "gear_bab_branch", "gear_bab_split", "gear_queue_order", "gear_gather_rows", "gear_scatter_rows",
+            "gear_crown_lower_static", "gear_crown_static_scratch_bytes")

@@ -5,6 +5,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <mutex>
 #include <new>
 #include <string>
 
@@ -158,6 +159,81 @@ extern "C" int gear_crown_lower(const gear_dag* dag, const double* x_L, const do
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "crown_megakernel launch");
   return GEAR_OK;
+}
+
+// ------------------------------------------------------------------ no-allocation entry point
+// Scratch for callers that must not allocate device memory themselves: a solver host that
+// hands this library a fixed device-memory plan (and no allocator), or a loop that cannot
+// afford cudaMalloc's implicit device synchronisation or an allocation failure mid-run.
+// Every GPU that loads this library holds the array until the process exits.
+namespace {
+constexpr int64_t kStaticScratchBytes = int64_t(64) << 20;   // 64 MiB
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+constexpr int kMaxDevices = 64;
+void* g_static_scratch_ptr[kMaxDevices] = {nullptr};
+std::mutex g_static_scratch_mu;
+
+// The array's name is only a host-side handle; the kernel needs its device address, which
+// cudaGetSymbolAddress gives per device (looked up once, with that device current).
+int static_scratch(void** out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
+  if (dev < 0 || dev >= kMaxDevices) return fail(GEAR_E_INVALID, "gear_crown_lower_static: %s", "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_static_scratch_mu);
+  if (!g_static_scratch_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess || !p) return cuda_fail(e == cudaSuccess ? cudaErrorInvalidSymbol : e, "cudaGetSymbolAddress(scratch)");
+    g_static_scratch_ptr[dev] = p;
+  }
+  *out = g_static_scratch_ptr[dev];
+  return GEAR_OK;
+}
+}  // namespace
+
+extern "C" int64_t gear_crown_static_scratch_bytes(void) { return kStaticScratchBytes; }
+
+extern "C" int gear_crown_lower_static(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
+                                       const double* C, double* lb, double* lA, double* lbias, void* stream) {
+  g_launches = 0;
+  if (!dag || !x_L || !x_U || !lb || batch < 0) return fail(GEAR_E_INVALID, "gear_crown_lower_static: %s", "bad arguments");
+  if (dag->hdr[gear::H_RETA] != 0 && !lA)
+    return fail(GEAR_E_INVALID, "gear_crown_lower_static: %s", "this program accumulates A in the lA output: lA is required");
+  if (batch == 0) return GEAR_OK;
+  const int64_t slot_bytes = dag->slot_doubles * (int64_t)sizeof(double);
+  const int64_t max_slots = kStaticScratchBytes / slot_bytes;
+  if (max_slots < 1) {
+    char msg[256];
+    snprintf(msg, sizeof(msg), "gear_crown_lower_static: one CTA of this program needs %lld bytes of scratch, "
+             "more than the static %lld bytes; use gear_crown_lower with a workspace",
+             (long long)slot_bytes, (long long)kStaticScratchBytes);
+    g_err = msg;
+    return GEAR_E_WORKSPACE;
+  }
+  void* scratch = nullptr;
+  int st = static_scratch(&scratch);
+  if (st != GEAR_OK) return st;
+  int64_t slots = slots_for(dag, batch);
+  if (slots > max_slots) slots = max_slots;
+  gear::Work wk;
+  wk.xL = x_L;
+  wk.xU = x_U;
+  wk.C = C;
+  wk.lb = lb;
+  wk.lA = lA;
+  wk.lbias = lbias;
+  wk.scratch = (double*)scratch;   // the kernel writes every scratch word before reading it: no clearing
+  wk.slot_doubles = dag->slot_doubles;
+  wk.B = batch;
+  wk.status = nullptr;
+  cudaError_t ea = cudaFuncSetAttribute(gear::crown_megakernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        dag->smem_bytes);
+  if (ea != cudaSuccess) return cuda_fail(ea, "cudaFuncSetAttribute");
+  gear::crown_megakernel<<<(unsigned)slots, gear::NT, dag->smem_bytes, (cudaStream_t)stream>>>(dag->P, wk);
+  g_launches = 1;
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "crown_megakernel launch");
 }
 
 // ------------------------------------------------------------------ branch and bound

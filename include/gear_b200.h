@@ -67,6 +67,24 @@ int gear_crown_lower(const gear_dag* dag, const double* x_L, const double* x_U, 
                      const double* C, double* lb, double* lA, double* lbias,
                      void* workspace, int64_t workspace_bytes, void* stream);
 
+/* gear_crown_lower without a workspace argument, for callers that cannot allocate device
+ * memory (a solver host that owns a fixed device-memory plan and gives this library no
+ * allocator, or a loop that must not pay cudaMalloc's implicit synchronisation). It has no
+ * counterpart in the reference. Its scratch is a fixed array inside the library
+ * (gear_crown_static_scratch_bytes(), 64 MiB) that every GPU loading the library keeps until
+ * the process exits; the batch is processed by as many CTAs as fit in it, and a program whose
+ * single CTA needs more scratch than that is rejected with GEAR_E_WORKSPACE. It calls no
+ * cudaMalloc / cudaFree. The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture. All calls share the
+ * one array, so calls that overlap on the GPU (different streams, different host threads on
+ * the same device) race: serialise them. The gear_dag handle itself is still created (and
+ * allocated) once by gear_dag_create. */
+int gear_crown_lower_static(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
+                            const double* C, double* lb, double* lA, double* lbias, void* stream);
+
+/* Size in bytes of gear_crown_lower_static's built-in scratch array. */
+int64_t gear_crown_static_scratch_bytes(void);
+
 /* Number of kernel launches the last gear_crown_lower on this thread issued. */
 int gear_last_launch_count(void);
 
