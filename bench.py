@@ -161,6 +161,8 @@ def main():
     ap.add_argument("--impl", default="gear", choices=["gear", "reference"])
     ap.add_argument("--cpu-per-core", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="cta", choices=["cta", "simt"],
+                    help="CROWN kernel: one box per CTA or one box per thread")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -181,7 +183,7 @@ def main():
     B = args.batch
     model = problems.make_instance(WORKLOAD, 0)
     lo, hi = problems.make_boxes(WORKLOAD, B, 0, seed_offset=500 + 7919 * rank)
-    bm = BoundedModule(model, lo[:2], device=str(dev))
+    bm = BoundedModule(model, lo[:2], device=str(dev), bound_opts={"gear_mode": args.mode})
     S = bm.final_node_width()
     n = lo.shape[1]
     eng = bm._engine(S, False)
@@ -267,13 +269,14 @@ def main():
         res = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-               "config": {"workload": WORKLOAD, "batch": B, "n": n, "spec_rows": S,
+               "config": {"workload": WORKLOAD, "batch": B, "n": n, "spec_rows": S, "kernel_mode": args.mode,
                           "parallelism": f"replicas{world}",
                           "l2": "inputs (x_L, x_U) and outputs (lA) larger than the 126 MB L2"},
                "gpu_launches": launches,
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "traffic": traffic,
-                            "kernel": "crown_megakernel", "peak_source": peak_kind},
+                            "kernel": "crown_megakernel" if args.mode == "cta" else "crown_simt_kernel",
+                            "peak_source": peak_kind},
                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * B * n * 8,
                        "d2h_bytes_per_step": B * S * 8},
                "clocks": clk.summary()}

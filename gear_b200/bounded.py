@@ -88,7 +88,8 @@ class BoundedModule:
         eng = self._engines.get(key)
         if eng is None:
             with torch.cuda.device(self.device):
-                eng = CrownEngine(self.graph, spec_rows=spec_rows, dense_c=dense_c)
+                eng = CrownEngine(self.graph, spec_rows=spec_rows, dense_c=dense_c,
+                                  mode=self.bound_opts.get("gear_mode", "cta"))
             self._engines[key] = eng
         return eng
 

@@ -38,7 +38,7 @@ constexpr double UNIT = EPS / 2;
 constexpr double EPSILON = 1e-12;               // operators/base.py:32
 constexpr double TIE_TOL = 1e-12;               // McCormick tie tolerance (see program.py)
 constexpr double STEP_PRE = 0.01;
-constexpr int NT = 256;                         // threads per CTA
+constexpr int NT = 64;                          // threads per CTA (one box per CTA)
 constexpr int NWARP = NT / 32;
 
 // sin/cos table offsets (gear_b200/tables.py SIN_TABLE_ORDER)
@@ -326,12 +326,12 @@ struct Box {
 
 __device__ __forceinline__ const int32_t* node_rec(const DevProgram* P, int v) { return P->nodes + v * NODE_REC; }
 
-// interval sums over the inputs of a reducesum output j (increasing input order)
-__device__ void ibp_element(const Box& bx, const int32_t* nd, int j, double* olo, double* ohi) {
-  const DevProgram* P = bx.P;
+// Interval of element j of a node from its inputs' intervals (the operators'
+// interval_propagate). V is the interval-arena view: a plain pointer (one box per CTA) or a
+// box-interleaved view (one box per thread).
+template <class V>
+__device__ void ibp_element_t(const DevProgram* P, V lo, V hi, const int32_t* nd, int j, double* olo, double* ohi) {
   const int kind = nd[N_KIND];
-  const double* lo = bx.lo;
-  const double* hi = bx.hi;
   double l = 0, h = 0;
   switch (kind) {
     case NK_MUL: {
@@ -439,6 +439,10 @@ __device__ void ibp_element(const Box& bx, const int32_t* nd, int j, double* olo
   }
   *olo = nan_lo(l);
   *ohi = nan_hi(h);
+}
+
+__device__ __forceinline__ void ibp_element(const Box& bx, const int32_t* nd, int j, double* olo, double* ohi) {
+  ibp_element_t<const double*>(bx.P, bx.lo, bx.hi, nd, j, olo, ohi);
 }
 
 // Linear / MatMul interval (interval_bound + BoundLinear._bound_box): warp per output row.
@@ -591,8 +595,11 @@ __device__ unsigned long long g_op_cycles[8192];
 #endif
 
 // ------------------------------------------------------------------ CROWN pass
-// Row arrays in shared memory, per side: bias, bias magnitude, charge, base, dev, berr, undef.
-enum { R_BIAS = 0, R_BMAG, R_CHG, R_BASE, R_DEV, R_BERR, R_UNDEF, R_COUNT };
+// Row arrays in shared memory, per side: VAL = bias + A x0 (NaN marks an undefined row),
+// ERR = every outward-rounding magnitude already scaled by its factor, plus |A| eps,
+// ROOT = the input term A x0 -/+ |A| eps (for lbias).
+enum { R_VAL = 0, R_ERR, R_ROOT, R_COUNT };
+constexpr double RE1 = 17 * EPS * 4;   // rounding_error(x, 1) / x
 
 struct PassCtx {
   const int32_t* pr;
@@ -671,6 +678,8 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int n = P->hdr[H_N];
   const int t = pr[P_T];
+  const double fbias = ((double)max(pr[P_NVISIT], 1) + n + 16) * EPS * 4;   // bias sums
+  const double fbox = ((double)n + 16) * EPS * 4;                             // box dot products
   const int32_t* tnd = node_rec(P, t);
 
   for (int k = tid; k < sides * R_COUNT * S; k += NT) ctx.rows[k] = 0.0;
@@ -777,10 +786,9 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
           }
           if (wide) { sb = warp_sum(sb); sm_ = warp_sum(sm_); sc = warp_sum(sc); und_ = warp_or(und_); }
           if (!wide || lane == 0) {
-            ctx.row(side, R_BIAS)[s] += sb;
-            ctx.row(side, R_BMAG)[s] += sm_;
-            ctx.row(side, R_CHG)[s] += sc;
-            if (und_) ctx.row(side, R_UNDEF)[s] = 1.0;
+            double* val = ctx.row(side, R_VAL);
+            val[s] = und_ ? NAN : val[s] + sb;
+            ctx.row(side, R_ERR)[s] += sm_ * fbias + sc;
           }
         }
         if (op[O_FOLD]) {
@@ -791,10 +799,9 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
             const double gk = gamma_k((double)op[O_WOUT]);
             double a = V[e0];
             int c = vcols[e0];
-            ctx.row(side, R_BASE)[s] += a * f[c];
-            ctx.row(side, R_DEV)[s] += fabs(a) * f[w + c];
-            ctx.row(side, R_BERR)[s] += fabs(a) * f[2 * w + c];
-            ctx.row(side, R_CHG)[s] += gk * (fabs(a) * f[2 * w + c]);
+            ctx.row(side, R_VAL)[s] += a * f[c];
+            ctx.row(side, R_ERR)[s] += fabs(a) * f[w + c] + (fabs(a) * f[2 * w + c]) * fbox +
+                                       gk * (fabs(a) * f[2 * w + c]);
           }
           continue;
         }
@@ -834,7 +841,7 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
         }
         if (uk >= 2) {
           if (wide) pmerge = warp_sum(pmerge);
-          if (!wide || lane == 0) ctx.row(side, R_CHG)[s] += gmerge * pmerge;
+          if (!wide || lane == 0) ctx.row(side, R_ERR)[s] += gmerge * pmerge;
         }
       }
     };
@@ -875,13 +882,13 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
               if (tid == 0) {
                 double tb = 0, tm = 0;
                 for (int w_ = 0; w_ < NWARP; ++w_) { tb += ctx.red[w_]; tm += ctx.red[NWARP + w_]; }
-                ctx.row(side, R_BIAS)[s] += tb;
-                ctx.row(side, R_BMAG)[s] += tm;
+                ctx.row(side, R_VAL)[s] += tb;
+                ctx.row(side, R_ERR)[s] += tm * fbias;
               }
               __syncthreads();
             } else if (lane == 0) {
-              ctx.row(side, R_BIAS)[s] += sb;
-              ctx.row(side, R_BMAG)[s] += sm_;
+              ctx.row(side, R_VAL)[s] += sb;
+              ctx.row(side, R_ERR)[s] += sm_ * fbias;
             }
           }
           if (e0 == e1) {
@@ -916,11 +923,11 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
             if (tid == 0) {
               double t_ = 0;
               for (int w_ = 0; w_ < NWARP; ++w_) t_ += ctx.red[w_];
-              ctx.row(side, R_CHG)[s] += t_;
+              ctx.row(side, R_ERR)[s] += t_;
             }
             __syncthreads();
           } else if (lane == 0) {
-            ctx.row(side, R_CHG)[s] += tot_;
+            ctx.row(side, R_ERR)[s] += tot_;
           }
         }
       }
@@ -947,9 +954,7 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
     const RowSplit rs = row_split(pr[P_XMAXROW]);
     for (int side = 0; side < sides; ++side) {
       const double* V = ctx.vals(side, pr[P_XBUF]);
-      double* rbase = ctx.row(side, R_BASE);
-      double* rdev = ctx.row(side, R_DEV);
-      double* rberr = ctx.row(side, R_BERR);
+      const double sign = side == 0 ? -1.0 : 1.0;
       for (int s = rs.first; s < S; s += rs.step) {
         int e0 = xrp[s], e1 = xrp[s + 1];
         double bs = 0, dv = 0, be = 0;
@@ -962,7 +967,11 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
           be += finite_abs(a) * finite_abs(fmax(fabs(l), fabs(h)));
         }
         if (rs.warp) { bs = warp_sum(bs); dv = warp_sum(dv); be = warp_sum(be); }
-        if (!rs.warp || lane == 0) { rbase[s] += bs; rdev[s] += dv; rberr[s] += be; }
+        if (!rs.warp || lane == 0) {
+          ctx.row(side, R_VAL)[s] += bs;
+          ctx.row(side, R_ERR)[s] += dv + be * fbox;
+          ctx.row(side, R_ROOT)[s] = bs + sign * dv;
+        }
       }
     }
   }
@@ -970,23 +979,17 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
 #ifdef GEAR_STEP_PROFILE
   if (tid == 0) atomicAdd(&g_op_cycles[8190], (unsigned long long)(clock64() - t_op));
 #endif
-  const double nvisit = (double)max(pr[P_NVISIT], 1);
   const bool final = pr[P_FINAL] != 0;
   for (int side = 0; side < sides; ++side) {
     double sign = side == 0 ? -1.0 : 1.0;
     for (int s = tid; s < S; s += NT) {
-      double bias = ctx.row(side, R_BIAS)[s];
-      double b = widen(bias, rounding_error(ctx.row(side, R_BMAG)[s], nvisit + n), sign);
-      double root = ctx.row(side, R_BASE)[s] + sign * ctx.row(side, R_DEV)[s];
-      root = widen(root, rounding_error(ctx.row(side, R_BERR)[s], n), sign);
-      if (!isfinite(root)) root = sign * INFINITY;
-      double tot = b + root;
-      tot = widen(tot, rounding_error(finite_abs(tot), 1) + ctx.row(side, R_CHG)[s], sign);
-      bool undef = ctx.row(side, R_UNDEF)[s] != 0.0;
-      if (undef) tot = sign * INFINITY;
+      double val = ctx.row(side, R_VAL)[s], er = ctx.row(side, R_ERR)[s];
+      double tot = val + sign * (er + (fabs(val) + er) * RE1);
+      const bool bad = isnan(tot) || tot == -sign * INFINITY;
+      if (bad) tot = sign * INFINITY;
       if (final) {
         double lbv = tot;
-        if (undef) {
+        if (bad) {
           // interval fallback for a discarded row (backward_bound.py:826)
           double fb = 0;
           if (pr[P_INIT] == 0) fb = bx.lo[tnd[N_CUR] + s];
@@ -1001,17 +1004,19 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
           lbv = fmax(lbv, fb);
         }
         wk.lb[(size_t)bx.b * S + s] = lbv;
-        if (wk.lbias) wk.lbias[(size_t)bx.b * S + s] = undef ? -INFINITY : tot - root;
+        if (wk.lbias) wk.lbias[(size_t)bx.b * S + s] = bad ? -INFINITY : tot - ctx.row(side, R_ROOT)[s];
+        ctx.row(side, R_VAL)[s] = bad ? NAN : tot;    // the lA rows of bad rows are cleared below
       } else {
         double* out = side == 0 ? bx.pres_lo : bx.pres_hi;
         out[s] = tot;
       }
     }
   }
+  __syncthreads();
   if (final && wk.lA && xdense) {
     // the input's A was accumulated in place; rows of undefined bounds become zero
     for (int s = warp; s < S; s += NWARP) {
-      if (ctx.row(0, R_UNDEF)[s] == 0.0) continue;
+      if (!isnan(ctx.row(0, R_VAL)[s])) continue;
       for (int c = lane; c < n; c += 32) ctx.la[(size_t)s * n + c] = 0.0;
     }
   } else if (final && wk.lA) {
@@ -1022,7 +1027,7 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
     if (xrp) {
       const double* V = ctx.vals(0, pr[P_XBUF]);
       for (int s = warp; s < S; s += NWARP) {
-        if (ctx.row(0, R_UNDEF)[s] != 0.0) continue;
+        if (isnan(ctx.row(0, R_VAL)[s])) continue;
         for (int e = xrp[s] + lane; e < xrp[s + 1]; e += 32) lA[(size_t)s * n + xcols[e]] = V[e];
       }
     }
@@ -1048,7 +1053,7 @@ __device__ void compare_node(const Box& bx, int v, double* tmp_lo, double* tmp_h
 }
 
 
-__global__ void __launch_bounds__(NT, 3) crown_megakernel(DevProgram Pg, Work wk) {
+__global__ void __launch_bounds__(NT, 12) crown_megakernel(DevProgram Pg, Work wk) {
   extern __shared__ double sm[];
   const int32_t* hdr = Pg.hdr;
   // shared memory: [pass working set | node table | op records of the running pass]

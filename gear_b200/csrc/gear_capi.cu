@@ -11,6 +11,7 @@
 
 #include "../../include/gear_b200.h"
 #include "crown_kernel.cuh"
+#include "crown_simt.cuh"
 #include "bab_kernels.cuh"
 
 namespace {
@@ -40,6 +41,9 @@ struct gear_dag {
   int device = 0;
   int num_sms = 0;
   int blocks_per_sm = 0;
+  int mode = 0;           // gear::ExecMode
+  int threads = 0;        // threads per CTA
+  int64_t boxes_per_slot = 1;
 };
 
 extern "C" const char* gear_last_error(void) { return g_err.c_str(); }
@@ -86,23 +90,46 @@ extern "C" int gear_dag_create(const int32_t* header, int64_t header_len, const 
   d->P.dp = dp;
   e = cudaGetLastError();
   if (e != cudaSuccess) { cudaFree(d->dev); delete d; return cuda_fail(e, "upload"); }
-  // per-CTA scratch: lo, hi, mag arenas; planes; fold vectors; 4 node-wide temporaries
-  d->slot_doubles = 3 * (int64_t)header[H_ARENA] + header[H_PLANES] + header[H_FOLDW] + 4 * (int64_t)header[H_MAXW] + 8;
-  d->slot_doubles = (d->slot_doubles + 31) / 32 * 32;
-  d->smem_bytes = header[H_SMEM] * (int)sizeof(double);
   cudaDeviceProp prop;
   e = cudaGetDeviceProperties(&prop, d->device);
   if (e != cudaSuccess) { cudaFree(d->dev); delete d; return cuda_fail(e, "cudaGetDeviceProperties"); }
-  if (d->smem_bytes > (int)prop.sharedMemPerBlockOptin) {
+  d->num_sms = prop.multiProcessorCount;
+  d->mode = header[H_MODE];
+  int bps = 0;
+  if (d->mode == MODE_SIMT) {
+    if (header[H_X_IN_LA] != 0) {
+      cudaFree(d->dev);
+      delete d;
+      return fail(GEAR_E_INVALID, "gear_dag_create: %s", "a box-per-thread program keeps the input's A in its buffers");
+    }
+    // per-CTA scratch: SIMT_T boxes, every per-box item box-interleaved
+    d->threads = SIMT_T;
+    d->boxes_per_slot = SIMT_T;
+    const int64_t items = 3 * (int64_t)header[H_ARENA] + header[H_PLANES] + header[H_FOLDW] +
+                          4 * (int64_t)header[H_MAXW] + header[H_SIMT_BUF] + header[H_SIMT_ROWS];
+    d->slot_doubles = items * SIMT_T;
+    d->smem_bytes = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, crown_simt_kernel, SIMT_T, 0);
+  } else if (d->mode == MODE_CTA) {
+    // per-CTA scratch: lo, hi, mag arenas; planes; fold vectors; 4 node-wide temporaries
+    d->threads = NT;
+    d->boxes_per_slot = 1;
+    d->slot_doubles = 3 * (int64_t)header[H_ARENA] + header[H_PLANES] + header[H_FOLDW] + 4 * (int64_t)header[H_MAXW] + 8;
+    d->slot_doubles = (d->slot_doubles + 31) / 32 * 32;
+    d->smem_bytes = header[H_SMEM] * (int)sizeof(double);
+    if (d->smem_bytes > (int)prop.sharedMemPerBlockOptin) {
+      cudaFree(d->dev);
+      delete d;
+      return fail(GEAR_E_INVALID, "gear_dag_create: %s", "pass working set exceeds shared memory");
+    }
+    e = cudaFuncSetAttribute(crown_megakernel, cudaFuncAttributeMaxDynamicSharedMemorySize, d->smem_bytes);
+    if (e != cudaSuccess) { cudaFree(d->dev); delete d; return cuda_fail(e, "cudaFuncSetAttribute"); }
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, crown_megakernel, NT, d->smem_bytes);
+  } else {
     cudaFree(d->dev);
     delete d;
-    return fail(GEAR_E_INVALID, "gear_dag_create: %s", "pass working set exceeds shared memory");
+    return fail(GEAR_E_INVALID, "gear_dag_create: %s", "unknown execution mode");
   }
-  e = cudaFuncSetAttribute(gear::crown_megakernel, cudaFuncAttributeMaxDynamicSharedMemorySize, d->smem_bytes);
-  if (e != cudaSuccess) { cudaFree(d->dev); delete d; return cuda_fail(e, "cudaFuncSetAttribute"); }
-  d->num_sms = prop.multiProcessorCount;
-  int bps = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, gear::crown_megakernel, gear::NT, d->smem_bytes);
   if (e != cudaSuccess || bps < 1) bps = 1;
   d->blocks_per_sm = bps;
   *out = d;
@@ -116,10 +143,30 @@ extern "C" int gear_dag_destroy(gear_dag* dag) {
   return GEAR_OK;
 }
 
+// CTAs of one launch: every resident CTA, or fewer when the batch has fewer boxes (CTA mode)
+// or tiles of SIMT_T boxes (SIMT mode)
 static int64_t slots_for(const gear_dag* d, int64_t batch) {
   int64_t slots = (int64_t)d->num_sms * d->blocks_per_sm;
-  if (batch < slots) slots = batch;
+  const int64_t units = (batch + d->boxes_per_slot - 1) / d->boxes_per_slot;
+  if (units < slots) slots = units;
   return slots < 1 ? 1 : slots;
+}
+
+static int launch_crown(const gear_dag* dag, const gear::Work& wk, int64_t slots, cudaStream_t stream) {
+  if (dag->mode == gear::MODE_SIMT) {
+    gear::crown_simt_kernel<<<(unsigned)slots, gear::SIMT_T, 0, stream>>>(dag->P, wk);
+    g_launches = 1;
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "crown_simt_kernel launch");
+  }
+  // the kernel's dynamic shared-memory limit is per function: set it for this program
+  cudaError_t ea = cudaFuncSetAttribute(gear::crown_megakernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        dag->smem_bytes);
+  if (ea != cudaSuccess) return cuda_fail(ea, "cudaFuncSetAttribute");
+  gear::crown_megakernel<<<(unsigned)slots, gear::NT, dag->smem_bytes, stream>>>(dag->P, wk);
+  g_launches = 1;
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "crown_megakernel launch");
 }
 
 extern "C" int64_t gear_crown_workspace_bytes(const gear_dag* dag, int64_t batch) {
@@ -136,7 +183,7 @@ extern "C" int gear_crown_lower(const gear_dag* dag, const double* x_L, const do
   if (!workspace || workspace_bytes < gear_crown_workspace_bytes(dag, batch))
     return fail(GEAR_E_WORKSPACE, "gear_crown_lower: %s", "workspace too small");
   if (dag->hdr[gear::H_RETA] == 0 && lA) return fail(GEAR_E_INVALID, "gear_crown_lower: %s", "program built without A");
-  if (dag->hdr[gear::H_RETA] != 0 && !lA)
+  if (dag->hdr[gear::H_RETA] != 0 && dag->hdr[gear::H_X_IN_LA] != 0 && !lA)
     return fail(GEAR_E_INVALID, "gear_crown_lower: %s", "this program accumulates A in the lA output: lA is required");
   gear::Work wk;
   wk.xL = x_L;
@@ -149,16 +196,7 @@ extern "C" int gear_crown_lower(const gear_dag* dag, const double* x_L, const do
   wk.slot_doubles = dag->slot_doubles;
   wk.B = batch;
   wk.status = nullptr;
-  int64_t slots = slots_for(dag, batch);
-  // the kernel's dynamic shared-memory limit is per function: set it for this program
-  cudaError_t ea = cudaFuncSetAttribute(gear::crown_megakernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        dag->smem_bytes);
-  if (ea != cudaSuccess) return cuda_fail(ea, "cudaFuncSetAttribute");
-  gear::crown_megakernel<<<(unsigned)slots, gear::NT, dag->smem_bytes, (cudaStream_t)stream>>>(dag->P, wk);
-  g_launches = 1;
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return cuda_fail(e, "crown_megakernel launch");
-  return GEAR_OK;
+  return launch_crown(dag, wk, slots_for(dag, batch), (cudaStream_t)stream);
 }
 
 // ------------------------------------------------------------------ no-allocation entry point
@@ -198,14 +236,14 @@ extern "C" int gear_crown_lower_static(const gear_dag* dag, const double* x_L, c
                                        const double* C, double* lb, double* lA, double* lbias, void* stream) {
   g_launches = 0;
   if (!dag || !x_L || !x_U || !lb || batch < 0) return fail(GEAR_E_INVALID, "gear_crown_lower_static: %s", "bad arguments");
-  if (dag->hdr[gear::H_RETA] != 0 && !lA)
+  if (dag->hdr[gear::H_RETA] != 0 && dag->hdr[gear::H_X_IN_LA] != 0 && !lA)
     return fail(GEAR_E_INVALID, "gear_crown_lower_static: %s", "this program accumulates A in the lA output: lA is required");
   if (batch == 0) return GEAR_OK;
   const int64_t slot_bytes = dag->slot_doubles * (int64_t)sizeof(double);
   const int64_t max_slots = kStaticScratchBytes / slot_bytes;
   if (max_slots < 1) {
     char msg[256];
-    snprintf(msg, sizeof(msg), "gear_crown_lower_static: one CTA of this program needs %lld bytes of scratch, "
+    snprintf(msg, sizeof(msg), "gear_crown_lower_static: one CTA slot of this program needs %lld bytes of scratch, "
              "more than the static %lld bytes; use gear_crown_lower with a workspace",
              (long long)slot_bytes, (long long)kStaticScratchBytes);
     g_err = msg;
@@ -227,13 +265,7 @@ extern "C" int gear_crown_lower_static(const gear_dag* dag, const double* x_L, c
   wk.slot_doubles = dag->slot_doubles;
   wk.B = batch;
   wk.status = nullptr;
-  cudaError_t ea = cudaFuncSetAttribute(gear::crown_megakernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        dag->smem_bytes);
-  if (ea != cudaSuccess) return cuda_fail(ea, "cudaFuncSetAttribute");
-  gear::crown_megakernel<<<(unsigned)slots, gear::NT, dag->smem_bytes, (cudaStream_t)stream>>>(dag->P, wk);
-  g_launches = 1;
-  cudaError_t e = cudaGetLastError();
-  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "crown_megakernel launch");
+  return launch_crown(dag, wk, slots, (cudaStream_t)stream);
 }
 
 // ------------------------------------------------------------------ branch and bound

@@ -39,8 +39,13 @@ constexpr int RED_SLOTS = 32;
 
 enum HeaderField {
   H_NNODES = 0, H_NSTEPS, H_NPASSES, H_NOPS, H_N, H_S, H_T, H_ARENA, H_PLANES, H_FOLDW,
-  H_SMEM, H_MAXS, H_SINOFF, H_MAXW, H_RETA, H_MAXOPS, HEADER_LEN = 16
+  H_SMEM, H_MAXS, H_SINOFF, H_MAXW, H_RETA, H_MAXOPS, H_SIMT_BUF, H_SIMT_ROWS, H_X_IN_LA, H_MODE,
+  HEADER_LEN = 20
 };
+
+// execution model of a program: one box per CTA (pass working set in shared memory) or one box
+// per thread (per-box state box-interleaved in global scratch)
+enum ExecMode { MODE_CTA = 0, MODE_SIMT = 1 };
 
 // Sin/cos table layout inside the float64 pool, from H_SINOFF (gear_b200/tables.py order).
 constexpr int SIN_N_PRE = 162;   // int(pi/2 / 0.01) + 5

@@ -15,11 +15,13 @@ from .program import Program
 class CrownEngine:
     """One graph and one specification kind (identity or dense C) on the current device."""
 
-    def __init__(self, graph: Graph, spec_rows: Optional[int] = None, dense_c: bool = False):
+    def __init__(self, graph: Graph, spec_rows: Optional[int] = None, dense_c: bool = False, mode: str = "cta"):
+        """mode: "cta" (one box per CTA) or "simt" (one box per thread); both give the same bounds."""
         if not torch.cuda.is_available():
             raise _lib.GearError("gear_b200 needs a CUDA device (no CPU fallback)")
         self.graph = graph
-        self.prog = Program(graph, spec_rows=spec_rows, dense_c=dense_c)
+        self.mode = mode
+        self.prog = Program(graph, spec_rows=spec_rows, dense_c=dense_c, mode=mode)
         p = self.prog
         L = _lib.lib()
         h = ctypes.c_void_p()

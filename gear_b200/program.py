@@ -47,6 +47,7 @@ N_KIND, N_W, N_NIN, N_IN0, N_IN1, N_CUR, N_PLANE, N_CVEC, N_MAP0, N_MAP1, N_W_OF
     N_WIN, N_INS, N_FOLD, N_INEXACT = range(16)
 
 # ---- steps
+MODES = {"cta": 0, "simt": 1}          # ExecMode in gear_program.h
 ST = {"ibp": 0, "mag": 1, "relax": 2, "pass": 3, "compare": 4, "fold": 5, "final": 6}
 STEP_REC = 4
 
@@ -118,7 +119,15 @@ class Program:
     """Compiled device program for one graph and one final specification shape."""
 
     def __init__(self, graph: Graph, spec_rows: Optional[int] = None, dense_c: bool = False,
-                 return_a: bool = True, smem_limit: int = 200 * 1024):
+                 return_a: bool = True, smem_limit: int = 200 * 1024, mode: str = "cta"):
+        """mode: "cta" runs one box per CTA with the pass working set in shared memory, and the
+        final pass accumulates the input's A directly in the lA output; "simt" runs one box per
+        thread with every per-box array box-interleaved in global scratch, and writes lA from the
+        pass buffers at the end."""
+        if mode not in MODES:
+            raise ProgramError(f"unknown execution mode {mode!r}")
+        self.mode = mode
+        self.x_in_la = mode == "cta"
         self.g = graph
         self.n = graph[0].width
         t = graph.output
@@ -429,13 +438,17 @@ class Program:
         self.int_pool = self.pools.int_array()
         self.dbl_pool = self.pools.dbl_array()
         max_ops = max((int(r[P_NOP]) for r in self.pass_recs), default=0)
+        # box-per-thread kernel: per-box scratch items (pass buffers and row arrays in global memory)
+        self.simt_buf = max((int(r[P_SIDES]) * int(r[P_SMEM]) for r in self.pass_recs), default=1)
+        self.simt_rows = max((int(r[P_SIDES]) * 3 * int(r[P_S]) for r in self.pass_recs), default=1)
         # shared memory: pass working set + staged node table + staged op records (in doubles)
         stage = (len(self.g) * NODE_REC + max_ops * OP_REC + 1) // 2 + 2
         self.smem_total = self.max_smem + stage
         self.header = np.array([len(self.g), len(self.steps), len(self.passes), len(self.op_recs),
                                 self.n, self.S, self.t, self.arena_w, self.plane_w, self.fold_w,
                                 self.smem_total, self.max_S, self.sin_off, self.maxw,
-                                1 if self.return_a else 0, max_ops], dtype=np.int32)
+                                1 if self.return_a else 0, max_ops, self.simt_buf, self.simt_rows,
+                                1 if self.x_in_la else 0, MODES[self.mode]], dtype=np.int32)
 
     def _emit_pass(self, pid, pi: PassInfo):
         g = self.g
@@ -463,7 +476,7 @@ class Program:
             for p in g[v].inputs:
                 if p not in first_use:
                     first_use[p] = i
-        xdense = pi.final and self.return_a and not fold and 0 in pats
+        xdense = pi.final and self.return_a and self.x_in_la and not fold and 0 in pats
         if not fold:
             last_use[0] = len(pi.order)
         free, bufoff, top = [], {}, 0
@@ -608,8 +621,8 @@ class Program:
         rec[P_XDENSE] = 1 if xdense else 0
         rec[P_TMAXROW] = int(np.diff(rowptr[pi.t]).max(initial=0))
         self.pass_recs.append(rec)
-        # kernel shared memory: per side 7 row arrays (S) + the entry buffers
-        self.max_smem = max(self.max_smem, pi.sides * (7 * S + smem) + 32)
+        # kernel shared memory: per side 3 row arrays (S) + the entry buffers
+        self.max_smem = max(self.max_smem, pi.sides * (3 * S + smem) + 32)
         self.max_S = max(self.max_S, S)
         pi.bufoff = bufoff
         pi.fold = fold

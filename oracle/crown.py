@@ -626,22 +626,26 @@ class CrownOracle:
             Ax = A.get(0, [None, None])[side]
             if Ax is None:
                 Ax = np.zeros((S, B, nin))
-            b = bias[side]
-            b = widen(b, rounding_error(bias_mag[side], max(nvisit, 1) + nin), sign)
+            # combined outward rounding: every magnitude is scaled by its rounding factor and
+            # added to one error term (bias sums over visits + n terms, the box dot over n terms)
+            f_bias = (max(nvisit, 1) + nin + 16) * EPS * 4
+            f_box = (nin + 16) * EPS * 4
             base = np.einsum("sbx,bx->sb", Ax, x0)
             dev = np.einsum("sbx,bx->sb", np.abs(Ax), eps)
-            root = base + sign * dev
-            berr = rounding_error(np.einsum("sbx,bx->sb", finite_abs(Ax), maxabs), nin)
-            root = widen(root, berr, sign)
-            root = np.where(np.isfinite(root), root, sign * np.inf)
-            tot = b + root
-            tot = widen(tot, rounding_error(finite_abs(tot), 1) + err[side], sign)
-            tot = np.where(undef[side], sign * np.inf, tot)
+            bmag = np.einsum("sbx,bx->sb", finite_abs(Ax), maxabs)
+            val = bias[side] + base
+            errt = err[side] + bias_mag[side] * f_bias + bmag * f_box + dev
+            with np.errstate(invalid="ignore"):
+                tot = val + sign * (errt + (np.abs(val) + errt) * (17 * EPS * 4))
+            bad = undef[side] | np.isnan(tot) | (tot == -sign * np.inf)
+            tot = np.where(bad, sign * np.inf, tot)
+            undef[side] = bad
             res[side] = tot.T.copy()
-            Ax = np.where(undef[side][:, :, None], 0.0, Ax)
+            root = base + sign * dev
+            Ax = np.where(bad[:, :, None], 0.0, Ax)
             # save_root_A (backward_bound.py:1629): lbias = bound minus the root's term
             with np.errstate(invalid="ignore"):
-                lbias = np.where(undef[side], sign * np.inf, tot - root)
+                lbias = np.where(bad, sign * np.inf, tot - root)
             resA[side] = (Ax.transpose(1, 0, 2).copy(), lbias.T.copy())
         return res[0], res[1], resA, (undef[0].T.copy(), undef[1].T.copy())
 

@@ -1,0 +1,80 @@
+"""Box-per-thread CROWN kernel (crown_simt_kernel) against the float64 CPU oracle and against
+the box-per-CTA kernel. Tolerance: 1e-9 relative (same rounding model, same tie-break; the two
+kernels sum in different orders)."""
+import numpy as np
+import pytest
+import torch
+
+from golden_cases import cases, load
+from gear_b200 import BoundedModule, BoundedTensor, PerturbationLpNorm, problems
+from gear_b200.engine import CrownEngine
+from oracle.crown import CrownOracle
+
+pytestmark = pytest.mark.gpu
+RTOL = 1e-9
+
+
+def _close(a, b, rtol=RTOL):
+    a, b = np.asarray(a), np.asarray(b)
+    both_inf = np.isinf(a) & np.isinf(b) & (np.sign(a) == np.sign(b))
+    err = np.where(both_inf, 0.0, np.abs(a - b) / np.maximum(1.0, np.abs(b)))
+    return float(np.nanmax(err)) if err.size else 0.0
+
+
+@pytest.mark.parametrize("case", cases())
+def test_simt_matches_oracle_on_fixture_boxes(case):
+    m, g, d, inject = load(case)
+    eng = CrownEngine(g, mode="simt")
+    lo = torch.tensor(d["x_L"], device="cuda")
+    hi = torch.tensor(d["x_U"], device="cuda")
+    lb, lA, lbias = eng.lower(lo, hi)
+    torch.cuda.synchronize()
+    olb, _, olA, olbias = CrownOracle(g).compute_bounds(d["x_L"], d["x_U"], d["C"])
+    assert _close(lb.cpu().numpy(), olb) < RTOL
+    assert _close(lA.cpu().numpy(), olA) < RTOL
+    assert _close(lbias.cpu().numpy(), olbias) < RTOL
+
+
+# batches that are not a multiple of the 64-box tile exercise the tail threads
+@pytest.mark.parametrize("workload,batch", [("quad_exp_n10", 300), ("dense_q_n200", 70)])
+def test_simt_matches_oracle_random_boxes(workload, batch):
+    m = problems.make_instance(workload, 0)
+    lo, hi = problems.make_boxes(workload, batch, 0)
+    bm = BoundedModule(m, lo[:2], device="cuda", bound_opts={"gear_mode": "simt"})
+    x = BoundedTensor(lo.cuda(), PerturbationLpNorm(x_L=lo.cuda(), x_U=hi.cuda()))
+    S = bm.final_node_width()
+    C = torch.eye(S, dtype=torch.float64).expand(batch, S, S)
+    lb, _, A = bm.compute_bounds(x=(x,), C=C.cuda(), method="CROWN", bound_upper=False, return_A=True)
+    rec = A[bm.output_name[0]][bm.input_name[0]]
+    olb, _, olA, olbias = CrownOracle(bm.graph).compute_bounds(lo.numpy(), hi.numpy(), C.numpy())
+    assert _close(lb.cpu().numpy(), olb) < RTOL
+    assert _close(rec["lA"].cpu().numpy(), olA) < RTOL
+    assert _close(rec["lbias"].cpu().numpy(), olbias) < RTOL
+
+
+def test_simt_dense_c_matches_oracle():
+    m = problems.make_instance("quad_exp_n10", 1)
+    lo, hi = problems.make_boxes("quad_exp_n10", 32, 1)
+    g = torch.Generator().manual_seed(3)
+    C = torch.randn(32, 2, 3, generator=g, dtype=torch.float64)
+    bm = BoundedModule(m, lo[:2], device="cuda", bound_opts={"gear_mode": "simt"})
+    x = BoundedTensor(lo.cuda(), PerturbationLpNorm(x_L=lo.cuda(), x_U=hi.cuda()))
+    lb, _, A = bm.compute_bounds(x=(x,), C=C.cuda(), method="CROWN", bound_upper=False, return_A=True)
+    olb, _, olA, _ = CrownOracle(bm.graph).compute_bounds(lo.numpy(), hi.numpy(), C.numpy())
+    assert _close(lb.cpu().numpy(), olb) < RTOL
+    assert _close(A["/y"]["/x"]["lA"].cpu().numpy(), olA) < RTOL
+
+
+@pytest.mark.parametrize("workload,batch", [("quad_exp_n10", 4096), ("dense_q_n200", 1000),
+                                            ("dense_a_n2048", 64)])
+def test_simt_matches_cta_kernel(workload, batch):
+    m = problems.make_instance(workload, 0)
+    lo, hi = problems.make_boxes(workload, batch, 0)
+    from gear_b200 import graph
+    g = graph.trace(m, lo[:2])
+    xL, xU = lo.cuda(), hi.cuda()
+    a = CrownEngine(g, mode="cta").lower(xL, xU)
+    b = CrownEngine(g, mode="simt").lower(xL, xU)
+    torch.cuda.synchronize()
+    for x, y in zip(a, b):
+        assert _close(y.cpu().numpy(), x.cpu().numpy()) < RTOL
