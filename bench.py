@@ -161,8 +161,9 @@ def main():
     ap.add_argument("--impl", default="gear", choices=["gear", "reference"])
     ap.add_argument("--cpu-per-core", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="cta", choices=["cta", "simt"],
-                    help="CROWN kernel: one box per CTA or one box per thread")
+    ap.add_argument("--mode", default="auto", choices=["auto", "cta", "simt"],
+                    help="CROWN kernel: one box per CTA, one box per thread, or the faster one timed on the "
+                         "first (warm-up) call")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -199,6 +200,7 @@ def main():
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    variant = eng.variant(B)
 
     def barrier():
         if world > 1:
@@ -269,13 +271,14 @@ def main():
         res = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-               "config": {"workload": WORKLOAD, "batch": B, "n": n, "spec_rows": S, "kernel_mode": args.mode,
+               "config": {"workload": WORKLOAD, "batch": B, "n": n, "spec_rows": S, "kernel_mode": args.mode, "kernel_variant": variant,
+                          "variant_ms": eng.timings.get(eng._bucket(B)),
                           "parallelism": f"replicas{world}",
                           "l2": "inputs (x_L, x_U) and outputs (lA) larger than the 126 MB L2"},
                "gpu_launches": launches,
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "traffic": traffic,
-                            "kernel": "crown_megakernel" if args.mode == "cta" else "crown_simt_kernel",
+                            "kernel": "crown_simt_kernel" if variant == "simt" else f"crown_megakernel<{variant[3:]}>",
                             "peak_source": peak_kind},
                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * B * n * 8,
                        "d2h_bytes_per_step": B * S * 8},

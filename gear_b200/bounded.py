@@ -89,7 +89,7 @@ class BoundedModule:
         if eng is None:
             with torch.cuda.device(self.device):
                 eng = CrownEngine(self.graph, spec_rows=spec_rows, dense_c=dense_c,
-                                  mode=self.bound_opts.get("gear_mode", "cta"))
+                                  mode=self.bound_opts.get("gear_mode", "auto"))
             self._engines[key] = eng
         return eng
 

@@ -38,8 +38,8 @@ constexpr double UNIT = EPS / 2;
 constexpr double EPSILON = 1e-12;               // operators/base.py:32
 constexpr double TIE_TOL = 1e-12;               // McCormick tie tolerance (see program.py)
 constexpr double STEP_PRE = 0.01;
-constexpr int NT = 64;                          // threads per CTA (one box per CTA)
-constexpr int NWARP = NT / 32;
+// The box-per-CTA kernel is instantiated for 64, 128 and 256 threads per CTA (template
+// parameter NT of every function below that splits work over the CTA); the program picks one.
 
 // sin/cos table offsets (gear_b200/tables.py SIN_TABLE_ORDER)
 constexpr int T_DL = 0, T_DU = SIN_N_PRE, T_XLLD = 2 * SIN_N_PRE, T_XLLC = T_XLLD + SIN_N_TB,
@@ -446,7 +446,9 @@ __device__ __forceinline__ void ibp_element(const Box& bx, const int32_t* nd, in
 }
 
 // Linear / MatMul interval (interval_bound + BoundLinear._bound_box): warp per output row.
+template <int NT>
 __device__ void ibp_linear(const Box& bx, const int32_t* nd, double* olo, double* ohi) {
+  constexpr int NWARP = NT / 32;
   const DevProgram* P = bx.P;
   int w = nd[N_W], win = nd[N_WIN];
   const double* W = P->dp + nd[N_W_OFF];
@@ -498,11 +500,13 @@ __device__ void ibp_linear(const Box& bx, const int32_t* nd, double* olo, double
   }
 }
 
+template <int NT>
 __device__ void ibp_node(const Box& bx, int v, double* olo, double* ohi) {
+  constexpr int NWARP = NT / 32;
   const int32_t* nd = node_rec(bx.P, v);
   int kind = nd[N_KIND];
   if (kind == NK_LINEAR || kind == NK_MATMUL) {
-    ibp_linear(bx, nd, olo, ohi);
+    ibp_linear<NT>(bx, nd, olo, ohi);
     return;
   }
   if (kind == NK_REDUCESUM) {
@@ -529,29 +533,55 @@ __device__ void ibp_node(const Box& bx, int v, double* olo, double* ohi) {
   for (int j = threadIdx.x; j < w; j += NT) ibp_element(bx, nd, j, olo + j, ohi + j);
 }
 
-// fold vectors of a linear/matmul on the input: W x0, |W| eps, |W| max(|xL|, |xU|)
-__device__ void fold_node(const Box& bx, int v) {
+// fold vectors of a linear/matmul on the input: W x0, |W| eps, |W| max(|xL|, |xU|). The box's
+// centre, radius and magnitude are staged in shared memory (`stage`, 3 win doubles); each thread
+// owns outputs j and reads column j of the transposed weights (coalesced across the threads).
+template <int NT>
+__device__ void fold_node(const Box& bx, int v, double* stage) {
   const DevProgram* P = bx.P;
   const int32_t* nd = node_rec(P, v);
-  int w = nd[N_W], win = nd[N_WIN];
-  const double* W = P->dp + nd[N_W_OFF];
+  const int w = nd[N_W], win = nd[N_WIN];
+  const double* Wt = P->dp + nd[N_WT_OFF];
   double* f = bx.fold + nd[N_FOLD];
-  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int j = warp; j < w; j += NWARP) {
-    const double* Wr = W + (int64_t)j * win;
+  double* xc = stage;
+  double* xr = stage + win;
+  double* xm = stage + 2 * win;
+  for (int i = threadIdx.x; i < win; i += NT) {
+    const double l = bx.xL[i], h = bx.xU[i];
+    xc[i] = (h + l) / 2.0;
+    xr[i] = (h - l) / 2.0;
+    xm[i] = finite_abs(fmax(fabs(l), fabs(h)));
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < w; j += NT) {
+    const double* col = Wt + j;
     double c = 0, r = 0, t = 0;
-    for (int i = lane; i < win; i += 32) {
-      double wv = Wr[i];
-      double l = bx.xL[i], h = bx.xU[i];
-      c += ((h + l) / 2.0) * wv;
-      r += ((h - l) / 2.0) * fabs(wv);
-      t += finite_abs(fmax(fabs(l), fabs(h))) * fabs(wv);
+    int i = 0;
+    for (; i + 4 <= win; i += 4) {
+      double wv[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) wv[q] = __ldg(col + (int64_t)(i + q) * w);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double aw = fabs(wv[q]);
+        c += xc[i + q] * wv[q];
+        r += xr[i + q] * aw;
+        t += xm[i + q] * aw;
+      }
     }
-    c = warp_sum(c); r = warp_sum(r); t = warp_sum(t);
-    if (lane == 0) { f[j] = c; f[w + j] = r; f[2 * w + j] = t; }
+    for (; i < win; ++i) {
+      const double wv = __ldg(col + (int64_t)i * w), aw = fabs(wv);
+      c += xc[i] * wv;
+      r += xr[i] * aw;
+      t += xm[i] * aw;
+    }
+    f[j] = c;
+    f[w + j] = r;
+    f[2 * w + j] = t;
   }
 }
 
+template <int NT>
 __device__ void relax_node(const Box& bx, int v) {
   const DevProgram* P = bx.P;
   const int32_t* nd = node_rec(P, v);
@@ -604,13 +634,14 @@ constexpr double RE1 = 17 * EPS * 4;   // rounding_error(x, 1) / x
 struct PassCtx {
   const int32_t* pr;
   int S, sides;
-  double* rows;      // [side][R_COUNT][S]
+  double* rows;      // [side][nrows][S]: VAL, ERR (+ ROOT in the final pass)
+  int nrows;
   double* red;       // RED_SLOTS reduction slots
   double* buf;       // [side][smem]
   double* la;        // this box's lA block (S x n) when the input's A lives there
   int32_t* stage_ops;
   int smem;
-  __device__ double* row(int side, int what) const { return rows + ((size_t)side * R_COUNT + what) * S; }
+  __device__ double* row(int side, int what) const { return rows + ((size_t)side * nrows + what) * S; }
   __device__ double* vals(int side, int off) const {
     return off == ROOT_IN_LA ? la : buf + (size_t)side * smem + off;
   }
@@ -621,7 +652,9 @@ struct RowSplit {
   int first, step, eoff, estep;
   bool warp;
 };
+template <int NT>
 __device__ __forceinline__ RowSplit row_split(int maxrow) {
+  constexpr int NWARP = NT / 32;
   RowSplit r;
   r.warp = maxrow > ROW_THREAD_MAX;
   r.first = r.warp ? (int)(threadIdx.x >> 5) : (int)threadIdx.x;
@@ -660,7 +693,9 @@ __device__ __forceinline__ double elem_coef(int kind, int slot, int side, double
   }
 }
 
+template <int NT>
 __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops, const Work& wk) {
+  constexpr int NWARP = NT / 32;
   const DevProgram* P = bx.P;
   const int32_t* pr = P->passes + pid * PASS_REC;
   PassCtx ctx;
@@ -669,7 +704,8 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
   ctx.sides = pr[P_SIDES];
   ctx.smem = pr[P_SMEM];
   ctx.rows = sm;
-  ctx.red = sm + (size_t)ctx.sides * R_COUNT * ctx.S;
+  ctx.nrows = pr[P_FINAL] != 0 ? R_COUNT : R_COUNT - 1;
+  ctx.red = sm + (size_t)ctx.sides * ctx.nrows * ctx.S;
   ctx.buf = ctx.red + RED_SLOTS;
   const bool xdense = pr[P_XDENSE] != 0;
   ctx.la = xdense ? wk.lA + (size_t)bx.b * ctx.S * P->hdr[H_N] : nullptr;
@@ -682,7 +718,7 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
   const double fbox = ((double)n + 16) * EPS * 4;                             // box dot products
   const int32_t* tnd = node_rec(P, t);
 
-  for (int k = tid; k < sides * R_COUNT * S; k += NT) ctx.rows[k] = 0.0;
+  for (int k = tid; k < sides * ctx.nrows * S; k += NT) ctx.rows[k] = 0.0;
   // initial A at t
   {
     const int32_t* trp = P->ip + pr[P_TRP];
@@ -896,25 +932,57 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
             continue;
           }
           double part = 0, pmerge = 0;
-          for (int j = eoff; j < win; j += estep) {
-            double acc0 = 0, acc1 = 0, ab0 = 0, ab1 = 0;
-            int e = e0;
-            for (; e + 1 < e1; e += 2) {
-              double a0 = V[e], a1 = V[e + 1];
-              double w0 = W[(int64_t)vcols[e] * win + j], w1 = W[(int64_t)vcols[e + 1] * win + j];
-              acc0 += a0 * w0; acc1 += a1 * w1;
-              ab0 += fabs(a0) * fabs(w0); ab1 += fabs(a1) * fabs(w1);
+          // JB columns per thread per sweep of the row's entries: their weight loads are in
+          // flight together instead of one dependent load chain per column
+          constexpr int JB = 4;
+          for (int jb = eoff; jb < win; jb += JB * estep) {
+            double acc[JB], ab[JB];
+            bool ok[JB];
+#pragma unroll
+            for (int q = 0; q < JB; ++q) { acc[q] = 0.0; ab[q] = 0.0; ok[q] = jb + q * estep < win; }
+            // entries in chunks of EB: their indices and coefficients first, then EB x JB weight
+            // loads in flight together, then the sums (in entry order)
+            constexpr int EB = 4;
+            for (int e = e0; e < e1; e += EB) {
+              int cq[EB];
+              double aq[EB];
+#pragma unroll
+              for (int r = 0; r < EB; ++r) {
+                const bool in = e + r < e1;
+                cq[r] = in ? __ldg(vcols + e + r) : 0;
+                aq[r] = in ? V[e + r] : 0.0;
+              }
+              double wq[EB][JB];
+#pragma unroll
+              for (int r = 0; r < EB; ++r) {
+                const double* Wr = W + (int64_t)cq[r] * win + jb;
+#pragma unroll
+                for (int q = 0; q < JB; ++q) wq[r][q] = (ok[q] && e + r < e1) ? __ldg(Wr + q * estep) : 0.0;
+              }
+#pragma unroll
+              for (int r = 0; r < EB; ++r) {
+                if (e + r >= e1) break;
+#pragma unroll
+                for (int q = 0; q < JB; ++q) {
+                  acc[q] += aq[r] * wq[r][q];
+                  ab[q] += fabs(aq[r]) * fabs(wq[r][q]);
+                }
+              }
             }
-            if (e < e1) {
-              double a0 = V[e], w0 = W[(int64_t)vcols[e] * win + j];
-              acc0 += a0 * w0; ab0 += fabs(a0) * fabs(w0);
+            double mq[JB], uq[JB];
+#pragma unroll
+            for (int q = 0; q < JB; ++q) {
+              mq[q] = ok[q] ? mu[jb + q * estep] : 0.0;
+              uq[q] = (ok[q] && !zero_u) ? Ur[jb + q * estep] : 0.0;
             }
-            double acc = acc0 + acc1;
-            Ur[j] = zero_u ? acc : Ur[j] + acc;
-            double m = mu[j];
-            double mf = isinf(m) ? 0.0 : m;
-            part += (ab0 + ab1) * mf;
-            pmerge += fabs(acc) * mf;
+#pragma unroll
+            for (int q = 0; q < JB; ++q) {
+              if (!ok[q]) continue;
+              Ur[jb + q * estep] = zero_u ? acc[q] : uq[q] + acc[q];
+              const double mf = isinf(mq[q]) ? 0.0 : mq[q];
+              part += ab[q] * mf;
+              pmerge += fabs(acc[q]) * mf;
+            }
           }
           double tot_ = gk * warp_sum(part) + gmerge * warp_sum(pmerge);
           if (block_rows) {
@@ -951,26 +1019,44 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
   const int32_t* xrp = (!fold && xnnz > 0) ? P->ip + pr[P_XRP] : nullptr;
   const int32_t* xcols = (!fold && xnnz > 0) ? P->ip + pr[P_XCOLS] : nullptr;
   if (xrp) {
-    const RowSplit rs = row_split(pr[P_XMAXROW]);
+    const RowSplit rs = row_split<NT>(pr[P_XMAXROW]);
     for (int side = 0; side < sides; ++side) {
       const double* V = ctx.vals(side, pr[P_XBUF]);
       const double sign = side == 0 ? -1.0 : 1.0;
       for (int s = rs.first; s < S; s += rs.step) {
         int e0 = xrp[s], e1 = xrp[s + 1];
         double bs = 0, dv = 0, be = 0;
-        for (int e = e0 + rs.eoff; e < e1; e += rs.estep) {
-          int c = xcols[e];
-          double a = xdense ? V[(size_t)s * n + c] : V[e];
-          double l = bx.xL[c], h = bx.xU[c];
-          bs += a * ((h + l) / 2.0);
-          dv += fabs(a) * ((h - l) / 2.0);
-          be += finite_abs(a) * finite_abs(fmax(fabs(l), fabs(h)));
+        constexpr int XB = 8;
+        // XB entries per step: index, coefficient and box loads issued before the sums
+        for (int e = e0 + rs.eoff; e < e1; e += XB * rs.estep) {
+          int cq[XB];
+          bool ok[XB];
+#pragma unroll
+          for (int q = 0; q < XB; ++q) {
+            ok[q] = e + q * rs.estep < e1;
+            cq[q] = ok[q] ? __ldg(xcols + e + q * rs.estep) : 0;
+          }
+          double aq[XB], lq[XB], hq[XB];
+#pragma unroll
+          for (int q = 0; q < XB; ++q) {
+            aq[q] = ok[q] ? (xdense ? V[(size_t)s * n + cq[q]] : V[e + q * rs.estep]) : 0.0;
+            lq[q] = ok[q] ? bx.xL[cq[q]] : 0.0;
+            hq[q] = ok[q] ? bx.xU[cq[q]] : 0.0;
+          }
+#pragma unroll
+          for (int q = 0; q < XB; ++q) {
+            if (!ok[q]) continue;
+            const double a = aq[q], l = lq[q], h = hq[q];
+            bs += a * ((h + l) / 2.0);
+            dv += fabs(a) * ((h - l) / 2.0);
+            be += finite_abs(a) * finite_abs(fmax(fabs(l), fabs(h)));
+          }
         }
         if (rs.warp) { bs = warp_sum(bs); dv = warp_sum(dv); be = warp_sum(be); }
         if (!rs.warp || lane == 0) {
           ctx.row(side, R_VAL)[s] += bs;
           ctx.row(side, R_ERR)[s] += dv + be * fbox;
-          ctx.row(side, R_ROOT)[s] = bs + sign * dv;
+          if (ctx.nrows > R_ROOT) ctx.row(side, R_ROOT)[s] = bs + sign * dv;
         }
       }
     }
@@ -1037,11 +1123,12 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
 
 __device__ __forceinline__ double magnitude(double l, double h) { return l > h ? INFINITY : fmax(-l, h); }
 
+template <int NT>
 __device__ void compare_node(const Box& bx, int v, double* tmp_lo, double* tmp_hi, bool with_mag) {
   // IBP of v from its inputs' current intervals, intersected with the pass result
   const int32_t* nd = node_rec(bx.P, v);
   int w = nd[N_W];
-  ibp_node(bx, v, tmp_lo, tmp_hi);
+  ibp_node<NT>(bx, v, tmp_lo, tmp_hi);
   __syncthreads();
   for (int j = threadIdx.x; j < w; j += NT) {
     double l = nan_lo(bx.pres_lo[j]), h = nan_hi(bx.pres_hi[j]);
@@ -1053,7 +1140,8 @@ __device__ void compare_node(const Box& bx, int v, double* tmp_lo, double* tmp_h
 }
 
 
-__global__ void __launch_bounds__(NT, 12) crown_megakernel(DevProgram Pg, Work wk) {
+template <int NT>
+__global__ void __launch_bounds__(NT, 768 / NT) crown_megakernel(DevProgram Pg, Work wk) {
   extern __shared__ double sm[];
   const int32_t* hdr = Pg.hdr;
   // shared memory: [pass working set | node table | op records of the running pass]
@@ -1092,10 +1180,10 @@ __global__ void __launch_bounds__(NT, 12) crown_megakernel(DevProgram Pg, Work w
       const int32_t* st = P.steps + si * STEP_REC;
       const int type = st[0], a = st[1];
       switch (type) {
-        case ST_FOLD: fold_node(bx, a); break;
+        case ST_FOLD: fold_node<NT>(bx, a, sm); break;
         case ST_IBP: {
           const int32_t* nd = node_rec(&P, a);
-          ibp_node(bx, a, tmp_lo, tmp_hi);
+          ibp_node<NT>(bx, a, tmp_lo, tmp_hi);
           __syncthreads();
           const bool with_mag = st[2] != 0;
           for (int j = threadIdx.x; j < nd[N_W]; j += NT) {
@@ -1112,9 +1200,9 @@ __global__ void __launch_bounds__(NT, 12) crown_megakernel(DevProgram Pg, Work w
           }
           break;
         }
-        case ST_RELAX: relax_node(bx, a); break;
-        case ST_PASS: case ST_FINAL: run_pass(bx, a, sm, sops, wk); break;
-        case ST_COMPARE: compare_node(bx, a, tmp_lo, tmp_hi, st[3] != 0); break;
+        case ST_RELAX: relax_node<NT>(bx, a); break;
+        case ST_PASS: case ST_FINAL: run_pass<NT>(bx, a, sm, sops, wk); break;
+        case ST_COMPARE: compare_node<NT>(bx, a, tmp_lo, tmp_hi, st[3] != 0); break;
         default: break;
       }
       __syncthreads();

@@ -100,25 +100,37 @@ __device__ void simt_ibp_node(const SBox& bx, int v, SView olo, SView ohi) {
 }
 
 __device__ void simt_fold_node(const SBox& bx, int v) {
-  // the input node's interval sits at arena offset 0: the box itself, box-interleaved
+  // the input node's interval sits at arena offset 0: the box itself, box-interleaved. JB
+  // outputs per sweep over the box, so the box is read w / JB times instead of w times.
   const DevProgram* P = bx.P;
   const int32_t* nd = node_rec(P, v);
   const int w = nd[N_W], win = nd[N_WIN];
   const double* W = P->dp + nd[N_W_OFF];
   SView f = bx.fold + nd[N_FOLD];
-  for (int j = 0; j < w; ++j) {
-    const double* Wr = W + (int64_t)j * win;
-    double c = 0, r = 0, t = 0;
+  constexpr int JB = 8;
+  for (int j0 = 0; j0 < w; j0 += JB) {
+    const int jn = min(JB, w - j0);
+    double c[JB], r[JB], t[JB];
+#pragma unroll
+    for (int q = 0; q < JB; ++q) { c[q] = 0.0; r[q] = 0.0; t[q] = 0.0; }
     for (int i = 0; i < win; ++i) {
-      double wv = __ldg(Wr + i), aw = fabs(wv);
-      double l = bx.lo[i], h = bx.hi[i];
-      c += ((h + l) / 2.0) * wv;
-      r += ((h - l) / 2.0) * aw;
-      t += finite_abs(fmax(fabs(l), fabs(h))) * aw;
+      const double l = bx.lo[i], h = bx.hi[i];
+      const double xc = (h + l) / 2.0, xr = (h - l) / 2.0, xm = finite_abs(fmax(fabs(l), fabs(h)));
+#pragma unroll
+      for (int q = 0; q < JB; ++q) {
+        if (q < jn) {
+          const double wv = __ldg(W + (int64_t)(j0 + q) * win + i), aw = fabs(wv);
+          c[q] += xc * wv;
+          r[q] += xr * aw;
+          t[q] += xm * aw;
+        }
+      }
     }
-    f[j] = c;
-    f[w + j] = r;
-    f[2 * w + j] = t;
+    for (int q = 0; q < jn; ++q) {
+      f[j0 + q] = c[q];
+      f[w + j0 + q] = r[q];
+      f[2 * w + j0 + q] = t[q];
+    }
   }
 }
 
@@ -330,10 +342,17 @@ __device__ void simt_run_pass(const SBox& bx, int pid, const Work& wk, bool live
                 }
               }
             }
-            for (int q = 0; q < jn; ++q) {
-              Ur[j0 + q] += acc[q];
-              const double m = mu[j0 + q];
-              const double mf = isinf(m) ? 0.0 : m;
+            double uq[JB], mq[JB];
+#pragma unroll
+            for (int q = 0; q < JB; ++q) {
+              uq[q] = q < jn ? Ur[j0 + q] : 0.0;
+              mq[q] = q < jn ? mu[j0 + q] : 0.0;
+            }
+#pragma unroll
+            for (int q = 0; q < JB; ++q) {
+              if (q >= jn) continue;
+              Ur[j0 + q] = uq[q] + acc[q];
+              const double mf = isinf(mq[q]) ? 0.0 : mq[q];
               part += ab[q] * mf;
               pmerge += fabs(acc[q]) * mf;
             }
@@ -397,13 +416,26 @@ __device__ void simt_run_pass(const SBox& bx, int pid, const Work& wk, bool live
       for (int s = 0; s < S; ++s) {
         const int e0 = __ldg(xrp + s), e1 = __ldg(xrp + s + 1);
         double bs = 0, dv = 0, be = 0;
-        for (int e = e0; e < e1; ++e) {
-          double a = V[e];
-          int c = __ldg(xcols + e);
-          double l = bx.lo[c], h = bx.hi[c];
-          bs += a * ((h + l) / 2.0);
-          dv += fabs(a) * ((h - l) / 2.0);
-          be += finite_abs(a) * finite_abs(fmax(fabs(l), fabs(h)));
+        // 4 entries per step: loads issued before the sums
+        for (int e = e0; e < e1; e += 4) {
+          int cq[4];
+          double aq[4], lq[4], hq[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) cq[q] = e + q < e1 ? __ldg(xcols + e + q) : 0;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            aq[q] = e + q < e1 ? V[e + q] : 0.0;
+            lq[q] = e + q < e1 ? bx.lo[cq[q]] : 0.0;
+            hq[q] = e + q < e1 ? bx.hi[cq[q]] : 0.0;
+          }
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            if (e + q >= e1) continue;
+            const double a = aq[q], l = lq[q], h = hq[q];
+            bs += a * ((h + l) / 2.0);
+            dv += fabs(a) * ((h - l) / 2.0);
+            be += finite_abs(a) * finite_abs(fmax(fabs(l), fabs(h)));
+          }
         }
         rval[s] += bs;
         rerr[s] += dv + be * fbox;

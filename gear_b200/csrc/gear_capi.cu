@@ -46,6 +46,30 @@ struct gear_dag {
   int64_t boxes_per_slot = 1;
 };
 
+// box-per-CTA kernel instances: dynamic shared-memory limit and resident CTAs per SM
+template <int NT>
+cudaError_t cta_occupancy_t(int smem_bytes, int* bps) {
+  cudaError_t e = cudaFuncSetAttribute(gear::crown_megakernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, gear::crown_megakernel<NT>, NT, smem_bytes);
+}
+static cudaError_t cta_occupancy(int threads, int smem_bytes, int* bps) {
+  switch (threads) {
+    case 64: return cta_occupancy_t<64>(smem_bytes, bps);
+    case 128: return cta_occupancy_t<128>(smem_bytes, bps);
+    case 256: return cta_occupancy_t<256>(smem_bytes, bps);
+    default: return cudaErrorInvalidValue;
+  }
+}
+template <int NT>
+cudaError_t cta_launch_t(const gear::DevProgram& P, const gear::Work& wk, int64_t slots, int smem_bytes, cudaStream_t st) {
+  // the kernel's dynamic shared-memory limit is per function: set it for this program
+  cudaError_t e = cudaFuncSetAttribute(gear::crown_megakernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+  if (e != cudaSuccess) return e;
+  gear::crown_megakernel<NT><<<(unsigned)slots, NT, smem_bytes, st>>>(P, wk);
+  return cudaGetLastError();
+}
+
 extern "C" const char* gear_last_error(void) { return g_err.c_str(); }
 extern "C" int gear_last_launch_count(void) { return g_launches; }
 
@@ -112,7 +136,7 @@ extern "C" int gear_dag_create(const int32_t* header, int64_t header_len, const 
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, crown_simt_kernel, SIMT_T, 0);
   } else if (d->mode == MODE_CTA) {
     // per-CTA scratch: lo, hi, mag arenas; planes; fold vectors; 4 node-wide temporaries
-    d->threads = NT;
+    d->threads = header[H_CTA_THREADS];
     d->boxes_per_slot = 1;
     d->slot_doubles = 3 * (int64_t)header[H_ARENA] + header[H_PLANES] + header[H_FOLDW] + 4 * (int64_t)header[H_MAXW] + 8;
     d->slot_doubles = (d->slot_doubles + 31) / 32 * 32;
@@ -122,9 +146,12 @@ extern "C" int gear_dag_create(const int32_t* header, int64_t header_len, const 
       delete d;
       return fail(GEAR_E_INVALID, "gear_dag_create: %s", "pass working set exceeds shared memory");
     }
-    e = cudaFuncSetAttribute(crown_megakernel, cudaFuncAttributeMaxDynamicSharedMemorySize, d->smem_bytes);
-    if (e != cudaSuccess) { cudaFree(d->dev); delete d; return cuda_fail(e, "cudaFuncSetAttribute"); }
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, crown_megakernel, NT, d->smem_bytes);
+    e = cta_occupancy(d->threads, d->smem_bytes, &bps);
+    if (e == cudaErrorInvalidValue) {
+      cudaFree(d->dev);
+      delete d;
+      return fail(GEAR_E_INVALID, "gear_dag_create: %s", "threads per CTA must be 64, 128 or 256");
+    }
   } else {
     cudaFree(d->dev);
     delete d;
@@ -159,13 +186,14 @@ static int launch_crown(const gear_dag* dag, const gear::Work& wk, int64_t slots
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "crown_simt_kernel launch");
   }
-  // the kernel's dynamic shared-memory limit is per function: set it for this program
-  cudaError_t ea = cudaFuncSetAttribute(gear::crown_megakernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        dag->smem_bytes);
-  if (ea != cudaSuccess) return cuda_fail(ea, "cudaFuncSetAttribute");
-  gear::crown_megakernel<<<(unsigned)slots, gear::NT, dag->smem_bytes, stream>>>(dag->P, wk);
+  cudaError_t e = cudaErrorInvalidValue;
+  switch (dag->threads) {
+    case 64: e = cta_launch_t<64>(dag->P, wk, slots, dag->smem_bytes, stream); break;
+    case 128: e = cta_launch_t<128>(dag->P, wk, slots, dag->smem_bytes, stream); break;
+    case 256: e = cta_launch_t<256>(dag->P, wk, slots, dag->smem_bytes, stream); break;
+    default: break;
+  }
   g_launches = 1;
-  cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "crown_megakernel launch");
 }
 

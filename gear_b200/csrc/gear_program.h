@@ -11,9 +11,10 @@ enum NodeKind {
   NK_SIN = 14, NK_COS = 15, NK_POW = 16, NK_REDUCESUM = 17, NK_MAP = 18, NK_CONCAT = 19
 };
 
+// N_WT_OFF: the weights of a linear/matmul node transposed, (in, out), for the forward products
 enum NodeField {
   N_KIND = 0, N_W, N_NIN, N_IN0, N_IN1, N_CUR, N_PLANE, N_CVEC, N_MAP0, N_MAP1, N_W_OFF, N_B_OFF,
-  N_WIN, N_INS, N_FOLD, N_INEXACT, NODE_REC
+  N_WIN, N_INS, N_FOLD, N_INEXACT, N_WT_OFF, NODE_REC
 };
 
 enum StepType { ST_IBP = 0, ST_MAG = 1, ST_RELAX = 2, ST_PASS = 3, ST_COMPARE = 4, ST_FOLD = 5, ST_FINAL = 6 };
@@ -33,14 +34,14 @@ enum OpField {
 // buffer offset marker: the input's A of a final pass accumulates in the lA output (row s at s * n)
 constexpr int ROOT_IN_LA = -2;
 // rows with at most this many entries are handled by one thread, longer rows by a warp
-constexpr int ROW_THREAD_MAX = 4;
+constexpr int ROW_THREAD_MAX = 16;
 // shared-memory reduction slots reserved after the row arrays
 constexpr int RED_SLOTS = 32;
 
 enum HeaderField {
   H_NNODES = 0, H_NSTEPS, H_NPASSES, H_NOPS, H_N, H_S, H_T, H_ARENA, H_PLANES, H_FOLDW,
   H_SMEM, H_MAXS, H_SINOFF, H_MAXW, H_RETA, H_MAXOPS, H_SIMT_BUF, H_SIMT_ROWS, H_X_IN_LA, H_MODE,
-  HEADER_LEN = 20
+  H_CTA_THREADS, H_R21, H_R22, H_R23, HEADER_LEN = 24
 };
 
 // execution model of a program: one box per CTA (pass working set in shared memory) or one box

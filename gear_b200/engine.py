@@ -12,33 +12,35 @@ from .graph import Graph
 from .program import Program
 
 
-class CrownEngine:
-    """One graph and one specification kind (identity or dense C) on the current device."""
+# kernel variants an "auto" engine chooses from: (execution mode, threads per CTA)
+VARIANTS = (("simt", 128), ("cta", 64), ("cta", 128), ("cta", 256))
+# the box-per-thread kernel keeps every per-box array in global memory: beyond this many
+# doubles per box it streams too much to compete, and "auto" does not try it
+SIMT_MAX_ITEMS = 65536
 
-    def __init__(self, graph: Graph, spec_rows: Optional[int] = None, dense_c: bool = False, mode: str = "cta"):
-        """mode: "cta" (one box per CTA) or "simt" (one box per thread); both give the same bounds."""
-        if not torch.cuda.is_available():
-            raise _lib.GearError("gear_b200 needs a CUDA device (no CPU fallback)")
-        self.graph = graph
-        self.mode = mode
-        self.prog = Program(graph, spec_rows=spec_rows, dense_c=dense_c, mode=mode)
+
+class _Dag:
+    """One compiled program uploaded to the device (a gear_dag handle)."""
+
+    def __init__(self, graph, spec_rows, dense_c, mode, cta_threads):
+        self.prog = Program(graph, spec_rows=spec_rows, dense_c=dense_c, mode=mode, cta_threads=cta_threads)
         p = self.prog
         L = _lib.lib()
         h = ctypes.c_void_p()
         arrs = [np.ascontiguousarray(a, dtype=np.int32) for a in
                 (p.header, p.node_arr, p.step_arr, p.pass_arr, p.op_arr, p.int_pool)]
         dbl = np.ascontiguousarray(p.dbl_pool, dtype=np.float64)
-        self._keep = (arrs, dbl)
         st = L.gear_dag_create(_lib.ptr_i32(arrs[0]), arrs[0].size, _lib.ptr_i32(arrs[1]), arrs[1].size,
                                _lib.ptr_i32(arrs[2]), arrs[2].size, _lib.ptr_i32(arrs[3]), arrs[3].size,
                                _lib.ptr_i32(arrs[4]), arrs[4].size, _lib.ptr_i32(arrs[5]), arrs[5].size,
                                _lib.ptr_dbl(dbl), dbl.size, ctypes.byref(h))
         _lib.check(st, "gear_dag_create")
         self.handle = h
-        self.n = p.n
-        self.S = p.S
-        self.dense_c = dense_c
-        self._ws = None
+        self.name = f"{mode}{cta_threads}" if mode == "cta" else mode
+
+    def simt_items(self):
+        p = self.prog
+        return 3 * p.arena_w + p.plane_w + p.fold_w + 4 * p.maxw + p.simt_buf + p.simt_rows
 
     def __del__(self):
         h = getattr(self, "handle", None)
@@ -49,11 +51,59 @@ class CrownEngine:
                 pass
             self.handle = None
 
+
+class CrownEngine:
+    """One graph and one specification kind (identity or dense C) on the current device.
+
+    mode "cta" runs one box per CTA (cta_threads threads), "simt" one box per thread; both
+    give the same bounds. mode "auto" times the kernel variants on the first call for each
+    batch size class (powers of two) on the caller's own boxes and keeps the fastest."""
+
+    def __init__(self, graph: Graph, spec_rows: Optional[int] = None, dense_c: bool = False, mode: str = "auto",
+                 cta_threads: int = 128):
+        if not torch.cuda.is_available():
+            raise _lib.GearError("gear_b200 needs a CUDA device (no CPU fallback)")
+        if mode not in ("auto", "cta", "simt"):
+            raise ValueError(f"unknown mode {mode!r}")
+        self.graph = graph
+        self.mode = mode
+        self.dense_c = dense_c
+        self._args = (graph, spec_rows, dense_c)
+        self._dags = {}
+        first = ("cta", cta_threads) if mode == "auto" else (mode, cta_threads)
+        d = self._dag(*first)
+        self.prog = d.prog
+        self.handle = d.handle
+        self.n = d.prog.n
+        self.S = d.prog.S
+        self._choice = {}          # batch size class -> variant
+        self.timings = {}          # batch size class -> {variant name: ms}
+        self._ws = None
+
+    def _dag(self, mode, threads):
+        key = (mode, threads if mode == "cta" else 0)
+        if key not in self._dags:
+            self._dags[key] = _Dag(*self._args, mode, threads)
+        return self._dags[key]
+
+    def _candidates(self):
+        items = self._dags[next(iter(self._dags))].simt_items()
+        return [(m, t) for m, t in VARIANTS if not (m == "simt" and items > SIMT_MAX_ITEMS)]
+
+    def variant(self, batch: int) -> str:
+        """Name of the kernel variant used for this batch size ("simt", "cta64", ...)."""
+        v = self._choice.get(self._bucket(batch))
+        if self.mode != "auto":
+            return self._dags[next(iter(self._dags))].name
+        return None if v is None else self._dag(*v).name
+
+    @staticmethod
+    def _bucket(batch):
+        return max(int(batch) - 1, 0).bit_length()
+
     def workspace(self, batch: int, device) -> torch.Tensor:
-        nbytes = int(_lib.lib().gear_crown_workspace_bytes(self.handle, batch))
-        if self._ws is None or self._ws.numel() < nbytes or self._ws.device != device:
-            self._ws = torch.empty(max(nbytes, 8), dtype=torch.uint8, device=device)
-        return self._ws
+        """Scratch for the current variant (self.handle) at this batch size."""
+        return self._workspace_bytes(int(_lib.lib().gear_crown_workspace_bytes(self.handle, batch)), device)
 
     def lower(self, x_L: torch.Tensor, x_U: torch.Tensor, C: Optional[torch.Tensor] = None,
               return_A: bool = True, out=None):
@@ -76,11 +126,47 @@ class CrownEngine:
             lbias = torch.empty(B, self.S, dtype=torch.float64, device=dev)
         else:
             lb, lA, lbias = out
-        ws = self.workspace(B, dev)
-        stream = torch.cuda.current_stream(dev).cuda_stream
-        st = _lib.lib().gear_crown_lower(self.handle, x_L.data_ptr(), x_U.data_ptr(), B,
-                                         C.data_ptr() if self.dense_c else None,
-                                         lb.data_ptr(), lA.data_ptr(),
-                                         lbias.data_ptr(), ws.data_ptr(), ws.numel(), stream)
-        _lib.check(st, "gear_crown_lower")
+        dag = self._select(x_L, x_U, C, lb, lA, lbias) if self.mode == "auto" else self._dags[next(iter(self._dags))]
+        self._launch(dag, x_L, x_U, C, lb, lA, lbias)
         return lb, (lA if return_A else None), lbias
+
+    def _launch(self, dag, x_L, x_U, C, lb, lA, lbias):
+        B = x_L.shape[0]
+        L = _lib.lib()
+        nbytes = int(L.gear_crown_workspace_bytes(dag.handle, B))
+        ws = self._workspace_bytes(nbytes, x_L.device)
+        stream = torch.cuda.current_stream(x_L.device).cuda_stream
+        st = L.gear_crown_lower(dag.handle, x_L.data_ptr(), x_U.data_ptr(), B,
+                                C.data_ptr() if self.dense_c else None,
+                                lb.data_ptr(), lA.data_ptr(), lbias.data_ptr(), ws.data_ptr(), ws.numel(), stream)
+        _lib.check(st, "gear_crown_lower")
+
+    def _select(self, x_L, x_U, C, lb, lA, lbias):
+        """The variant for this batch size class; timed on these boxes the first time."""
+        B = x_L.shape[0]
+        key = self._bucket(B)
+        if key not in self._choice:
+            times = {}
+            for cand in self._candidates():
+                dag = self._dag(*cand)
+                self._launch(dag, x_L[:min(B, 64)], x_U[:min(B, 64)], C[:min(B, 64)] if self.dense_c else None,
+                             lb, lA, lbias)       # warm-up: module load, workspace
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                self._launch(dag, x_L, x_U, C, lb, lA, lbias)
+                e1.record()
+                torch.cuda.synchronize()
+                times[cand] = e0.elapsed_time(e1)
+            best = min(times, key=times.get)
+            self._choice[key] = best
+            self.timings[key] = {self._dag(*c).name: t for c, t in times.items()}
+        dag = self._dag(*self._choice[key])
+        self.handle = dag.handle
+        self.prog = dag.prog
+        return dag
+
+    def _workspace_bytes(self, nbytes, device):
+        if self._ws is None or self._ws.numel() < nbytes or self._ws.device != device:
+            self._ws = None
+            self._ws = torch.empty(max(nbytes, 8), dtype=torch.uint8, device=device)
+        return self._ws

@@ -41,10 +41,10 @@ from .graph import Graph, MAP_KINDS
 NK = {"input": 0, "linear": 1, "matmul": 2, "mul": 3, "mulc": 4, "add": 5, "sub": 6, "addc": 7,
       "subc": 8, "rsubc": 9, "neg": 10, "sqr": 11, "exp": 12, "log": 13, "sin": 14, "cos": 15,
       "pow": 16, "reducesum": 17, "map": 18, "concat": 19}
-NODE_REC = 16
-# node record fields
+NODE_REC = 17
+# node record fields (N_WT_OFF: the weights transposed, (in, out), for the forward products)
 N_KIND, N_W, N_NIN, N_IN0, N_IN1, N_CUR, N_PLANE, N_CVEC, N_MAP0, N_MAP1, N_W_OFF, N_B_OFF, \
-    N_WIN, N_INS, N_FOLD, N_INEXACT = range(16)
+    N_WIN, N_INS, N_FOLD, N_INEXACT, N_WT_OFF = range(17)
 
 # ---- steps
 MODES = {"cta": 0, "simt": 1}          # ExecMode in gear_program.h
@@ -59,7 +59,7 @@ OP_REC = 32
 (O_KIND, O_V, O_SLOT, O_FIRST, O_VBUF, O_VNNZ, O_VRP, O_VCOLS, O_U, O_UBUF, O_UNNZ, O_URP,
  O_UCOLS, O_UMERGE, O_NTGT, O_TGT, O_SPTR, O_SRC, O_DENSE, O_FOLD, O_WOUT, O_VMAXROW, O_UMAXROW, O_VROWS,
  O_TPTR, O_UK, O_TMAXROW, O_SHORT, O_NSHORT, O_LONG, O_NLONG, O_SINGLE) = range(32)
-ROW_THREAD_MAX = 4   # rows with at most this much work run on one thread, longer rows on a warp
+ROW_THREAD_MAX = 16  # rows with at most this much work run on one thread, longer rows on a warp
 ROOT_IN_LA = -2     # buffer marker: the input's A of a final pass accumulates in the lA output
 
 PLANES_PER_ELEM = {"mul": 6, "sqr": 4, "exp": 4, "log": 4, "sin": 4, "cos": 4, "pow": 4}
@@ -119,13 +119,17 @@ class Program:
     """Compiled device program for one graph and one final specification shape."""
 
     def __init__(self, graph: Graph, spec_rows: Optional[int] = None, dense_c: bool = False,
-                 return_a: bool = True, smem_limit: int = 200 * 1024, mode: str = "cta"):
+                 return_a: bool = True, smem_limit: int = 200 * 1024, mode: str = "cta",
+                 cta_threads: int = 128):
         """mode: "cta" runs one box per CTA with the pass working set in shared memory, and the
         final pass accumulates the input's A directly in the lA output; "simt" runs one box per
         thread with every per-box array box-interleaved in global scratch, and writes lA from the
         pass buffers at the end."""
         if mode not in MODES:
             raise ProgramError(f"unknown execution mode {mode!r}")
+        if cta_threads not in (64, 128, 256):
+            raise ProgramError("threads per CTA must be 64, 128 or 256")
+        self.cta_threads = int(cta_threads)
         self.mode = mode
         self.x_in_la = mode == "cta"
         self.g = graph
@@ -417,6 +421,7 @@ class Program:
             elif k in ("linear", "matmul"):
                 W = a["W"] if k == "linear" else a["W"].T      # (out, in)
                 r[N_W_OFF] = P.add_dbl(np.ascontiguousarray(W))
+                r[N_WT_OFF] = P.add_dbl(np.ascontiguousarray(W.T))
                 r[N_WIN] = W.shape[1]
                 if k == "linear" and a.get("b") is not None:
                     r[N_B_OFF] = P.add_dbl(a["b"])
@@ -427,7 +432,9 @@ class Program:
         self.sin_lens = [len(tb[k]) for k in tables.SIN_TABLE_ORDER]
 
     def _finish(self):
-        self.max_smem = 0
+        # the pass working set doubles as the staging area of the box (centre, radius, magnitude)
+        # for the fold products, which run before any pass
+        self.max_smem = 3 * self.n + 32 if self.fold_off else 0
         self.max_S = 1
         for pid, pi in enumerate(self.passes):
             self._emit_pass(pid, pi)
@@ -448,7 +455,8 @@ class Program:
                                 self.n, self.S, self.t, self.arena_w, self.plane_w, self.fold_w,
                                 self.smem_total, self.max_S, self.sin_off, self.maxw,
                                 1 if self.return_a else 0, max_ops, self.simt_buf, self.simt_rows,
-                                1 if self.x_in_la else 0, MODES[self.mode]], dtype=np.int32)
+                                1 if self.x_in_la else 0, MODES[self.mode], self.cta_threads, 0, 0, 0],
+                               dtype=np.int32)
 
     def _emit_pass(self, pid, pi: PassInfo):
         g = self.g
@@ -621,8 +629,10 @@ class Program:
         rec[P_XDENSE] = 1 if xdense else 0
         rec[P_TMAXROW] = int(np.diff(rowptr[pi.t]).max(initial=0))
         self.pass_recs.append(rec)
-        # kernel shared memory: per side 3 row arrays (S) + the entry buffers
-        self.max_smem = max(self.max_smem, pi.sides * (3 * S + smem) + 32)
+        # kernel shared memory: per side the row arrays (S each: VAL, ERR, and ROOT in the final
+        # pass) + the entry buffers, then the reduction slots
+        nrows = 3 if pi.final else 2
+        self.max_smem = max(self.max_smem, pi.sides * (nrows * S + smem) + 32)
         self.max_S = max(self.max_S, S)
         pi.bufoff = bufoff
         pi.fold = fold

@@ -22,9 +22,11 @@ def _close(a, b, rtol=RTOL):
 
 
 @pytest.mark.parametrize("case", cases())
-def test_gpu_matches_oracle_on_fixture_boxes(case):
+@pytest.mark.parametrize("threads", [64, 128, 256])
+def test_gpu_matches_oracle_on_fixture_boxes(case, threads):
+    """Every box-per-CTA kernel instance (64, 128, 256 threads) against the oracle."""
     m, g, d, inject = load(case)
-    eng = CrownEngine(g)
+    eng = CrownEngine(g, mode="cta", cta_threads=threads)
     lo = torch.tensor(d["x_L"], device="cuda")
     hi = torch.tensor(d["x_U"], device="cuda")
     lb, lA, lbias = eng.lower(lo, hi)
@@ -65,3 +67,23 @@ def test_gpu_dense_c_matches_oracle():
     olb, _, olA, _ = o.compute_bounds(lo.numpy(), hi.numpy(), C.numpy())
     assert _close(lb.cpu().numpy(), olb) < RTOL
     assert _close(A["/y"]["/x"]["lA"].cpu().numpy(), olA) < RTOL
+
+
+@pytest.mark.parametrize("workload,batch", [("quad_exp_n10", 2048), ("dense_q_n200", 300)])
+def test_auto_engine_picks_a_variant_and_matches_oracle(workload, batch):
+    """mode="auto" times the variants on the first call and every later call uses the pick."""
+    from gear_b200 import graph
+    m = problems.make_instance(workload, 0)
+    lo, hi = problems.make_boxes(workload, batch, 0)
+    g = graph.trace(m, lo[:2])
+    eng = CrownEngine(g, mode="auto")
+    first = eng.lower(lo.cuda(), hi.cuda())
+    second = eng.lower(lo.cuda(), hi.cuda())
+    torch.cuda.synchronize()
+    assert eng.variant(batch) in {"simt", "cta64", "cta128", "cta256"}
+    assert len(eng.timings) == 1
+    for a, b in zip(first, second):
+        assert torch.equal(a, b)           # same variant, same arithmetic: bit-identical
+    olb, _, olA, olbias = CrownOracle(g).compute_bounds(lo.numpy(), hi.numpy())
+    assert _close(first[0].cpu().numpy(), olb) < RTOL
+    assert _close(first[1].cpu().numpy(), olA) < RTOL
