@@ -693,6 +693,66 @@ __device__ __forceinline__ double elem_coef(int kind, int slot, int side, double
   }
 }
 
+// One row of a GEMV step: Ur[j] (+)= sum_{e0 <= e < e1} V[e] W[vcols[e], j] for this thread's
+// columns j = eoff + q estep, with the charges' partial sums <|A||W|, m> (part) and
+// <|A W|, m> (pmerge). JB columns per thread per sweep, EB entries per chunk: EB x JB weight
+// loads in flight together.
+template <int JB, int EB>
+__device__ __forceinline__ void gemv_row(const double* V, const int32_t* vcols, int e0, int e1, const double* W,
+                                         int win, double* Ur, const double* mu, bool zero_u, int eoff, int estep,
+                                         double& part, double& pmerge) {
+    // JB columns per thread per sweep of the row's entries: their weight loads are in
+    // flight together instead of one dependent load chain per column
+    for (int jb = eoff; jb < win; jb += JB * estep) {
+      double acc[JB], ab[JB];
+      bool ok[JB];
+#pragma unroll
+      for (int q = 0; q < JB; ++q) { acc[q] = 0.0; ab[q] = 0.0; ok[q] = jb + q * estep < win; }
+      // entries in chunks of EB: their indices and coefficients first, then EB x JB weight
+      // loads in flight together, then the sums (in entry order)
+      for (int e = e0; e < e1; e += EB) {
+        int cq[EB];
+        double aq[EB];
+#pragma unroll
+        for (int r = 0; r < EB; ++r) {
+          const bool in = e + r < e1;
+          cq[r] = in ? __ldg(vcols + e + r) : 0;
+          aq[r] = in ? V[e + r] : 0.0;
+        }
+        double wq[EB][JB];
+#pragma unroll
+        for (int r = 0; r < EB; ++r) {
+          const double* Wr = W + (int64_t)cq[r] * win + jb;
+#pragma unroll
+          for (int q = 0; q < JB; ++q) wq[r][q] = (ok[q] && e + r < e1) ? __ldg(Wr + q * estep) : 0.0;
+        }
+#pragma unroll
+        for (int r = 0; r < EB; ++r) {
+          if (e + r >= e1) break;
+#pragma unroll
+          for (int q = 0; q < JB; ++q) {
+            acc[q] += aq[r] * wq[r][q];
+            ab[q] += fabs(aq[r]) * fabs(wq[r][q]);
+          }
+        }
+      }
+      double mq[JB], uq[JB];
+#pragma unroll
+      for (int q = 0; q < JB; ++q) {
+        mq[q] = ok[q] ? mu[jb + q * estep] : 0.0;
+        uq[q] = (ok[q] && !zero_u) ? Ur[jb + q * estep] : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < JB; ++q) {
+        if (!ok[q]) continue;
+        Ur[jb + q * estep] = zero_u ? acc[q] : uq[q] + acc[q];
+        const double mf = isinf(mq[q]) ? 0.0 : mq[q];
+        part += ab[q] * mf;
+        pmerge += fabs(acc[q]) * mf;
+      }
+    }
+}
+
 template <int NT>
 __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops, const Work& wk) {
   constexpr int NWARP = NT / 32;
@@ -778,7 +838,21 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
 
     // ---- per-row work of a non-GEMV op: bias/charges over v's row, zero u's row on its first
     //      contribution, pull the row's moves (or fold it into the concretisation)
-    auto row_body = [&](int s, int eoff, int estep, bool wide) {
+    // sum over the threads working on one row: a warp (mode 1) or the CTA (mode 2, every thread
+    // takes part; two barriers). Fixed order: deterministic.
+    auto row_sum = [&](double v, int mode) -> double {
+      v = warp_sum(v);
+      if (mode == 1) return v;
+      if (lane == 0) ctx.red[warp] = v;
+      __syncthreads();
+      double t = 0.0;
+      for (int w_ = 0; w_ < NWARP; ++w_) t += ctx.red[w_];
+      __syncthreads();
+      return t;
+    };
+    // mode 0: one thread per row, 1: a warp, 2: the whole CTA (every thread calls with the same s)
+    auto row_body = [&](int s, int eoff, int estep, int mode) {
+      const bool lead = mode == 0 || (mode == 1 ? lane == 0 : tid == 0);
       const int e0 = vrp[s], e1 = vrp[s + 1];
       for (int side = 0; side < sides; ++side) {
         const double* V = ctx.vals(side, op[O_VBUF]);
@@ -820,8 +894,13 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
               }
             }
           }
-          if (wide) { sb = warp_sum(sb); sm_ = warp_sum(sm_); sc = warp_sum(sc); und_ = warp_or(und_); }
-          if (!wide || lane == 0) {
+          if (mode != 0) {
+            sb = row_sum(sb, mode);
+            sm_ = row_sum(sm_, mode);
+            sc = row_sum(sc, mode);
+            und_ = row_sum((double)und_, mode) != 0.0;
+          }
+          if (lead) {
             double* val = ctx.row(side, R_VAL);
             val[s] = und_ ? NAN : val[s] + sb;
             ctx.row(side, R_ERR)[s] += sm_ * fbias + sc;
@@ -829,7 +908,7 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
         }
         if (op[O_FOLD]) {
           // linear/matmul on the input, one entry per row: exact fold into the concretisation
-          if (e0 < e1 && (!wide || lane == 0)) {
+          if (e0 < e1 && lead) {
             const double* f = bx.fold + vnd[N_FOLD];
             const int w = vnd[N_W];
             const double gk = gamma_k((double)op[O_WOUT]);
@@ -845,7 +924,8 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
         if (zero_u) {
           if (u_la) for (int j = eoff; j < n; j += estep) U[(size_t)s * n + j] = 0.0;
           else for (int j = urp[s] + eoff; j < urp[s + 1]; j += estep) U[j] = 0.0;
-          if (wide) __syncwarp();
+          if (mode == 1) __syncwarp();
+          if (mode == 2) __syncthreads();
         }
         const int32_t* tptr = P->ip + op[O_TPTR];
         const int k0 = tptr[s], k1 = tptr[s + 1];
@@ -876,8 +956,8 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
           }
         }
         if (uk >= 2) {
-          if (wide) pmerge = warp_sum(pmerge);
-          if (!wide || lane == 0) ctx.row(side, R_ERR)[s] += gmerge * pmerge;
+          if (mode != 0) pmerge = row_sum(pmerge, mode);
+          if (lead) ctx.row(side, R_ERR)[s] += gmerge * pmerge;
         }
       }
     };
@@ -886,8 +966,13 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
       const int32_t* shortr = P->ip + op[O_SHORT];
       const int32_t* longr = P->ip + op[O_LONG];
       const int nshort = op[O_NSHORT], nlong = op[O_NLONG];
-      for (int i = tid; i < nshort; i += NT) row_body(shortr[i], 0, 1, false);
-      for (int i = warp; i < nlong; i += NWARP) row_body(longr[i], lane, 32, true);
+      for (int i = tid; i < nshort; i += NT) row_body(shortr[i], 0, 1, 0);
+      if (2 * nlong <= NWARP) {
+        // few long rows (single rows of a chain): the whole CTA on each, instead of idle warps
+        for (int i = 0; i < nlong; ++i) row_body(longr[i], tid, NT, 2);
+      } else {
+        for (int i = warp; i < nlong; i += NWARP) row_body(longr[i], lane, 32, 1);
+      }
     } else {
       // ---- GEMV: A_u[s, :] (+)= sum_e A_v[e] W[c_e, :]; charges gamma_w <|A_v||W|, m_u> and merges
       const bool block_rows = op[O_VROWS] < NWARP;   // few rows: the whole CTA on each row
@@ -932,58 +1017,9 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
             continue;
           }
           double part = 0, pmerge = 0;
-          // JB columns per thread per sweep of the row's entries: their weight loads are in
-          // flight together instead of one dependent load chain per column
-          constexpr int JB = 4;
-          for (int jb = eoff; jb < win; jb += JB * estep) {
-            double acc[JB], ab[JB];
-            bool ok[JB];
-#pragma unroll
-            for (int q = 0; q < JB; ++q) { acc[q] = 0.0; ab[q] = 0.0; ok[q] = jb + q * estep < win; }
-            // entries in chunks of EB: their indices and coefficients first, then EB x JB weight
-            // loads in flight together, then the sums (in entry order)
-            constexpr int EB = 4;
-            for (int e = e0; e < e1; e += EB) {
-              int cq[EB];
-              double aq[EB];
-#pragma unroll
-              for (int r = 0; r < EB; ++r) {
-                const bool in = e + r < e1;
-                cq[r] = in ? __ldg(vcols + e + r) : 0;
-                aq[r] = in ? V[e + r] : 0.0;
-              }
-              double wq[EB][JB];
-#pragma unroll
-              for (int r = 0; r < EB; ++r) {
-                const double* Wr = W + (int64_t)cq[r] * win + jb;
-#pragma unroll
-                for (int q = 0; q < JB; ++q) wq[r][q] = (ok[q] && e + r < e1) ? __ldg(Wr + q * estep) : 0.0;
-              }
-#pragma unroll
-              for (int r = 0; r < EB; ++r) {
-                if (e + r >= e1) break;
-#pragma unroll
-                for (int q = 0; q < JB; ++q) {
-                  acc[q] += aq[r] * wq[r][q];
-                  ab[q] += fabs(aq[r]) * fabs(wq[r][q]);
-                }
-              }
-            }
-            double mq[JB], uq[JB];
-#pragma unroll
-            for (int q = 0; q < JB; ++q) {
-              mq[q] = ok[q] ? mu[jb + q * estep] : 0.0;
-              uq[q] = (ok[q] && !zero_u) ? Ur[jb + q * estep] : 0.0;
-            }
-#pragma unroll
-            for (int q = 0; q < JB; ++q) {
-              if (!ok[q]) continue;
-              Ur[jb + q * estep] = zero_u ? acc[q] : uq[q] + acc[q];
-              const double mf = isinf(mq[q]) ? 0.0 : mq[q];
-              part += ab[q] * mf;
-              pmerge += fabs(acc[q]) * mf;
-            }
-          }
+          if (block_rows) gemv_row<2, 8>(V, vcols, e0, e1, W, win, Ur, mu, zero_u, eoff, estep, part, pmerge);
+          else if (op[O_VMAXROW] <= 2) gemv_row<8, 1>(V, vcols, e0, e1, W, win, Ur, mu, zero_u, eoff, estep, part, pmerge);
+          else gemv_row<4, 4>(V, vcols, e0, e1, W, win, Ur, mu, zero_u, eoff, estep, part, pmerge);
           double tot_ = gk * warp_sum(part) + gmerge * warp_sum(pmerge);
           if (block_rows) {
             if (lane == 0) ctx.red[warp] = tot_;
