@@ -105,15 +105,15 @@ def _cpu_worker(args):
     return time.perf_counter() - t, lo.shape[0]
 
 
-def cpu_baseline(per_core=16, cores=None):
+def cpu_baseline(per_core=16, cores=None, workload=WORKLOAD):
     """The float64 CPU oracle (restatement of the reference's compute_bounds) on a bounded
     sample: per_core boxes on each of `cores` spawned processes; value = boxes / slowest."""
     import multiprocessing as mp
     import torch
     from gear_b200 import graph, problems
     cores = cores or os.cpu_count() or 1
-    m = problems.make_instance(WORKLOAD, 0)
-    lo, hi = problems.make_boxes(WORKLOAD, per_core * cores, 0, seed_offset=900)
+    m = problems.make_instance(workload, 0)
+    lo, hi = problems.make_boxes(workload, per_core * cores, 0, seed_offset=900)
     g = graph.trace(m, lo[:2])
     jobs = [(g, lo[i * per_core:(i + 1) * per_core].numpy(), hi[i * per_core:(i + 1) * per_core].numpy())
             for i in range(cores)]
@@ -127,7 +127,7 @@ def cpu_baseline(per_core=16, cores=None):
     slowest = max(r[0] for r in res)
     boxes = sum(r[1] for r in res)
     return {"value": boxes / slowest, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{boxes} {WORKLOAD} sub-boxes ({per_core} per process on {cores} spawned processes, "
+            "sample": f"{boxes} {workload} sub-boxes ({per_core} per process on {cores} spawned processes, "
                       f"float64 numpy oracle, 1 thread each; slowest process {slowest:.2f} s)"}
 
 
@@ -138,7 +138,7 @@ def run_reference(args):
     per_core = max(4, args.cpu_per_core)
     vals = []
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(per_core=per_core)
+        r = cpu_baseline(per_core=per_core, workload=args.workload)
         if i >= args.warmup:
             vals.append(r["value"])
     v = statistics.median(vals)
@@ -146,7 +146,7 @@ def run_reference(args):
     out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * 1 / v,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-           "data": "synthetic", "config": {"workload": WORKLOAD, "batch": r["sample"]},
+           "data": "synthetic", "config": {"workload": args.workload, "batch": r["sample"]},
            "cpu_baseline": r, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 
@@ -161,6 +161,8 @@ def main():
     ap.add_argument("--impl", default="gear", choices=["gear", "reference"])
     ap.add_argument("--cpu-per-core", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default=WORKLOAD, help="benchmark workload (profiling of other shapes)")
+    ap.add_argument("--cta-threads", type=int, default=128, help="threads per CTA of --mode cta")
     ap.add_argument("--mode", default="auto", choices=["auto", "cta", "simt"],
                     help="CROWN kernel: one box per CTA, one box per thread, or the faster one timed on the "
                          "first (warm-up) call")
@@ -182,9 +184,10 @@ def main():
     from gear_b200 import problems, BoundedModule
     from gear_b200 import _lib
     B = args.batch
-    model = problems.make_instance(WORKLOAD, 0)
-    lo, hi = problems.make_boxes(WORKLOAD, B, 0, seed_offset=500 + 7919 * rank)
-    bm = BoundedModule(model, lo[:2], device=str(dev), bound_opts={"gear_mode": args.mode})
+    model = problems.make_instance(args.workload, 0)
+    lo, hi = problems.make_boxes(args.workload, B, 0, seed_offset=500 + 7919 * rank)
+    bm = BoundedModule(model, lo[:2], device=str(dev), bound_opts={"gear_mode": args.mode,
+                                                                  "gear_cta_threads": args.cta_threads})
     S = bm.final_node_width()
     n = lo.shape[1]
     eng = bm._engine(S, False)
@@ -256,7 +259,10 @@ def main():
     if rank == 0:
         peak, peak_kind = _peaks()
         ms_launch = ms / args.steps
-        alg_bytes = B * (16 * n + 8 * S + 8 * S + 8 * S * n)       # boxes in; lb, lbias, lA out
+        # algorithmic bytes of the executed schedule (A entries read + written by the passes,
+        # float64) plus boxes in and lb, lbias, lA out
+        prog = eng.prog
+        alg_bytes = B * prog.alg_bytes_per_box()
         achieved = alg_bytes / (ms_launch / 1000.0) / 1e9
         traffic = None
         tfile = os.path.join(ROOT, "profiles", "dram_traffic.json")
@@ -264,14 +270,15 @@ def main():
             try:
                 with open(tfile) as f:
                     tj = json.load(f)
-                traffic = tj.get(WORKLOAD, {}).get("bytes_per_box")
+                kname = "crown_simt_kernel" if variant == "simt" else f"crown_megakernel<{variant[3:]}>"
+                traffic = tj.get(args.workload, {}).get(kname, {}).get("bytes_per_box")
                 traffic = traffic * B if traffic is not None else None
             except Exception:
                 traffic = None
         res = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-               "config": {"workload": WORKLOAD, "batch": B, "n": n, "spec_rows": S, "kernel_mode": args.mode, "kernel_variant": variant,
+               "config": {"workload": args.workload, "batch": B, "n": n, "spec_rows": S, "kernel_mode": args.mode, "kernel_variant": variant,
                           "variant_ms": eng.timings.get(eng._bucket(B)),
                           "parallelism": f"replicas{world}",
                           "l2": "inputs (x_L, x_U) and outputs (lA) larger than the 126 MB L2"},
@@ -279,13 +286,15 @@ def main():
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "traffic": traffic,
                             "kernel": "crown_simt_kernel" if variant == "simt" else f"crown_megakernel<{variant[3:]}>",
-                            "peak_source": peak_kind},
+                            "peak_source": peak_kind,
+                            "alg_bytes_per_box": prog.alg_bytes_per_box(), "work_per_box": prog.work,
+                            "fp64_gemm_gflops": prog.work["gemm_flops"] * B / (ms_launch / 1000.0) / 1e9},
                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * B * n * 8,
                        "d2h_bytes_per_step": B * S * 8},
                "clocks": clk.summary()}
         if world == 1 and not args.no_cpu_baseline:
             try:
-                res["cpu_baseline"] = cpu_baseline(per_core=args.cpu_per_core)
+                res["cpu_baseline"] = cpu_baseline(per_core=args.cpu_per_core, workload=args.workload)
             except Exception as ex:  # the baseline is reported, not required
                 res["cpu_baseline"] = {"value": None, "error": str(ex)[:200]}
         print(json.dumps(res))

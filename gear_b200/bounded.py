@@ -89,7 +89,8 @@ class BoundedModule:
         if eng is None:
             with torch.cuda.device(self.device):
                 eng = CrownEngine(self.graph, spec_rows=spec_rows, dense_c=dense_c,
-                                  mode=self.bound_opts.get("gear_mode", "auto"))
+                                  mode=self.bound_opts.get("gear_mode", "auto"),
+                                  cta_threads=int(self.bound_opts.get("gear_cta_threads", 128)))
             self._engines[key] = eng
         return eng
 

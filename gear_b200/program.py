@@ -435,6 +435,12 @@ class Program:
         # the pass working set doubles as the staging area of the box (centre, radius, magnitude)
         # for the fold products, which run before any pass
         self.max_smem = 3 * self.n + 32 if self.fold_off else 0
+        # algorithmic work per box of the executed schedule: A entries read and written by the
+        # backward passes (both sides), concretisation reads, and GEMM-shaped flops at dense
+        # nodes (2 per multiply-add of A W, plus the fold products W x0, |W| eps, |W| |x|)
+        self.work = {"a_read": 0, "a_written": 0, "gemm_flops": 0, "node_visits": 0, "passes": len(self.passes)}
+        for v in self.fold_off:
+            self.work["gemm_flops"] += 3 * 2 * self.g[v].width * self.n
         self.max_S = 1
         for pid, pi in enumerate(self.passes):
             self._emit_pass(pid, pi)
@@ -549,6 +555,12 @@ class Program:
                 r[O_FOLD] = 1 if (p == 0 and fold) else 0
                 r[O_VMAXROW] = int(np.diff(rowptr[v]).max(initial=0))
                 r[O_VROWS] = int((np.diff(rowptr[v]) > 0).sum())
+                sd = pi.sides
+                self.work["a_read"] += sd * nnz[v]
+                if r[O_DENSE] == 1 and r[O_FOLD] == 0:
+                    vlen = np.diff(rowptr[v])
+                    self.work["gemm_flops"] += sd * 2 * int(vlen.sum()) * g[p].width
+                    self.work["a_written"] += sd * int(np.diff(rowptr[p])[vlen > 0].sum())
                 if r[O_FOLD] == 1:
                     r[O_UBUF] = -1
                     r[O_UNNZ] = 0
@@ -580,6 +592,7 @@ class Program:
                         # entry (s, c) of the input's A lives at lA[s * n + c]
                         tgt = trow * self.n + cols[0][tgt]
                     r[O_NTGT] = len(tgt)
+                    self.work["a_written"] += pi.sides * len(tgt)
                     r[O_TGT] = P.add_int(tgt)
                     r[O_SPTR] = P.add_int(sptr)
                     r[O_SRC] = P.add_int(src)
@@ -628,6 +641,9 @@ class Program:
         rec[P_XMAXROW] = int(np.diff(rowptr[0]).max(initial=0)) if (0 in pats and not fold) else 0
         rec[P_XDENSE] = 1 if xdense else 0
         rec[P_TMAXROW] = int(np.diff(rowptr[pi.t]).max(initial=0))
+        self.work["a_written"] += pi.sides * nnz[pi.t]
+        self.work["a_read"] += pi.sides * x_nnz
+        self.work["node_visits"] += int(rec[P_NVISIT])
         self.pass_recs.append(rec)
         # kernel shared memory: per side the row arrays (S each: VAL, ERR, and ROOT in the final
         # pass) + the entry buffers, then the reduction slots
@@ -699,6 +715,12 @@ class Program:
         return tgt, sptr, src
 
     # ================================================================= info
+    def alg_bytes_per_box(self) -> int:
+        """Algorithmic bytes per bounded box, float64 throughout: 8 (A read + A written) of the
+        executed schedule + the box in (16 n) + lb, lbias out (16 S) + lA out (8 S n)."""
+        w = self.work
+        return 8 * (w["a_read"] + w["a_written"]) + 16 * self.n + 16 * self.S + 8 * self.S * self.n
+
     def describe(self) -> str:
         lines = [f"nodes={len(self.g)} steps={len(self.steps)} passes={len(self.passes)} ops={len(self.op_recs)} "
                  f"arena={self.arena_w} planes={self.plane_w} fold={self.fold_w} smem_doubles={self.max_smem}"]
