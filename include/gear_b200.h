@@ -18,6 +18,13 @@
  *                        PerturbationLpNorm(x_L, x_U)),), C, method='CROWN',
  *                        bound_upper=False, return_A=True, needed_A_dict)  bound_general.py:1275
  *                        as called by get_lower_bound_naive (complete_verifier/input_split/bounding.py:317)
+ *   gear_bab_prune    <- get_remaining_index, solving mode        complete_verifier/input_split/branching_domains.py:412-558
+ *                        + discarded-threshold minimum              batch_branch_and_bound.py:628-636
+ *   gear_bab_branch   <- input_split_branching, method 'sb', sb_sum complete_verifier/input_split/branching_heuristics.py:25-202
+ *   gear_bab_split    <- input_split_parallel                      complete_verifier/input_split/split.py:26-122
+ *                        + child keys (_raise_child_keys)          batch_branch_and_bound.py:189-225
+ *   gear_queue_order  <- UnsortedInputDomainList.sort / pick_out_batch  branching_domains.py:1171-1240, :831-962
+ *   gear_gather_rows, gear_scatter_rows <- TensorStorage pop / append    complete_verifier/input_split/tensor_storage.py:351-408
  */
 #ifndef GEAR_B200_H
 #define GEAR_B200_H
@@ -58,14 +65,54 @@ int64_t gear_crown_workspace_bytes(const gear_dag* dag, int64_t batch);
  *   x_L, x_U  (batch, n) float64      box of every subdomain
  *   C         (batch, S, w_out) float64, or NULL for the identity specification
  *   lb        (batch, S) float64      lower bound of every specification row
- *   lA        (batch, S, n) float64   A of the bound w.r.t. the input (required: the
- *                                     final pass accumulates A in this buffer)
+ *   lA        (batch, S, n) float64   A of the bound w.r.t. the input (required for a
+ *                                     box-per-CTA program, whose final pass accumulates A
+ *                                     in this buffer; optional for a box-per-thread one)
  *   lbias     (batch, S) float64 or NULL      bias of that plane (lb minus the
  *                                            concretised A term)
  * `stream` is a cudaStream_t (NULL: the legacy default stream). Asynchronous. */
 int gear_crown_lower(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
                      const double* C, double* lb, double* lA, double* lbias,
                      void* workspace, int64_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------- branch and bound step
+ * All arrays are device memory; `stream` is a cudaStream_t. Every call is asynchronous. */
+
+/* Bytes of workspace gear_bab_prune needs for `batch` boxes. */
+int64_t gear_bab_workspace_bytes(int64_t batch);
+
+/* Prune (solving mode): keep[b] = 0 when some row proves box b done (lb_j > thr_j on a finite
+ * row, lb_0 >= thr_0, or lb_0 = +inf with a finite thr_0). kept[0..n_kept) lists the kept boxes
+ * in order; disc_min (one double, in/out) is lowered to the smallest finite thr_0 of the
+ * discarded boxes. lb, thr (batch, S). */
+int gear_bab_prune(const double* lb, const double* thr, int64_t batch, int S, uint8_t* keep, int32_t* kept,
+                   int32_t* n_kept, double* disc_min, void* workspace, int64_t ws_bytes, void* stream);
+
+/* Split variable per box: argmax over i of sum_s max(|lA[b,s,i]|, coeff_thresh) (hi-lo)/2
+ * (lowest index on ties); the widest variable when any lA/lb/thr is not finite, or when the
+ * chosen width is below min_width_ratio of the widest relative to root_width (n). */
+int gear_bab_branch(const double* lA, const double* lo, const double* hi, const double* lb, const double* thr,
+                    int64_t batch, int S, int n, const double* root_width, double coeff_thresh,
+                    double min_width_ratio, int32_t* split_idx, void* workspace, int64_t ws_bytes, void* stream);
+
+/* Bisect the kept boxes at the midpoint of split_idx: children (2 n_kept, n) ordered
+ * [upper halves of kept[0..n_kept); lower halves]. With child_key non-NULL also the children's
+ * keys (2 n_kept, S): the parent's lb, row 0 raised to the parent plane's minimum over the child
+ * box (rounded down). */
+int gear_bab_split(const double* lo, const double* hi, const int32_t* kept, int64_t n_kept, int n,
+                   const int32_t* split_idx, const double* lb, const double* lA, const double* lbias, int S,
+                   double* child_lo, double* child_hi, double* child_key, void* stream);
+
+/* Queue order of `count` slots: key descending, insertion id ascending on ties (bitonic sort;
+ * order_len >= the next power of two of count). The batch is taken from the end. */
+int gear_queue_order(const double* key, const int64_t* id, const int32_t* slots, int64_t count, int32_t* order,
+                     int64_t order_len, void* stream);
+
+/* dst[i, :] = src[rows[i], :] and dst[rows[i], :] = src[i, :] for float64 rows of `width`. */
+int gear_gather_rows(const double* src, const int32_t* rows, int64_t count, int64_t width, double* dst,
+                     void* stream);
+int gear_scatter_rows(const double* src, const int32_t* rows, int64_t count, int64_t width, double* dst,
+                      void* stream);
 
 /* gear_crown_lower without a workspace argument, for callers that cannot allocate device
  * memory (a solver host that owns a fixed device-memory plan and gives this library no
