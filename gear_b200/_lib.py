@@ -56,6 +56,10 @@ def lib():
         L.gear_gather_rows.restype = i32
         L.gear_scatter_rows.argtypes = [vp, vp, i64, i64, vp, vp]
         L.gear_scatter_rows.restype = i32
+        L.gear_constrained_workspace_bytes.argtypes = [i64, i32]
+        L.gear_constrained_workspace_bytes.restype = i64
+        L.gear_constrained_lower.argtypes = [vp, vp, i64, i32, vp, i32, vp, vp, i32, i32, vp, vp, vp, i64, vp]
+        L.gear_constrained_lower.restype = i32
         _LIB = L
     return _LIB
 
@@ -80,4 +84,5 @@ def ptr_dbl(a):
 EXPORTED = ("gear_dag_create", "gear_dag_destroy", "gear_crown_workspace_bytes", "gear_crown_lower",
             "gear_last_launch_count", "gear_last_error", "gear_bab_workspace_bytes", "gear_bab_prune",
             "gear_bab_branch", "gear_bab_split", "gear_queue_order", "gear_gather_rows", "gear_scatter_rows",
-            "gear_crown_lower_static", "gear_crown_static_scratch_bytes")
+            "gear_crown_lower_static", "gear_crown_static_scratch_bytes", "gear_constrained_workspace_bytes",
+            "gear_constrained_lower")

@@ -13,6 +13,7 @@
 #include "crown_kernel.cuh"
 #include "crown_simt.cuh"
 #include "bab_kernels.cuh"
+#include "concretize_kernels.cuh"
 
 namespace {
 thread_local std::string g_err;
@@ -416,6 +417,82 @@ extern "C" int gear_scatter_rows(const double* src, const int32_t* rows, int64_t
   g_launches = 1;
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_scatter_rows");
+}
+
+// ------------------------------------------------------------------ constrained concretisation
+namespace {
+struct CcLayout {
+  size_t d, score, infeasible, uncovered, nkeep, glob, total;
+};
+CcLayout cc_layout(int64_t batch, int K) {
+  CcLayout L;
+  size_t o = 0;
+  auto take = [&](size_t bytes) { size_t at = o; o += (bytes + 255) / 256 * 256; return at; };
+  L.d = take((size_t)batch * K * sizeof(double));
+  L.score = take((size_t)batch * K * sizeof(double));
+  L.infeasible = take((size_t)batch * sizeof(int));
+  L.uncovered = take((size_t)batch * sizeof(int));
+  L.nkeep = take((size_t)batch * sizeof(int));
+  L.glob = take(2 * sizeof(int));
+  L.total = o;
+  return L;
+}
+}  // namespace
+
+extern "C" int64_t gear_constrained_workspace_bytes(int64_t batch, int K) {
+  if (batch < 0 || K < 0) return -1;
+  return (int64_t)cc_layout(batch, K).total;
+}
+
+extern "C" int gear_constrained_lower(const double* x_L, const double* x_U, int64_t batch, int n, const double* obj,
+                                      int H, const double* A, const double* b, int K, int max_rows, double* lb,
+                                      uint8_t* infeasible, void* workspace, int64_t ws_bytes, void* stream) {
+  g_launches = 0;
+  if (!x_L || !x_U || !obj || !lb || batch < 0 || n < 1 || H < 1 || K < 0 || max_rows < 0 || (K > 0 && (!A || !b)))
+    return fail(GEAR_E_INVALID, "gear_constrained_lower: %s", "bad arguments");
+  if (batch == 0) return GEAR_OK;
+  const CcLayout L = cc_layout(batch, K);
+  if (!workspace || ws_bytes < (int64_t)L.total)
+    return fail(GEAR_E_WORKSPACE, "gear_constrained_lower: %s", "workspace smaller than gear_constrained_workspace_bytes");
+  const size_t per = gear::cc::sweep_smem_per_warp(n, K);
+  int warps = (int)((size_t)(160 << 10) / per);
+  if (warps > 4) warps = 4;
+  if (warps < 1) {
+    if (per > (size_t)(227 << 10))
+      return fail(GEAR_E_INVALID, "gear_constrained_lower: %s", "too many variables or rows for one warp's shared memory");
+    warps = 1;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  char* ws = (char*)workspace;
+  gear::cc::Work w;
+  w.xL = x_L; w.xU = x_U; w.obj = obj; w.A = A; w.b = b;
+  w.d = (double*)(ws + L.d);
+  w.score = (double*)(ws + L.score);
+  w.infeasible = (int*)(ws + L.infeasible);
+  w.uncovered = (int*)(ws + L.uncovered);
+  w.nkeep = (int*)(ws + L.nkeep);
+  w.glob = (int*)(ws + L.glob);
+  w.lb = lb;
+  w.infeasible_out = infeasible;
+  w.B = batch; w.X = n; w.H = H; w.K = K; w.max_rows = max_rows;
+  // the per-box counters and flags start at zero on every call
+  cudaError_t e = cudaMemsetAsync(ws + L.infeasible, 0, L.total - L.infeasible, st);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+  int launches = 0;
+  if (K > 0) {
+    const int64_t rows = batch * K;
+    gear::cc::concretize_rows_kernel<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(w);
+    gear::cc::concretize_boxes_kernel<<<(unsigned)((batch + 255) / 256), 256, 0, st>>>(w);
+    launches += 2;
+  }
+  const size_t smem = per * warps;
+  e = cudaFuncSetAttribute(gear::cc::concretize_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+  const int64_t items = batch * H;
+  gear::cc::concretize_sweep_kernel<<<(unsigned)((items + warps - 1) / warps), 32 * warps, smem, st>>>(w);
+  g_launches = launches + 1;
+  e = cudaGetLastError();
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_constrained_lower");
 }
 
 #ifdef GEAR_STEP_PROFILE

@@ -25,6 +25,8 @@
  *                        + child keys (_raise_child_keys)          batch_branch_and_bound.py:189-225
  *   gear_queue_order  <- UnsortedInputDomainList.sort / pick_out_batch  branching_domains.py:1171-1240, :831-962
  *   gear_gather_rows, gear_scatter_rows <- TensorStorage pop / append    complete_verifier/input_split/tensor_storage.py:351-408
+ *   gear_constrained_lower <- sort_out_constr_batches + constraints_solving(sign=-1)
+ *                        (+ drop_redundant_constraints, _solve_dual_var)  solver/auto_LiRPA/concretize_func.py:168-850
  */
 #ifndef GEAR_B200_H
 #define GEAR_B200_H
@@ -113,6 +115,22 @@ int gear_gather_rows(const double* src, const int32_t* rows, int64_t count, int6
                      void* stream);
 int gear_scatter_rows(const double* src, const int32_t* rows, int64_t count, int64_t width, double* dst,
                       void* stream);
+
+/* ---------------------------------------------------------------- constrained concretisation */
+
+/* Bytes of workspace gear_constrained_lower needs. */
+int64_t gear_constrained_workspace_bytes(int64_t batch, int K);
+
+/* Lower bounds lb (batch, H) of obj (batch, H, n) . x over each box [x_L, x_U] (batch, n)
+ * intersected with the rows A (batch, K, n) x + b (batch, K) <= 0, by the sequential dual sweep:
+ * rows that cannot bind on the box are skipped, each remaining row k (at most max_rows of them,
+ * the most binding, when max_rows > 0) gets the multiplier beta_k >= 0 that maximises the one-row
+ * Lagrangian of the current objective, and the bound is widened by an outward rounding term and
+ * never below the box bound. A box that some row excludes gets +inf (and infeasible[b] = 1 when
+ * `infeasible` is non-NULL). Rows with a non-finite entry are ignored. n <= ~2000. */
+int gear_constrained_lower(const double* x_L, const double* x_U, int64_t batch, int n, const double* obj, int H,
+                           const double* A, const double* b, int K, int max_rows, double* lb, uint8_t* infeasible,
+                           void* workspace, int64_t ws_bytes, void* stream);
 
 /* gear_crown_lower without a workspace argument, for callers that cannot allocate device
  * memory (a solver host that owns a fixed device-memory plan and gives this library no
