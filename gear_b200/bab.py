@@ -48,14 +48,22 @@ class BaBStats:
 class DomainQueue:
     """Device-resident pool of open subdomains (structure of arrays over slots)."""
 
-    def __init__(self, n: int, S: int, capacity: int, device):
+    def __init__(self, n: int, S: int, capacity: int, device, cuts: bool = False):
+        """cuts: also keep per domain the cut rows A (S, n), b (S) inherited from its parent."""
         self.n, self.S, self.device = n, S, device
+        self.cuts = cuts
         self.cap = 0
-        self.lo = self.hi = self.key = self.thr = self.ids = None
+        self.lo = self.hi = self.key = self.thr = self.ids = self.cutA = self.cutb = None
         self.free: List[torch.Tensor] = []
         self.active = torch.empty(0, dtype=torch.int32, device=device)
         self.next_id = 0
         self._grow(max(capacity, 1))
+
+    def _fields(self):
+        f = [("lo", self.n), ("hi", self.n), ("key", self.S), ("thr", self.S)]
+        if self.cuts:
+            f += [("cutA", self.S * self.n), ("cutb", self.S)]
+        return f
 
     def _grow(self, cap):
         dev = self.device
@@ -64,6 +72,9 @@ class DomainQueue:
                    key=torch.full((cap, self.S), math.inf, dtype=torch.float64, device=dev),
                    thr=torch.empty(cap, self.S, dtype=torch.float64, device=dev),
                    ids=torch.zeros(cap, dtype=torch.int64, device=dev))
+        if self.cuts:
+            new["cutA"] = torch.empty(cap, self.S * self.n, dtype=torch.float64, device=dev)
+            new["cutb"] = torch.empty(cap, self.S, dtype=torch.float64, device=dev)
         if self.cap:
             for k in new:
                 new[k][:self.cap] = getattr(self, k)
@@ -76,7 +87,7 @@ class DomainQueue:
     def __len__(self):
         return int(self.active.numel())
 
-    def push(self, lo, hi, key, thr):
+    def push(self, lo, hi, key, thr, cutA=None, cutb=None):
         m = lo.shape[0]
         if m == 0:
             return
@@ -86,9 +97,11 @@ class DomainQueue:
         self.free_slots = self.free_slots[:-m]
         L = _lib.lib()
         stream = torch.cuda.current_stream(self.device).cuda_stream
-        for src, dst, w in ((lo, self.lo, self.n), (hi, self.hi, self.n), (key, self.key, self.S),
-                            (thr, self.thr, self.S)):
-            _lib.check(L.gear_scatter_rows(_p(src.contiguous()), _p(slots), m, w, _p(dst), stream), "gear_scatter_rows")
+        vals = {"lo": lo, "hi": hi, "key": key, "thr": thr, "cutA": cutA, "cutb": cutb}
+        for name, w in self._fields():
+            src = vals[name].reshape(m, w).contiguous()
+            _lib.check(L.gear_scatter_rows(_p(src), _p(slots), m, w, _p(getattr(self, name)), stream),
+                       "gear_scatter_rows")
         self.ids[slots.long()] = torch.arange(self.next_id, self.next_id + m, device=self.device)
         self.next_id += m
         self.active = torch.cat([self.active, slots])
@@ -108,9 +121,10 @@ class DomainQueue:
         slots = order[N - b:].contiguous()
         self.active = order[:N - b].contiguous()
         out = []
-        for src, w in ((self.lo, self.n), (self.hi, self.n), (self.key, self.S), (self.thr, self.S)):
+        for name, w in self._fields():
             dst = torch.empty(b, w, dtype=torch.float64, device=self.device)
-            _lib.check(L.gear_gather_rows(_p(src), _p(slots), b, w, _p(dst), stream), "gear_gather_rows")
+            _lib.check(L.gear_gather_rows(_p(getattr(self, name)), _p(slots), b, w, _p(dst), stream),
+                       "gear_gather_rows")
             out.append(dst)
         self.free_slots = torch.cat([self.free_slots, slots])
         return out
@@ -129,7 +143,14 @@ class BaB:
 
     def __init__(self, graph: Graph, lo: torch.Tensor, hi: torch.Tensor, rhs: Optional[torch.Tensor] = None,
                  device="cuda", batch: int = 4096, sb_coeff_thresh: float = 1e-3,
-                 sb_min_width_ratio: float = 1e-3, model: Optional[torch.nn.Module] = None):
+                 sb_min_width_ratio: float = 1e-3, model: Optional[torch.nn.Module] = None,
+                 constrained: bool = False, max_constraint_rows: int = 16):
+        """constrained: the reference's complete clipping mode's constrained concretisation
+        (batch_branch_and_bound.py:422-428): every child keeps its parent's planes
+        lA_j x + lbias_j <= thr_j as cut rows, and the objective row of its CROWN bound is
+        concretised over the box intersected with them (concretize_func.py:415-850, at most
+        max_constraint_rows rows per box, the f3 setting's concretize_max_constraint_rows);
+        a box that the cuts exclude is pruned."""
         self.device = torch.device(device)
         self.graph = graph
         self.engine = CrownEngine(graph)
@@ -145,9 +166,13 @@ class BaB:
         self.rhs = (torch.zeros(self.S - 1, dtype=torch.float64) if rhs is None else rhs.to(torch.float64)).to(self.device)
         self.incumbent = math.inf
         self.x_best = None
-        self.queue = DomainQueue(self.n, self.S, 4 * batch, self.device)
+        self.constrained = constrained
+        self.max_constraint_rows = max_constraint_rows
+        self.queue = DomainQueue(self.n, self.S, 4 * batch, self.device, cuts=constrained)
         key = torch.full((1, self.S), -math.inf, dtype=torch.float64, device=self.device)
-        self.queue.push(lo, hi, key, self._thresholds(1))
+        cutA = torch.zeros(1, self.S * self.n, dtype=torch.float64, device=self.device) if constrained else None
+        cutb = torch.full((1, self.S), -1.0, dtype=torch.float64, device=self.device) if constrained else None
+        self.queue.push(lo, hi, key, self._thresholds(1), cutA, cutb)
         self.disc_min = torch.full((1,), math.inf, dtype=torch.float64, device=self.device)
         self.stats = BaBStats()
         self._ws = torch.empty(1, dtype=torch.uint8, device=self.device)
@@ -196,12 +221,15 @@ class BaB:
         q = self.queue
         if len(q) == 0:
             return 0
-        lo, hi, key, thr = q.pop(self.batch)
+        popped = q.pop(self.batch)
+        lo, hi, key, thr = popped[:4]
         B = lo.shape[0]
         thr[:, 0] = self.incumbent          # thresholds follow the current incumbent
         self.update_incumbent((lo + hi) / 2)
         thr[:, 0] = self.incumbent
         lb, lA, lbias = self.engine.lower(lo, hi)
+        if self.constrained:
+            self._constrained_objective(lo, hi, lb, lA, lbias, popped[4], popped[5])
         L = _lib.lib()
         stream = torch.cuda.current_stream(self.device).cuda_stream
         keep = torch.empty(B, dtype=torch.uint8, device=self.device)
@@ -224,8 +252,39 @@ class BaB:
             ckey = torch.empty(2 * K, self.S, dtype=torch.float64, device=self.device)
             _lib.check(L.gear_bab_split(_p(lo), _p(hi), _p(kept), K, self.n, _p(split_idx), _p(lb), _p(lA),
                                         _p(lbias), self.S, _p(clo), _p(chi), _p(ckey), stream), "gear_bab_split")
-            q.push(clo, chi, ckey, torch.cat([thr[kept[:K].long()]] * 2))
+            cuts = self._cuts(lA, lbias, thr, kept[:K].long()) if self.constrained else (None, None)
+            q.push(clo, chi, ckey, torch.cat([thr[kept[:K].long()]] * 2), *cuts)
         return B
+
+    def _cuts(self, lA, lbias, thr, parents):
+        """Cut rows of the children (both halves of every kept parent) in standard form
+        A x + b <= 0 from the parents' planes lA_j x + lbias_j <= thr_j
+        (construct_cut_constraints, input_split/utils.py:113-129); a row with an infinite
+        threshold (the objective before any incumbent) is the inert row 0 x - 1 <= 0."""
+        A = lA[parents].reshape(parents.numel(), self.S, self.n)
+        t = thr[parents]
+        b = lbias[parents] - t
+        inactive = torch.isposinf(t)
+        A = A.masked_fill(inactive.unsqueeze(-1), 0.0)
+        b = b.masked_fill(inactive, -1.0)
+        A = A.reshape(parents.numel(), -1)
+        return torch.cat([A, A]), torch.cat([b, b])
+
+    def _constrained_objective(self, lo, hi, lb, lA, lbias, cutA, cutb):
+        """Raise the objective row's bound to lbias_0 + min of lA_0 x over the box intersected
+        with the inherited cut rows; +inf (pruned) when the rows exclude the box."""
+        from .concretize import constraints_solving
+        B = lo.shape[0]
+        obj = lA[:, :1, :]
+        val, infeasible = constraints_solving(lo, hi, obj, (cutA.reshape(B, self.S, self.n), cutb),
+                                              sign=-1.0, max_rows=self.max_constraint_rows,
+                                              return_infeasible=True)
+        new = val[:, 0, 0] + lbias[:, 0]
+        # the addition is rounded: widen it down by u |result| (fp_enclosure.add_bound)
+        new = torch.where(torch.isfinite(new), new - torch.abs(new) * (17 * 4 * 2.220446049250313e-16), new)
+        new = torch.where(torch.isnan(new), lb[:, 0], new)
+        lb[:, 0] = torch.maximum(lb[:, 0], new)
+        lb[:, 0] = torch.where(infeasible, torch.full_like(new, math.inf), lb[:, 0])
 
     def run(self, rel_gap: float = 1e-4, max_iterations: int = 10000, time_limit: float = 60.0):
         t0 = time.perf_counter()
