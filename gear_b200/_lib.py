@@ -60,6 +60,12 @@ def lib():
         L.gear_constrained_workspace_bytes.restype = i64
         L.gear_constrained_lower.argtypes = [vp, vp, i64, i32, vp, i32, vp, vp, i32, i32, vp, vp, vp, i64, vp]
         L.gear_constrained_lower.restype = i32
+        L.gear_clip_domains.argtypes = [vp, vp, vp, vp, vp, vp, i64, i32, i32, i32, vp, vp]
+        L.gear_clip_domains.restype = i32
+        L.gear_bab_child_keys.argtypes = [vp, vp, vp, vp, vp, vp, i64, i32, i32, vp, vp]
+        L.gear_bab_child_keys.restype = i32
+        L.gear_bab_compact.argtypes = [vp, i64, vp, vp, vp, i64, vp]
+        L.gear_bab_compact.restype = i32
         _LIB = L
     return _LIB
 
@@ -85,4 +91,4 @@ EXPORTED = ("gear_dag_create", "gear_dag_destroy", "gear_crown_workspace_bytes",
             "gear_last_launch_count", "gear_last_error", "gear_bab_workspace_bytes", "gear_bab_prune",
             "gear_bab_branch", "gear_bab_split", "gear_queue_order", "gear_gather_rows", "gear_scatter_rows",
             "gear_crown_lower_static", "gear_crown_static_scratch_bytes", "gear_constrained_workspace_bytes",
-            "gear_constrained_lower")
+            "gear_constrained_lower", "gear_clip_domains", "gear_bab_child_keys", "gear_bab_compact")

@@ -42,6 +42,7 @@ class BaBStats:
     iterations: int = 0
     bounded: int = 0
     pruned: int = 0
+    clipped_empty: int = 0
     history: List[dict] = field(default_factory=list)
 
 
@@ -144,13 +145,16 @@ class BaB:
     def __init__(self, graph: Graph, lo: torch.Tensor, hi: torch.Tensor, rhs: Optional[torch.Tensor] = None,
                  device="cuda", batch: int = 4096, sb_coeff_thresh: float = 1e-3,
                  sb_min_width_ratio: float = 1e-3, model: Optional[torch.nn.Module] = None,
-                 constrained: bool = False, max_constraint_rows: int = 16):
+                 constrained: bool = False, max_constraint_rows: int = 16, clip: bool = False,
+                 clip_iterations: int = 1):
         """constrained: the reference's complete clipping mode's constrained concretisation
         (batch_branch_and_bound.py:422-428): every child keeps its parent's planes
         lA_j x + lbias_j <= thr_j as cut rows, and the objective row of its CROWN bound is
         concretised over the box intersected with them (concretize_func.py:415-850, at most
         max_constraint_rows rows per box, the f3 setting's concretize_max_constraint_rows);
-        a box that the cuts exclude is pruned."""
+        a box that the cuts exclude is pruned.
+        clip: domain clipping of the children with their parent's planes (clip.py:237-470,
+        clip_iterations rounds); children that become empty are dropped."""
         self.device = torch.device(device)
         self.graph = graph
         self.engine = CrownEngine(graph)
@@ -166,6 +170,8 @@ class BaB:
         self.rhs = (torch.zeros(self.S - 1, dtype=torch.float64) if rhs is None else rhs.to(torch.float64)).to(self.device)
         self.incumbent = math.inf
         self.x_best = None
+        self.clip = clip
+        self.clip_iterations = clip_iterations
         self.constrained = constrained
         self.max_constraint_rows = max_constraint_rows
         self.queue = DomainQueue(self.n, self.S, 4 * batch, self.device, cuts=constrained)
@@ -250,10 +256,45 @@ class BaB:
             clo = torch.empty(2 * K, self.n, dtype=torch.float64, device=self.device)
             chi = torch.empty_like(clo)
             ckey = torch.empty(2 * K, self.S, dtype=torch.float64, device=self.device)
-            _lib.check(L.gear_bab_split(_p(lo), _p(hi), _p(kept), K, self.n, _p(split_idx), _p(lb), _p(lA),
-                                        _p(lbias), self.S, _p(clo), _p(chi), _p(ckey), stream), "gear_bab_split")
+            parents = torch.cat([kept[:K], kept[:K]])
+            if not self.clip:
+                _lib.check(L.gear_bab_split(_p(lo), _p(hi), _p(kept), K, self.n, _p(split_idx), _p(lb), _p(lA),
+                                            _p(lbias), self.S, _p(clo), _p(chi), _p(ckey), stream), "gear_bab_split")
+            else:
+                # split, clip the children with their parent's planes, then key the clipped boxes
+                # (the reordered loop: split -> clip -> child key, batch_branch_and_bound.py:505-535)
+                _lib.check(L.gear_bab_split(_p(lo), _p(hi), _p(kept), K, self.n, _p(split_idx), None, None, None,
+                                            self.S, _p(clo), _p(chi), None, stream), "gear_bab_split")
+                nonempty = torch.empty(2 * K, dtype=torch.uint8, device=self.device)
+                _lib.check(L.gear_clip_domains(_p(clo), _p(chi), _p(thr), _p(lA), _p(lbias), _p(parents), 2 * K,
+                                               self.S, self.n, self.clip_iterations, _p(nonempty), stream),
+                           "gear_clip_domains")
+                _lib.check(L.gear_bab_child_keys(_p(lb), _p(lA), _p(lbias), _p(clo), _p(chi), _p(kept), K, self.S,
+                                                 self.n, _p(ckey), stream), "gear_bab_child_keys")
             cuts = self._cuts(lA, lbias, thr, kept[:K].long()) if self.constrained else (None, None)
-            q.push(clo, chi, ckey, torch.cat([thr[kept[:K].long()]] * 2), *cuts)
+            cthr = torch.cat([thr[kept[:K].long()]] * 2)
+            fields = [clo, chi, ckey, cthr, *cuts]
+            if self.clip:
+                # children the clipping emptied are done: drop them before they enter the queue
+                live = torch.empty(2 * K, dtype=torch.int32, device=self.device)
+                nl = torch.zeros(1, dtype=torch.int32, device=self.device)
+                ws2 = self._ws_bytes(int(L.gear_bab_workspace_bytes(2 * K)))
+                _lib.check(L.gear_bab_compact(_p(nonempty), 2 * K, _p(live), _p(nl), _p(ws2), ws2.numel(), stream),
+                           "gear_bab_compact")
+                m = int(nl.item())
+                self.stats.clipped_empty += 2 * K - m
+                out = []
+                for f in fields:
+                    if f is None:
+                        out.append(None)
+                        continue
+                    g = torch.empty(m, f.shape[1], dtype=torch.float64, device=self.device)
+                    if m:
+                        _lib.check(L.gear_gather_rows(_p(f.contiguous()), _p(live), m, f.shape[1], _p(g), stream),
+                                   "gear_gather_rows")
+                    out.append(g)
+                fields = out
+            q.push(*fields)
         return B
 
     def _cuts(self, lA, lbias, thr, parents):

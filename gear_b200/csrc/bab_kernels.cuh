@@ -287,5 +287,117 @@ __global__ void scatter_rows_kernel(const double* src, const int32_t* rows, int6
   dst[(int64_t)rows[r] * w + j] = src[t];
 }
 
+
+// ------------------------------------------------------------------ domain clipping
+// clip_domains / _clip_main_fn (complete_verifier/input_split/clip.py:138-486), lower planes:
+// shrink each box along every coordinate to where each plane lA_s x + lbias_s can still be
+// <= thr_s; a box some plane already proves done becomes empty (x_L[0] = next double above
+// x_U[0]). One warp per box, lanes over coordinates; the per-row plane minima and their
+// rounding bounds sit in shared memory (3 S doubles per warp).
+__device__ __forceinline__ double next_up(double x) {
+  if (isnan(x) || x == INFINITY) return x;
+  if (x == 0.0) return 4.9406564584124654e-324;
+  long long b = __double_as_longlong(x);
+  return __longlong_as_double(x > 0 ? b + 1 : b - 1);
+}
+__device__ __forceinline__ double next_dn(double x) { return -next_up(-x); }
+constexpr double CLIP_EPS = 2.220446049250313e-16;
+constexpr double CLIP_TINY = 2.2250738585072014e-308;
+
+__device__ __forceinline__ double clip_fabs_fin(double v) { return isfinite(v) ? fabs(v) : 0.0; }
+
+__device__ void clip_planes(const double* A, const double* lbias, int S, int n, const double* xl, const double* xu,
+                            double* dm, double* dm_err, double* box_err) {
+  const int lane = threadIdx.x & 31;
+  const double under = (n + 16) * CLIP_TINY * CLIP_EPS;
+  for (int s = 0; s < S; ++s) {
+    const double* a = A + (int64_t)s * n;
+    double ax = 0, ae = 0, mag = 0;
+    for (int i = lane; i < n; i += 32) {
+      const double l = xl[i], u = xu[i], ai = a[i];
+      ax += ai * ((u + l) / 2);
+      ae += fabs(ai) * ((u - l) / 2);
+      mag += clip_fabs_fin(ai) * clip_fabs_fin(fmax(fabs(l), fabs(u)));
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      ax += __shfl_xor_sync(0xffffffffu, ax, o);
+      ae += __shfl_xor_sync(0xffffffffu, ae, o);
+      mag += __shfl_xor_sync(0xffffffffu, mag, o);
+    }
+    if (lane == 0) {
+      const double be = (mag + clip_fabs_fin(lbias[s])) * ((n + 16) * CLIP_EPS * 4);
+      dm[s] = ax - ae + lbias[s];
+      box_err[s] = be;
+      dm_err[s] = be * ((double)(n + 4) / (4.0 * (n + 16))) + under;
+    }
+  }
+  __syncwarp();
+}
+
+__global__ void clip_kernel(double* x_L, double* x_U, const double* thr, const double* lA, const double* lbias,
+                            const int32_t* parent, int64_t B, int S, int n, int num_iters, uint8_t* nonempty) {
+  extern __shared__ double clip_sm[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int64_t b = (int64_t)blockIdx.x * (blockDim.x >> 5) + wid;
+  if (b >= B) return;
+  double* dm = clip_sm + (size_t)wid * 3 * S;
+  double* dm_err = dm + S;
+  double* box_err = dm_err + S;
+  const int64_t p = parent ? parent[b] : b;
+  const double* A = lA + p * S * n;
+  const double* t = thr + p * S;
+  const double* lb_ = lbias + p * S;
+  double* xl = x_L + b * n;
+  double* xu = x_U + b * n;
+  // boxes with non-finite data stay as they are
+  int fin = 1;
+  for (int k = lane; k < S * n; k += 32) fin &= isfinite(A[k]) ? 1 : 0;
+  for (int s = lane; s < S; s += 32) fin &= ((isfinite(t[s]) || t[s] == INFINITY) && isfinite(lb_[s])) ? 1 : 0;
+  fin = __all_sync(0xffffffffu, fin);
+  if (fin) {
+    clip_planes(A, lb_, S, n, xl, xu, dm, dm_err, box_err);
+    const double under = (n + 16) * CLIP_TINY * CLIP_EPS;
+    int cert = 0;
+    for (int s = lane; s < S; s += 32) cert |= (dm[s] - box_err[s] - under > t[s]) ? 1 : 0;
+    cert = __any_sync(0xffffffffu, cert);
+    if (cert) {
+      if (lane == 0) xl[0] = next_up(xu[0]);
+    } else {
+      for (int it = 0; it < num_iters; ++it) {
+        if (it > 0) clip_planes(A, lb_, S, n, xl, xu, dm, dm_err, box_err);
+        for (int i = lane; i < n; i += 32) {
+          const double l = xl[i], u = xu[i];
+          const double xh = (u + l) / 2, e = (u - l) / 2;
+          double nu = u, nl = l;
+          for (int s = 0; s < S; ++s) {
+            const double ai = A[(int64_t)s * n + i];
+            if (!(ai > 0) && !(ai < 0)) continue;
+            const double ax = ai * xh, ae = fabs(ai) * e;
+            const double cmo = dm[s] - ax + ae;
+            const double num = t[s] - cmo;
+            const double mag = clip_fabs_fin(t[s]) + clip_fabs_fin(dm[s]) + clip_fabs_fin(ax) + clip_fabs_fin(ae);
+            const double err = mag * (4 * CLIP_EPS) + under + dm_err[s];
+            const bool f = isfinite(num);
+            const double lo_n = f ? num - err : num, hi_n = f ? num + err : num;
+            const double ql = lo_n / ai, qh = hi_n / ai;
+            if (ai > 0) nu = fmin(nu, next_up(fmax(ql, qh)));
+            else nl = fmax(nl, next_dn(fmin(ql, qh)));
+          }
+          xl[i] = nl;
+          xu[i] = nu;
+        }
+        __syncwarp();
+      }
+    }
+    __syncwarp();
+  }
+  if (nonempty) {
+    int ok = 1;
+    for (int i = lane; i < n; i += 32) ok &= (xl[i] <= xu[i]) ? 1 : 0;
+    ok = __all_sync(0xffffffffu, ok);
+    if (lane == 0) nonempty[b] = ok ? 1 : 0;
+  }
+}
+
 }  // namespace bab
 }  // namespace gear

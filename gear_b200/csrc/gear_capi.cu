@@ -419,6 +419,59 @@ extern "C" int gear_scatter_rows(const double* src, const int32_t* rows, int64_t
   return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_scatter_rows");
 }
 
+extern "C" int gear_clip_domains(double* x_L, double* x_U, const double* thr, const double* lA, const double* lbias,
+                                 const int32_t* parent, int64_t batch, int S, int n, int num_iters,
+                                 uint8_t* nonempty, void* stream) {
+  if (!x_L || !x_U || !thr || !lA || !lbias || batch < 0 || S < 1 || n < 1 || num_iters < 1)
+    return fail(GEAR_E_INVALID, "gear_clip_domains: %s", "bad arguments");
+  if (batch == 0) return GEAR_OK;
+  const size_t per = (size_t)3 * S * sizeof(double);
+  int warps = 8;
+  while (warps > 1 && per * warps > (size_t)(96 << 10)) warps >>= 1;
+  if (per * warps > (size_t)(200 << 10)) return fail(GEAR_E_INVALID, "gear_clip_domains: %s", "too many rows");
+  cudaError_t e = cudaFuncSetAttribute(gear::bab::clip_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(per * warps));
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+  gear::bab::clip_kernel<<<(unsigned)((batch + warps - 1) / warps), 32 * warps, per * warps, (cudaStream_t)stream>>>(
+      x_L, x_U, thr, lA, lbias, parent, batch, S, n, num_iters, nonempty);
+  g_launches = 1;
+  e = cudaGetLastError();
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_clip_domains");
+}
+
+extern "C" int gear_bab_child_keys(const double* lb, const double* lA, const double* lbias, const double* child_lo,
+                                   const double* child_hi, const int32_t* kept, int64_t n_kept, int S, int n,
+                                   double* child_key, void* stream) {
+  using namespace gear::bab;
+  if (!lb || !lA || !lbias || !child_lo || !child_hi || !kept || !child_key || n_kept < 0 || S < 1 || n < 1)
+    return fail(GEAR_E_INVALID, "gear_bab_child_keys: %s", "bad arguments");
+  if (n_kept == 0) return GEAR_OK;
+  child_keys_kernel<<<grid_for(2 * n_kept * 32), BT, 0, (cudaStream_t)stream>>>(lb, lA, lbias, child_lo, child_hi, kept,
+                                                                              n_kept, S, n, child_key);
+  g_launches = 1;
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_bab_child_keys");
+}
+
+extern "C" int gear_bab_compact(const uint8_t* keep, int64_t batch, int32_t* kept, int32_t* n_kept, void* workspace,
+                                int64_t ws_bytes, void* stream) {
+  using namespace gear::bab;
+  if (!keep || !kept || !n_kept || batch < 0) return fail(GEAR_E_INVALID, "gear_bab_compact: %s", "bad arguments");
+  if (!workspace || ws_bytes < gear_bab_workspace_bytes(batch))
+    return fail(GEAR_E_WORKSPACE, "gear_bab_compact: %s", "workspace too small");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (batch == 0) { cudaMemsetAsync(n_kept, 0, sizeof(int32_t), st); return GEAR_OK; }
+  int64_t nblocks = (batch + BT - 1) / BT;
+  if (nblocks > (int64_t)BT * 1024) return fail(GEAR_E_INVALID, "gear_bab_compact: %s", "batch too large");
+  int32_t* counts = (int32_t*)((char*)workspace + 64);
+  count_kernel<<<(unsigned)nblocks, BT, 0, st>>>(keep, batch, counts);
+  scan_counts_kernel<<<1, BT, 0, st>>>(counts, (int)nblocks, n_kept);
+  compact_kernel<<<(unsigned)nblocks, BT, 0, st>>>(keep, batch, counts, kept);
+  g_launches = 3;
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_bab_compact");
+}
+
 // ------------------------------------------------------------------ constrained concretisation
 namespace {
 struct CcLayout {

@@ -25,6 +25,9 @@
  *                        + child keys (_raise_child_keys)          batch_branch_and_bound.py:189-225
  *   gear_queue_order  <- UnsortedInputDomainList.sort / pick_out_batch  branching_domains.py:1171-1240, :831-962
  *   gear_gather_rows, gear_scatter_rows <- TensorStorage pop / append    complete_verifier/input_split/tensor_storage.py:351-408
+ *   gear_clip_domains <- clip_domains / _clip_main_fn (lower planes)  complete_verifier/input_split/clip.py:138-486
+ *   gear_bab_child_keys <- _raise_child_keys                      batch_branch_and_bound.py:189-225
+ *   gear_bab_compact  <- the index compaction of filter_verified_domains  branching_domains.py:238-410
  *   gear_constrained_lower <- sort_out_constr_batches + constraints_solving(sign=-1)
  *                        (+ drop_redundant_constraints, _solve_dual_var)  solver/auto_LiRPA/concretize_func.py:168-850
  */
@@ -115,6 +118,28 @@ int gear_gather_rows(const double* src, const int32_t* rows, int64_t count, int6
                      void* stream);
 int gear_scatter_rows(const double* src, const int32_t* rows, int64_t count, int64_t width, double* dst,
                       void* stream);
+
+/* Domain clipping, in place: shrink every box [x_L, x_U] (batch, n) along each coordinate to the
+ * part where each plane lA_s x + lbias_s (s < S) can still be <= thr_s, rounding every candidate
+ * outward; a box some plane already proves done becomes empty (x_L[0] = next double above x_U[0]).
+ * The planes of box b are row parent[b] of lA (.., S, n), lbias and thr (.., S) (parent NULL:
+ * row b). num_iters >= 1 repeats the clip with the plane minima of the clipped box. A box with a
+ * non-finite plane, bias or a -inf/NaN threshold is left as it is. nonempty (batch) or NULL
+ * receives 1 for a box that is not empty afterwards. */
+int gear_clip_domains(double* x_L, double* x_U, const double* thr, const double* lA, const double* lbias,
+                      const int32_t* parent, int64_t batch, int S, int n, int num_iters, uint8_t* nonempty,
+                      void* stream);
+
+/* Child keys of split children (child_lo, child_hi (2 n_kept, n), [upper halves; lower halves]
+ * of the parents kept[0..n_kept)): the parent's lb, row 0 raised to the parent plane's minimum
+ * over the child box, rounded down. */
+int gear_bab_child_keys(const double* lb, const double* lA, const double* lbias, const double* child_lo,
+                        const double* child_hi, const int32_t* kept, int64_t n_kept, int S, int n,
+                        double* child_key, void* stream);
+
+/* kept[0..n_kept) = the indices b with keep[b] != 0, in order. Workspace: gear_bab_workspace_bytes. */
+int gear_bab_compact(const uint8_t* keep, int64_t batch, int32_t* kept, int32_t* n_kept, void* workspace,
+                     int64_t ws_bytes, void* stream);
 
 /* ---------------------------------------------------------------- constrained concretisation */
 
