@@ -66,6 +66,9 @@ def lib():
         L.gear_bab_child_keys.restype = i32
         L.gear_bab_compact.argtypes = [vp, i64, vp, vp, vp, i64, vp]
         L.gear_bab_compact.restype = i32
+        L.gear_dual_lower_bound.argtypes = [vp, vp, vp, vp, i32, i64, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp,
+                                            i32, vp, vp, vp, vp]
+        L.gear_dual_lower_bound.restype = i32
         _LIB = L
     return _LIB
 
@@ -91,4 +94,5 @@ EXPORTED = ("gear_dag_create", "gear_dag_destroy", "gear_crown_workspace_bytes",
             "gear_last_launch_count", "gear_last_error", "gear_bab_workspace_bytes", "gear_bab_prune",
             "gear_bab_branch", "gear_bab_split", "gear_queue_order", "gear_gather_rows", "gear_scatter_rows",
             "gear_crown_lower_static", "gear_crown_static_scratch_bytes", "gear_constrained_workspace_bytes",
-            "gear_constrained_lower", "gear_clip_domains", "gear_bab_child_keys", "gear_bab_compact")
+            "gear_constrained_lower", "gear_clip_domains", "gear_bab_child_keys", "gear_bab_compact",
+            "gear_dual_lower_bound")

@@ -14,6 +14,7 @@
 #include "crown_simt.cuh"
 #include "bab_kernels.cuh"
 #include "concretize_kernels.cuh"
+#include "dual_kernels.cuh"
 
 namespace {
 thread_local std::string g_err;
@@ -470,6 +471,32 @@ extern "C" int gear_bab_compact(const uint8_t* keep, int64_t batch, int32_t* kep
   g_launches = 3;
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_bab_compact");
+}
+
+// ------------------------------------------------------------------ rigorous LP dual bound
+extern "C" int gear_dual_lower_bound(const int32_t* colptr, const int32_t* rows, const int32_t* perm, const double* val,
+                                     int val_batched, int64_t batch, int m, int n, int nnz, const double* c,
+                                     const double* c0, const double* h, const double* l, const double* u,
+                                     const double* y, const double* tol, const double* c_err, const double* c0_err,
+                                     int infeasibility, double* lb, double* E, uint8_t* dd, void* stream) {
+  g_launches = 0;
+  if (!colptr || (nnz > 0 && (!rows || !perm || !val)) || !h || !l || !u || !y || !lb || batch < 0 || m < 0 || n < 0 ||
+      nnz < 0)
+    return fail(GEAR_E_INVALID, "gear_dual_lower_bound: %s", "bad arguments");
+  if (batch == 0) return GEAR_OK;
+  const size_t smem = (size_t)m * sizeof(double);
+  if (smem > (size_t)(200 << 10)) return fail(GEAR_E_INVALID, "gear_dual_lower_bound: %s", "too many rows");
+  cudaError_t e = cudaFuncSetAttribute(gear::dual::dual_bound_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+  gear::dual::Lp p;
+  p.colptr = colptr; p.rows = rows; p.perm = perm; p.val = val; p.val_batched = val_batched;
+  p.c = c; p.c0 = c0; p.h = h; p.l = l; p.u = u; p.y = y; p.tol = tol; p.c_err = c_err; p.c0_err = c0_err;
+  p.lb = lb; p.E = E; p.dd = dd; p.B = batch; p.m = m; p.n = n; p.nnz = nnz; p.infeasibility = infeasibility;
+  gear::dual::dual_bound_kernel<<<(unsigned)batch, gear::dual::DT, smem, (cudaStream_t)stream>>>(p);
+  g_launches = 1;
+  e = cudaGetLastError();
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_dual_lower_bound");
 }
 
 // ------------------------------------------------------------------ constrained concretisation

@@ -28,6 +28,7 @@
  *   gear_clip_domains <- clip_domains / _clip_main_fn (lower planes)  complete_verifier/input_split/clip.py:138-486
  *   gear_bab_child_keys <- _raise_child_keys                      batch_branch_and_bound.py:189-225
  *   gear_bab_compact  <- the index compaction of filter_verified_domains  branching_domains.py:238-410
+ *   gear_dual_lower_bound <- dual_lower_bound / certify_infeasible    complete_verifier/nlp_solver/rigorous_dual.py:1-238
  *   gear_constrained_lower <- sort_out_constr_batches + constraints_solving(sign=-1)
  *                        (+ drop_redundant_constraints, _solve_dual_var)  solver/auto_LiRPA/concretize_func.py:168-850
  */
@@ -140,6 +141,22 @@ int gear_bab_child_keys(const double* lb, const double* lA, const double* lbias,
 /* kept[0..n_kept) = the indices b with keep[b] != 0, in order. Workspace: gear_bab_workspace_bytes. */
 int gear_bab_compact(const uint8_t* keep, int64_t batch, int32_t* kept, int32_t* n_kept, void* workspace,
                      int64_t ws_bytes, void* stream);
+
+/* ---------------------------------------------------------------- rigorous LP dual bound
+ * For each domain b: a float64 lb <= D(y) = c0 - h^T y + sum_j min(r_j l_j, r_j u_j), r = c + G^T y,
+ * the weak-duality bound of min c^T z + c0 s.t. G z <= h, l <= z <= u, exact on the given floats
+ * (rounding enclosed; double-double recomputation of r where the error term exceeds tol/10, tol
+ * NULL: max(1e-5, 1e-4 |value|)). G: m x n, nnz entries in CSC order: colptr (n+1), rows (nnz),
+ * perm (nnz) = entry index of each CSC position into val (val_batched ? (batch, nnz) : (1, nnz)),
+ * entries of a column in their original order. c, c_err (batch, n), c0, c0_err (batch) may be
+ * NULL (zero). y < 0 counts as 0. -inf where nothing is certified. infeasibility = 1: the
+ * double-double rule of certify_infeasible (c = c0 = 0 then; lb > 0 proves G z <= h infeasible on
+ * the box). E (batch) and dd (batch, 1 = double-double used) may be NULL. */
+int gear_dual_lower_bound(const int32_t* colptr, const int32_t* rows, const int32_t* perm, const double* val,
+                          int val_batched, int64_t batch, int m, int n, int nnz, const double* c, const double* c0,
+                          const double* h, const double* l, const double* u, const double* y, const double* tol,
+                          const double* c_err, const double* c0_err, int infeasibility, double* lb, double* E,
+                          uint8_t* dd, void* stream);
 
 /* ---------------------------------------------------------------- constrained concretisation */
 
