@@ -42,4 +42,25 @@ class SinWide(torch.nn.Module):
         return torch.cat([(a + b).sum(1, keepdim=True), (a * b).sum(1, keepdim=True)], 1)
 
 
-MODELS = {"mixed_ops": (MixedOps, 6), "sin_wide": (SinWide, 5)}
+class DirectOps(torch.nn.Module):
+    """Only operators the reference's direct program emitter accepts (nn.Linear with bias, cos,
+    neg, sub, slices, gathers, unsqueeze, pow 2, exp, log, concatenation)."""
+
+    def __init__(self, seed=5):
+        super().__init__()
+        g = torch.Generator().manual_seed(seed)
+        self.lin = torch.nn.Linear(6, 3).to(F64)
+        with torch.no_grad():
+            self.lin.weight.copy_(torch.randn(3, 6, generator=g, dtype=F64))
+            self.lin.bias.copy_(torch.randn(3, generator=g, dtype=F64))
+        self.register_buffer("idx", torch.tensor([4, 0, 2]))
+        self.box = (-1.0, 1.0)
+
+    def forward(self, x):
+        y = self.lin(x)
+        z = torch.cos(x[:, 1:4]) - y * x[:, self.idx] + torch.exp(-y) + (y ** 2)
+        w = torch.log(x[:, 0:3] * x[:, 3:6] + 2.0)
+        return torch.cat([z.sum(1, keepdim=True), (-x[:, 5]).unsqueeze(1), w.sum(1, keepdim=True)], 1)
+
+
+MODELS = {"mixed_ops": (MixedOps, 6), "sin_wide": (SinWide, 5), "direct_ops": (DirectOps, 6)}

@@ -87,3 +87,22 @@ def test_auto_engine_picks_a_variant_and_matches_oracle(workload, batch):
     olb, _, olA, olbias = CrownOracle(g).compute_bounds(lo.numpy(), hi.numpy())
     assert _close(first[0].cpu().numpy(), olb) < RTOL
     assert _close(first[1].cpu().numpy(), olA) < RTOL
+
+
+def test_gpu_bounds_of_a_lowered_node_program():
+    """A NodeProgram from the reference's gear front end, lowered to the IR, bounds on the GPU
+    exactly like the directly traced model."""
+    import os
+    from gear_b200.lowering import ProgramModule
+    data = torch.load(os.path.join(os.path.dirname(__file__), "golden", "programs.pt"), weights_only=False)
+    p = data["programs"]["dense_q_n200"]
+    m = problems.make_instance("dense_q_n200", 0)
+    lo, hi = problems.make_boxes("dense_q_n200", 96, 0)
+    prog = ProgramModule(p["nodes_op"], p["nodes_in"], p["nodes_out"])
+    a = BoundedModule(prog, lo[:2], device="cuda")
+    b = BoundedModule(m, lo[:2], device="cuda")
+    x = BoundedTensor(lo.cuda(), PerturbationLpNorm(x_L=lo.cuda(), x_U=hi.cuda()))
+    la, _, Aa = a.compute_bounds(x=(x,), method="CROWN", bound_upper=False, return_A=True)
+    lb, _, Ab = b.compute_bounds(x=(x,), method="CROWN", bound_upper=False, return_A=True)
+    assert torch.equal(la, lb)
+    assert torch.equal(Aa["/y"]["/x"]["lA"], Ab["/y"]["/x"]["lA"])
