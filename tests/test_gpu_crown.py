@@ -99,8 +99,9 @@ def test_gpu_bounds_of_a_lowered_node_program():
     m = problems.make_instance("dense_q_n200", 0)
     lo, hi = problems.make_boxes("dense_q_n200", 96, 0)
     prog = ProgramModule(p["nodes_op"], p["nodes_in"], p["nodes_out"])
-    a = BoundedModule(prog, lo[:2], device="cuda")
-    b = BoundedModule(m, lo[:2], device="cuda")
+    opts = {"gear_mode": "cta"}            # one kernel for both: identical arithmetic
+    a = BoundedModule(prog, lo[:2], device="cuda", bound_opts=opts)
+    b = BoundedModule(m, lo[:2], device="cuda", bound_opts=opts)
     x = BoundedTensor(lo.cuda(), PerturbationLpNorm(x_L=lo.cuda(), x_U=hi.cuda()))
     la, _, Aa = a.compute_bounds(x=(x,), method="CROWN", bound_upper=False, return_A=True)
     lb, _, Ab = b.compute_bounds(x=(x,), method="CROWN", bound_upper=False, return_A=True)
