@@ -309,6 +309,83 @@ __device__ void relax_mul(double xl, double xu, double yl, double yu, double* p)
   p[5] = (yl * xu - yu * xl) * r_u - yl * xu;
 }
 
+// ------------------------------------------------------------------ powers (BoundPow)
+// Parameters of a pow node: dp[N_CVEC] = {exponent, class, table length}, class 0 = odd
+// integer, 1 = even integer, 2 = non-integer (base restricted to x >= 0); an odd exponent's
+// tangent-point tables d_lower, d_upper (grid 0.01) start at dp[N_MAP0].
+enum { POW_ODD = 0, POW_EVEN = 1, POW_FRAC = 2 };
+
+__device__ __forceinline__ double pow_table_pick(const double* t, int len, double bound, double dflt) {
+  // retrieve_from_precompute: entry trunc(bound / 0.01) + 1 (at least 1), else the default
+  const double v = bound / STEP_PRE;
+  if (!(v < 1.0e15)) return dflt;
+  const long long i = (v > 0 ? (long long)v : 0) + 1;
+  return i < len ? t[i] : dflt;
+}
+
+// BoundPow.bound_relax (operators/s_shaped.py:881-1035), plain CROWN; u already raised to
+// lower + 1e-8 by the caller (bound_backward). q = (lw, lb, uw, ub).
+__device__ void relax_pow(const DevProgram* P, const int32_t* nd, double l, double u, double* q) {
+  const double* pp = P->dp + nd[N_CVEC];
+  const double p = pp[0];
+  const int cls = (int)pp[1];
+  if (cls == POW_ODD) {
+    const int len = (int)pp[2];
+    const double* dlo_t = P->dp + nd[N_MAP0];
+    const double* dup_t = dlo_t + len;
+    auto f = [&](double x) { return pow(x, p); };
+    auto df = [&](double x) { return p * pow(x, p - 1); };
+    auto d2 = [&](double x) { return p * (p - 1) * pow(x, p - 2); };
+    const double yl = f(l), yu = f(u), width = u - l;
+    double kd = (yu - yl) / fmax(width, 1e-8);
+    if (width < 1e-8) kd = df(l);
+    const bool conv = d2(l) >= 0;
+    const bool mneg = d2(l) >= 0 && d2(u) >= 0, mpos = d2(l) < 0 && d2(u) < 0, mboth = !(mneg || mpos);
+    double lw = 0, lb = 0, uw = 0, ub = 0;
+    if (mneg) { uw = kd; ub = -l * kd + yl; }
+    if (mpos) { lw = kd; lb = -l * kd + yl; }
+    const double dup = pow_table_pick(dup_t, len, u, l);
+    const double dlo = pow_table_pick(dlo_t, len, -l, u);
+    const bool dl_dir = (conv ? kd < df(l) : kd > df(u)) && mboth;
+    const bool du_dir = (conv ? kd < df(u) : kd > df(l)) && mboth;
+    const double m = (l + u) / 2, ym = f(m), km = df(m);
+    if (mneg) { lw = km; lb = -m * km + ym; }
+    if (mpos) { uw = km; ub = -m * km + ym; }
+    if (dl_dir) { lw = kd; lb = -l * kd + yl; }
+    if (mboth && !dl_dir) { const double k = df(dlo); lw = k; lb = -dlo * k + f(dlo); }
+    if (du_dir) { uw = kd; ub = -l * kd + yl; }
+    if (mboth && !du_dir) { const double k = df(dup); uw = k; ub = -dup * k + f(dup); }
+    // inverse-S smoothing: the tangent at the midpoint where the table's point is on the far side
+    if (mboth && dlo < m) { lw = km; lb = -m * km + ym; }
+    if (mboth && dup >= m) { uw = km; ub = -m * km + ym; }
+    q[0] = lw; q[1] = lb; q[2] = uw; q[3] = ub;
+    return;
+  }
+  if (cls == POW_EVEN) {
+    const double yl = pow(l, p), yu = pow(u, p);
+    const double eps = fmax(fabs(yl), fabs(yu)) * 1e-6 + 1e-12;
+    const double uk = (yu - yl) / fmax(u - l, 1e-8);
+    const double mid = l >= 0 ? l : (u <= 0 ? u : 0.0);
+    const double lk = p * pow(mid, p - 1);
+    q[0] = lk; q[1] = -mid * lk + (pow(mid, p) - eps);
+    q[2] = uk; q[3] = -l * uk + (yl + eps);
+    return;
+  }
+  // non-integer exponent, l >= 0: concave (p < 1) or convex (p > 1) tangent and secant
+  const double lt = p < 1 ? fmax(l, 1e-9) : l;
+  const double fl = (p < 1 && l == 0) ? 0.0 : pow(l, p);
+  const double fu = pow(u, p);
+  const double ks = (fu - fl) / fmax(u - l, 1e-8);
+  const double m = (lt + u) / 2;
+  double kt, fm;
+  if (p > 1 && m == 0) { kt = 0; fm = 0; }
+  else { kt = p * pow(m, p - 1); fm = pow(m, p); }
+  if (p < 1) { q[0] = ks; q[1] = -l * ks + fl; q[2] = kt; q[3] = -m * kt + fm; }
+  else { q[0] = kt; q[1] = -m * kt + fm; q[2] = ks; q[3] = -l * ks + fl; }
+}
+
+__device__ __forceinline__ double magnitude(double l, double h) { return l > h ? INFINITY : fmax(-l, h); }
+
 // ------------------------------------------------------------------ per-box context
 struct Box {
   const DevProgram* P;
@@ -403,6 +480,26 @@ __device__ void ibp_element_t(const DevProgram* P, V lo, V hi, const int32_t* nd
         };
         h = crossing(xl, xu, maxp) ? 1.0 : pmax(fl, fu);
         l = crossing(xl, xu, minp) ? -1.0 : pmin(fl, fu);
+      }
+      break;
+    }
+    case NK_POW: {
+      // interval_propagate (s_shaped.py:1083-1121)
+      const int32_t* a = node_rec(P, nd[N_IN0]);
+      double xl = lo[a[N_CUR] + j], xu = hi[a[N_CUR] + j];
+      const double* pp = P->dp + nd[N_CVEC];
+      const double p = pp[0];
+      const int cls = (int)pp[1];
+      if (cls == POW_FRAC) {
+        l = pow(fmax(xl, 0.0), p);
+        h = pow(xu, p);
+      } else {
+        const double pl = pow(xl, p), pu = pow(xu, p);
+        if (cls == POW_ODD) { l = pl; h = pu; }
+        else {
+          l = (xl < 0 && xu > 0) ? 0.0 : fmin(pl, pu);
+          h = fmax(pl, pu);
+        }
       }
       break;
     }
@@ -605,8 +702,16 @@ __device__ void relax_node(const Box& bx, int v) {
       const int32_t* a = node_rec(P, nd[N_IN0]);
       double l = bx.lo[a[N_CUR] + j], u = bx.hi[a[N_CUR] + j];
       double* p = pl + 4 * j;
+      if (kind == NK_POW) {
+        // bound_backward raises the input's stored upper bound to lower + 1e-8 (persistent)
+        u = fmax(u, l + 1e-8);
+        bx.hi[a[N_CUR] + j] = u;
+        bx.mag[a[N_CUR] + j] = magnitude(l, u);
+        if ((int)P->dp[nd[N_CVEC] + 1] == POW_FRAC) l = fmax(l, 0.0);   // base restricted to x >= 0
+      }
       bool bad = !(isfinite(l) && isfinite(u));
       if (kind == NK_LOG) bad = bad || !(l > 0);
+      if (kind == NK_POW) bad = bad || !(u >= 0 || (int)P->dp[nd[N_CVEC] + 1] != POW_FRAC);
       if (bad) {
         p[0] = p[1] = p[2] = p[3] = NAN;
       } else if (kind == NK_SQR) relax_sqr(l, u, p);
@@ -614,6 +719,7 @@ __device__ void relax_node(const Box& bx, int v) {
       else if (kind == NK_LOG) relax_log(l, u, p);
       else if (kind == NK_SIN) relax_sin(T, l, u, p);
       else if (kind == NK_COS) relax_cos(T, l, u, p);
+      else if (kind == NK_POW) relax_pow(P, nd, l, u, p);
     }
   }
 }
@@ -669,7 +775,7 @@ __device__ __forceinline__ double elem_coef(int kind, int slot, int side, double
                                             double cval, double* bterm) {
   *bterm = 0.0;
   switch (kind) {
-    case NK_SQR: case NK_EXP: case NK_LOG: case NK_SIN: case NK_COS: {
+    case NK_SQR: case NK_EXP: case NK_LOG: case NK_SIN: case NK_COS: case NK_POW: {
       // lower side: positive -> (lw, lb), negative -> (uw, ub); upper side: reversed
       double wp = side == 0 ? pl[0] : pl[2], bp = side == 0 ? pl[1] : pl[3];
       double wn = side == 0 ? pl[2] : pl[0], bn = side == 0 ? pl[3] : pl[1];
@@ -812,7 +918,8 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
     const int32_t* vrp = P->ip + op[O_VRP];
     const int32_t* vcols = P->ip + op[O_VCOLS];
     const double* pl = vnd[N_PLANE] >= 0 ? bx.planes + vnd[N_PLANE] : nullptr;
-    const bool relax = (kind == NK_SQR || kind == NK_EXP || kind == NK_LOG || kind == NK_SIN || kind == NK_COS);
+    const bool relax = (kind == NK_SQR || kind == NK_EXP || kind == NK_LOG || kind == NK_SIN || kind == NK_COS ||
+                        kind == NK_POW);
     const int ppe = kind == NK_MUL ? 6 : 4;
     const int u = op[O_U];
     const int32_t* und = u >= 0 ? node_rec(P, u) : nullptr;
@@ -1156,8 +1263,6 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
   }
   __syncthreads();
 }
-
-__device__ __forceinline__ double magnitude(double l, double h) { return l > h ? INFINITY : fmax(-l, h); }
 
 template <int NT>
 __device__ void compare_node(const Box& bx, int v, double* tmp_lo, double* tmp_hi, bool with_mag) {

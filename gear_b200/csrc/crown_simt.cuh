@@ -156,15 +156,24 @@ __device__ void simt_relax_node(const SBox& bx, int v) {
       for (int k = 0; k < 6; ++k) pl[6 * j + k] = q[k];
     } else {
       double l = bx.lo[a[N_CUR] + j], u = bx.hi[a[N_CUR] + j];
+      if (kind == NK_POW) {
+        // bound_backward raises the input's stored upper bound to lower + 1e-8 (persistent)
+        u = fmax(u, l + 1e-8);
+        bx.hi[a[N_CUR] + j] = u;
+        bx.mag[a[N_CUR] + j] = magnitude(l, u);
+        if ((int)P->dp[nd[N_CVEC] + 1] == POW_FRAC) l = fmax(l, 0.0);
+      }
       bool bad = !(isfinite(l) && isfinite(u));
       if (kind == NK_LOG) bad = bad || !(l > 0);
+      if (kind == NK_POW) bad = bad || !(u >= 0 || (int)P->dp[nd[N_CVEC] + 1] != POW_FRAC);
       if (bad) {
         q[0] = q[1] = q[2] = q[3] = NAN;
       } else if (kind == NK_SQR) relax_sqr(l, u, q);
       else if (kind == NK_EXP) relax_exp(l, u, q);
       else if (kind == NK_LOG) relax_log(l, u, q);
       else if (kind == NK_SIN) relax_sin(T, l, u, q);
-      else relax_cos(T, l, u, q);
+      else if (kind == NK_COS) relax_cos(T, l, u, q);
+      else relax_pow(P, nd, l, u, q);
       for (int k = 0; k < 4; ++k) pl[4 * j + k] = q[k];
     }
   }
@@ -215,7 +224,8 @@ __device__ void simt_run_pass(const SBox& bx, int pid, const Work& wk, bool live
     const int32_t* vcols = P->ip + op[O_VCOLS];
     const bool has_pl = vnd[N_PLANE] >= 0;
     SView pl = has_pl ? bx.planes + vnd[N_PLANE] : bx.planes;
-    const bool relax = (kind == NK_SQR || kind == NK_EXP || kind == NK_LOG || kind == NK_SIN || kind == NK_COS);
+    const bool relax = (kind == NK_SQR || kind == NK_EXP || kind == NK_LOG || kind == NK_SIN || kind == NK_COS ||
+                        kind == NK_POW);
     const int ppe = kind == NK_MUL ? 6 : 4;
     const int u = op[O_U];
     const int32_t* und = u >= 0 ? node_rec(P, u) : nullptr;

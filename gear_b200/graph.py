@@ -480,6 +480,10 @@ class _TraceMode(TorchFunctionMode):
                 raise GraphError("variable exponent")
             p = args[1]
             p = float(p.item()) if _is_tensor(p) else float(p)
+            if p == 1.0:
+                return self.nid(args[0])             # x ** 1 is x (BoundPow passes A through)
+            if not (p > 0) or math.isinf(p):
+                raise GraphError(f"pow with exponent {p}: only positive finite exponents are supported")
             return g.add("pow", [self.nid(args[0])], self.per_box_shape(out), exponent=p)
         if func in (T.sum, torch.sum):
             x = args[0]

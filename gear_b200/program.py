@@ -164,8 +164,6 @@ class Program:
         off = 0
         for nd in g.nodes:
             if nd.kind in PLANES_PER_ELEM:
-                if nd.kind == "pow":
-                    raise ProgramError("pow with exponent other than 2 is not supported by the GPU engine")
                 self.plane_off[nd.id] = off
                 off += nd.width * PLANES_PER_ELEM[nd.kind]
         self.plane_w = off
@@ -418,6 +416,22 @@ class Program:
                 r[N_MAP0] = P.add_int(a["cmap"])
                 r[N_INS] = P.add_int(nd.inputs)
                 r[N_WIN] = sum(g[q].width for q in nd.inputs)
+            elif k == "pow":
+                # {exponent, class (0 odd, 1 even integer, 2 non-integer), table length}; an odd
+                # exponent's tangent tables (d_lower then d_upper) at N_MAP0, a float64-pool offset
+                pexp = float(a["exponent"])
+                if not (pexp > 0) or not np.isfinite(pexp):
+                    raise ProgramError(f"pow with exponent {pexp} is not supported")
+                if pexp == int(pexp):
+                    cls = 0 if int(pexp) % 2 == 1 else 1
+                else:
+                    cls = 2
+                tlen = 0
+                if cls == 0:
+                    d_lo, d_up = tables.pow_tables_cached(int(pexp))
+                    tlen = d_lo.size
+                    r[N_MAP0] = P.add_dbl(np.concatenate([d_lo, d_up]))
+                r[N_CVEC] = P.add_dbl(np.array([pexp, float(cls), float(tlen)]))
             elif k in ("linear", "matmul"):
                 W = a["W"] if k == "linear" else a["W"].T      # (out, in)
                 r[N_W_OFF] = P.add_dbl(np.ascontiguousarray(W))

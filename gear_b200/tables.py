@@ -118,3 +118,62 @@ def build():
 
 SIN_TABLE_ORDER = ("d_lower", "d_upper", "xl_lower_d", "xl_lower_c", "xl_upper_d", "xl_upper_c",
                    "xu_lower_d", "xu_lower_c", "xu_upper_d", "xu_upper_c")
+
+
+# ---------------------------------------------------------------- odd integer powers
+POW_X_LIMIT = 500.0
+_POW_CACHE = {}
+
+
+def pow_tables_cached(p: int):
+    """pow_tables(p), built once per process."""
+    if p not in _POW_CACHE:
+        _POW_CACHE[p] = pow_tables(p)
+    return _POW_CACHE[p]
+
+
+@torch.no_grad()
+def pow_tables(p: int, max_iter: int = 100):
+    """Tangent-point tables of an odd power x**p on the grid 0.01 * [0, 50005) (the reference's
+    BoundPow.precompute_relaxation, auto_LiRPA/operators/s_shaped.py:695-764, x_limit 500):
+    d_upper[i] <= 0 is the tangent point whose tangent stays above the curve up to 0.01 i, and
+    d_lower[i] >= 0 the one whose tangent stays below it down to -0.01 i. 100-step bisections in
+    float64 on the CPU. Returns (d_lower, d_upper) as float64 numpy arrays."""
+    func = lambda x: torch.pow(x, p)
+    dfunc = lambda x: p * torch.pow(x, p - 1)
+    n = int(POW_X_LIMIT / STEP_PRE)
+
+    def below(up, d):        # the tangent at d lower-bounds the curve at up
+        return dfunc(d) * (up - d) + func(d) <= func(up)
+
+    def above(lo, d):        # the tangent at d upper-bounds the curve at lo
+        return dfunc(d) * (lo - d) + func(d) >= func(lo)
+
+    upper = STEP_PRE * torch.arange(0, n + 5, dtype=torch.float64)
+    r = torch.zeros_like(upper)
+    l = -torch.ones_like(upper)
+    while True:
+        c = above(upper, l).int()
+        l = c * l + (1 - c) * (l * 2)
+        if c.sum() == l.numel():
+            break
+    for _ in range(max_iter):
+        m = (l + r) / 2
+        c = above(upper, m).int()
+        l = c * m + (1 - c) * l
+        r = c * r + (1 - c) * m
+    d_upper = l.clone()
+    lower = -STEP_PRE * torch.arange(0, n + 5, dtype=torch.float64)
+    l = torch.zeros_like(upper)
+    r = torch.ones_like(upper)
+    while True:
+        c = below(lower, r).int()
+        r = c * r + (1 - c) * (r * 2)
+        if c.sum() == l.numel():
+            break
+    for _ in range(max_iter):
+        m = (l + r) / 2
+        c = below(lower, m).int()
+        l = (1 - c) * m + c * l
+        r = (1 - c) * r + c * m
+    return r.clone().numpy(), d_upper.numpy()

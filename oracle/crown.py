@@ -122,6 +122,110 @@ def relax_exp(l, u):
     return lw, lb, uw, ub
 
 
+def _pw(x, p):
+    """x ** p as the reference evaluates it (torch.pow on float64 tensors)."""
+    import torch
+    return torch.pow(torch.as_tensor(np.asarray(x, np.float64)), p).numpy()
+
+
+def _retrieve(table, bound, default):
+    """retrieve_from_precompute (s_shaped.py:223-245): index trunc(bound / 0.01) + 1."""
+    with np.errstate(invalid="ignore"):
+        idx = np.maximum(np.trunc(bound / 0.01), 0)
+    idx = np.where(np.isfinite(idx), idx, len(table)).astype(np.float64) + 1
+    inside = idx < len(table)
+    return np.where(inside, table[np.minimum(idx, len(table) - 1).astype(np.int64)], default)
+
+
+def relax_pow(l, u, p):
+    """BoundPow.bound_relax (operators/s_shaped.py:881-1035), plain CROWN, for an exponent p that
+    is an integer >= 3 (odd: inverse-S relaxation with tangent tables, even: convex with the 1e-6
+    relative widening) or a non-integer > 0 (x >= 0: convex / concave tangent and secant). The
+    input upper bound is first raised to lower + 1e-8 (bound_backward, :791/:801)."""
+    u = np.maximum(u, l + 1e-8)
+    if p == int(p) and int(p) % 2 == 1:
+        from .pow_tables import tables
+        p = int(p)
+        f = lambda x: _pw(x, p)
+        df = lambda x: p * _pw(x, p - 1)
+        d2 = lambda x: p * (p - 1) * _pw(x, p - 2)
+        y_l, y_u = f(l), f(u)
+        width = u - l
+        k_dir = (y_u - y_l) / np.maximum(width, 1e-8)
+        k_dir = np.where(width < 1e-8, df(l), k_dir)
+        conv = d2(l) >= 0
+        mneg = (d2(l) >= 0) & (d2(u) >= 0)
+        mpos = (d2(l) < 0) & (d2(u) < 0)
+        mboth = ~(mneg | mpos)
+        lw, lb, uw, ub = [np.zeros_like(l) for _ in range(4)]
+
+        def put(mask, kind, k, x0, y0):
+            nonlocal lw, lb, uw, ub
+            k = np.broadcast_to(k, l.shape)
+            b = -x0 * k + y0
+            if kind == "lower":
+                lw, lb = np.where(mask, k, lw), np.where(mask, b, lb)
+            else:
+                uw, ub = np.where(mask, k, uw), np.where(mask, b, ub)
+        put(mneg, "upper", k_dir, l, y_l)
+        put(mpos, "lower", k_dir, l, y_l)
+        d_lo_t, d_up_t = tables(p)
+        d_upper = _retrieve(d_up_t, u, l)
+        d_lower = _retrieve(d_lo_t, -l, u)
+        dl_dir = np.where(conv, k_dir < df(l), k_dir > df(u)) & mboth
+        du_dir = np.where(conv, k_dir < df(u), k_dir > df(l)) & mboth
+        m = (l + u) / 2
+        y_m, k_m = f(m), df(m)
+        put(mneg, "lower", k_m, m, y_m)
+        put(mpos, "upper", k_m, m, y_m)
+        put(dl_dir, "lower", k_dir, l, y_l)
+        put(mboth & ~dl_dir, "lower", df(d_lower), d_lower, f(d_lower))
+        put(du_dir, "upper", k_dir, l, y_l)
+        put(mboth & ~du_dir, "upper", df(d_upper), d_upper, f(d_upper))
+        put(mboth & (d_lower < m), "lower", k_m, m, y_m)
+        put(mboth & (d_upper >= m), "upper", k_m, m, y_m)
+        return lw, lb, uw, ub
+    if p == int(p):
+        p = int(p)
+        y_l, y_u = _pw(l, p), _pw(u, p)
+        eps = np.maximum(np.abs(y_l), np.abs(y_u)) * 1e-6 + 1e-12
+        uk = (y_u - y_l) / np.maximum(u - l, 1e-8)
+        ub = -l * uk + (y_l + eps)
+        mid = np.where(l >= 0, l, np.where(u <= 0, u, 0.0))
+        lk = p * _pw(mid, p - 1)
+        lb = -mid * lk + (_pw(mid, p) - eps)
+        return lk, lb, uk, ub
+    # non-integer exponent on x >= 0
+    l_t = np.maximum(l, 1e-9) if p < 1 else l
+    if p < 1:
+        zl = l == 0
+        f_l = np.where(zl, 0.0, _pw(np.where(zl, 1.0, l), p))
+    else:
+        f_l = _pw(l, p)
+    f_u = _pw(u, p)
+    k_s = (f_u - f_l) / np.maximum(u - l, 1e-8)
+    m = (l_t + u) / 2
+    if p > 1:
+        z = m == 0
+        ms = np.where(z, 1.0, m)
+        k_t = np.where(z, 0.0, p * _pw(ms, p - 1))
+        f_m = np.where(z, 0.0, _pw(ms, p))
+    else:
+        k_t = p * _pw(m, p - 1)
+        f_m = _pw(m, p)
+    if p < 1:
+        return k_s, -l * k_s + f_l, k_t, -m * k_t + f_m
+    return k_t, -m * k_t + f_m, k_s, -l * k_s + f_l
+
+
+def pow_domain(l, u, p):
+    """The interval BoundPow relaxes: a non-integer exponent restricts the base to x >= 0
+    (domain_aware_ops); an interval entirely below 0 has no relaxation (undefined)."""
+    if p == int(p):
+        return l, u, np.zeros(np.shape(l), bool)
+    return np.maximum(l, 0.0), u, ~(u >= 0)
+
+
 def relax_log(l, u):
     """operators/convex_concave.py:64-92 (input already known to be > 0)."""
     with np.errstate(all="ignore"):
@@ -426,6 +530,16 @@ def ibp_node(n, ivs):
             lo, hi = ivs[0]
             l2 = np.where(hi < 0, hi ** 2, np.where(lo > 0, lo ** 2, 0.0))
             return l2, np.maximum(lo ** 2, hi ** 2)
+        if k == "pow":
+            lo, hi = ivs[0]
+            p = float(a["exponent"])
+            if p == int(p):
+                pl, pu = _pw(lo, int(p)), _pw(hi, int(p))
+                if int(p) % 2 == 1:
+                    return pl, pu
+                cross = (lo < 0) & (hi > 0)
+                return np.where(cross, 0.0, np.minimum(pl, pu)), np.maximum(pl, pu)
+            return _pw(np.maximum(lo, 0.0), p), _pw(hi, p)
         if k == "exp":
             lo, hi = ivs[0]
             return np.exp(lo), np.exp(hi)
@@ -530,6 +644,19 @@ class CrownOracle:
             bad = ~(np.isfinite(l) & np.isfinite(u))
             if k == "log":
                 bad = bad | ~(l > 0)
+            if k == "pow":
+                # BoundPow.bound_backward raises the input node's stored upper bound to
+                # lower + 1e-8 before relaxing (s_shaped.py:791, :801); the change persists
+                i0 = n.inputs[0]
+                with np.errstate(invalid="ignore"):
+                    u = np.maximum(u, l + 1e-8)
+                self.bounds[i0] = (self.bounds[i0][0], u)
+                if i0 in self.computed:
+                    c_l, c_u = self.computed[i0]
+                    with np.errstate(invalid="ignore"):
+                        self.computed[i0] = (c_l, np.maximum(c_u, c_l + 1e-8))
+                l, u, off = pow_domain(l, u, float(n.attrs["exponent"]))
+                bad = bad | off
             ls, us = np.where(bad, 0.0, l), np.where(bad, 1.0, u)
             if k == "sqr":
                 p = relax_sqr(ls, us)
@@ -541,6 +668,9 @@ class CrownOracle:
                 p = self.sin.relax_sin(ls, us)
             elif k == "cos":
                 p = self.sin.relax_cos(ls, us)
+            elif k == "pow":
+                with np.errstate(all="ignore"):
+                    p = relax_pow(ls, us, float(n.attrs["exponent"]))
             else:
                 raise NotImplementedError(k)
             p = tuple(np.where(bad, 0.0, q) for q in p)

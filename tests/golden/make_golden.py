@@ -87,6 +87,11 @@ def main(ref_root):
     cases.append(("dense_a_n2048", 0, 2))
     cases.append(("mixed_ops", 0, 12))
     cases.append(("sin_wide", 0, 12))
+    cases.append(("pow_ops", 0, 12))
+    cases.append(("pow_ops", 1, 12))
+    only = set(sys.argv[2:])
+    if only:
+        cases = [c for c in cases if c[0] in only]
 
     for name, inst, batch in cases:
         if name in problems.WORKLOADS:

@@ -63,4 +63,23 @@ class DirectOps(torch.nn.Module):
         return torch.cat([z.sum(1, keepdim=True), (-x[:, 5]).unsqueeze(1), w.sum(1, keepdim=True)], 1)
 
 
-MODELS = {"mixed_ops": (MixedOps, 6), "sin_wide": (SinWide, 5), "direct_ops": (DirectOps, 6)}
+class PowOps(torch.nn.Module):
+    """Odd, even and fractional powers (BoundPow): x**3, x**4, x**5 and (x + 2)**1.5, (x + 2)**0.5."""
+
+    def __init__(self, seed=9):
+        super().__init__()
+        g = torch.Generator().manual_seed(seed)
+        for name, k in (("a", 4), ("b", 4), ("c", 4), ("d", 4)):
+            self.register_buffer(name, torch.randn(k, generator=g, dtype=F64))
+        self.box = (-1.2, 1.5)
+
+    def forward(self, x):
+        t3 = (x[:, 0:4] ** 3 * self.a).sum(1, keepdim=True)
+        t4 = (x[:, 1:5] ** 4 * self.b).sum(1, keepdim=True)
+        z = x[:, 2:6] + 2.0
+        t15 = (z ** 1.5 * self.c).sum(1, keepdim=True)
+        t05 = (z ** 0.5 * self.d).sum(1, keepdim=True)
+        return torch.cat([t3 + t4, t15 - t05, (x[:, 5] ** 5).unsqueeze(1)], 1)
+
+
+MODELS = {"mixed_ops": (MixedOps, 6), "sin_wide": (SinWide, 5), "direct_ops": (DirectOps, 6), "pow_ops": (PowOps, 6)}

@@ -31,8 +31,15 @@ def test_simt_matches_oracle_on_fixture_boxes(case):
     torch.cuda.synchronize()
     olb, _, olA, olbias = CrownOracle(g).compute_bounds(d["x_L"], d["x_U"], d["C"])
     assert _close(lb.cpu().numpy(), olb) < RTOL
-    assert _close(lA.cpu().numpy(), olA) < RTOL
-    assert _close(lbias.cpu().numpy(), olbias) < RTOL
+    # On a degenerate box a power's relaxation is a secant over the reference's 1e-8 widening:
+    # its slope amplifies the last-bit difference of pow (torch on the CPU vs CUDA) by ~1e8, so
+    # the planes (lA, lbias) there agree to 1e-6; the bound itself still agrees to RTOL.
+    lA_, lbias_ = lA.cpu().numpy(), lbias.cpu().numpy()
+    flat = (d["x_U"] - d["x_L"]).min(1) < 1e-6
+    tol = np.where(flat & any(nd.kind == "pow" for nd in g.nodes), 1e-6, RTOL)
+    for b in range(lA_.shape[0]):
+        assert _close(lA_[b], olA[b]) < tol[b]
+        assert _close(lbias_[b], olbias[b]) < tol[b]
 
 
 # batches that are not a multiple of the 64-box tile exercise the tail threads
