@@ -33,6 +33,10 @@ def lib():
                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                        ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
         L.gear_crown_lower.restype = ctypes.c_int
+        L.gear_crown_lower_ibp.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
+        L.gear_crown_lower_ibp.restype = ctypes.c_int
         L.gear_last_error.argtypes = []
         L.gear_last_error.restype = ctypes.c_char_p
         L.gear_last_launch_count.argtypes = []
@@ -95,4 +99,4 @@ EXPORTED = ("gear_dag_create", "gear_dag_destroy", "gear_crown_workspace_bytes",
             "gear_bab_branch", "gear_bab_split", "gear_queue_order", "gear_gather_rows", "gear_scatter_rows",
             "gear_crown_lower_static", "gear_crown_static_scratch_bytes", "gear_constrained_workspace_bytes",
             "gear_constrained_lower", "gear_clip_domains", "gear_bab_child_keys", "gear_bab_compact",
-            "gear_dual_lower_bound")
+            "gear_dual_lower_bound", "gear_crown_lower_ibp")

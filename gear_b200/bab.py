@@ -146,7 +146,7 @@ class BaB:
                  device="cuda", batch: int = 4096, sb_coeff_thresh: float = 1e-3,
                  sb_min_width_ratio: float = 1e-3, model: Optional[torch.nn.Module] = None,
                  constrained: bool = False, max_constraint_rows: int = 16, clip: bool = False,
-                 clip_iterations: int = 1):
+                 clip_iterations: int = 1, ibp_enhancement: bool = True):
         """constrained: the reference's complete clipping mode's constrained concretisation
         (batch_branch_and_bound.py:422-428): every child keeps its parent's planes
         lA_j x + lbias_j <= thr_j as cut rows, and the objective row of its CROWN bound is
@@ -154,7 +154,10 @@ class BaB:
         max_constraint_rows rows per box, the f3 setting's concretize_max_constraint_rows);
         a box that the cuts exclude is pruned.
         clip: domain clipping of the children with their parent's planes (clip.py:237-470,
-        clip_iterations rounds); children that become empty are dropped."""
+        clip_iterations rounds); children that become empty are dropped.
+        ibp_enhancement: every bound is the larger of CROWN's and the plain IBP bound of the
+        output (get_lower_bound_with_ibp_enhancement, bounding.py:789-948, on by default in the
+        reference)."""
         self.device = torch.device(device)
         self.graph = graph
         self.engine = CrownEngine(graph)
@@ -170,6 +173,7 @@ class BaB:
         self.rhs = (torch.zeros(self.S - 1, dtype=torch.float64) if rhs is None else rhs.to(torch.float64)).to(self.device)
         self.incumbent = math.inf
         self.x_best = None
+        self.ibp_enhancement = ibp_enhancement
         self.clip = clip
         self.clip_iterations = clip_iterations
         self.constrained = constrained
@@ -233,7 +237,8 @@ class BaB:
         thr[:, 0] = self.incumbent          # thresholds follow the current incumbent
         self.update_incumbent((lo + hi) / 2)
         thr[:, 0] = self.incumbent
-        lb, lA, lbias = self.engine.lower(lo, hi)
+        lb_ibp = torch.empty(B, self.S, dtype=torch.float64, device=self.device) if self.ibp_enhancement else None
+        lb, lA, lbias = self.engine.lower(lo, hi, lb_ibp=lb_ibp)
         if self.constrained:
             self._constrained_objective(lo, hi, lb, lA, lbias, popped[4], popped[5])
         L = _lib.lib()

@@ -53,6 +53,7 @@ struct Work {
   double* lb;            // (B, S)
   double* lA;            // (B, S, n) or null
   double* lbias;         // (B, S) or null
+  double* lb_ibp;        // (B, S) or null: the rows' IBP bound; lb is then max(CROWN, IBP)
   double* scratch;       // per-slot scratch
   int64_t slot_doubles;
   int64_t B;
@@ -307,6 +308,38 @@ __device__ void relax_mul(double xl, double xu, double yl, double yu, double* p)
   p[3] = (yu - yl) * r_u + yl;
   p[4] = (xl - xu) * r_u + xu;
   p[5] = (yl * xu - yu * xl) * r_u - yl * xu;
+}
+
+// Lower bound of specification row s over the output interval [lo, hi] (width wt), as the
+// reference's IBP pass applies C (BoundLinear._bound_box, operators/linear.py:621-653): center
+// minus deviation (or, with an infinite endpoint, endpoints picked by sign), widened by
+// rounding_error(|C| max(|lo|, |hi|), wt). Cb: this box's rows of C, or null for the identity.
+template <class V>
+__device__ double spec_row_lower(const double* Cb, int wt, V lo, V hi, int off, int s) {
+  bool fin = true;
+  for (int k = 0; k < wt; ++k) fin = fin && isfinite(lo[off + k]) && isfinite(hi[off + k]);
+  double lower, mag;
+  if (!Cb) {
+    const double l = lo[off + s], h = hi[off + s];
+    lower = fin ? (h + l) / 2 - (h - l) / 2 : l;
+    mag = finite_abs(fmax(fabs(l), fabs(h)));
+  } else {
+    const double* c = Cb + (int64_t)s * wt;
+    double center = 0, dev = 0, sl = 0;
+    mag = 0;
+    for (int k = 0; k < wt; ++k) {
+      const double w = c[k], l = lo[off + k], h = hi[off + k];
+      if (fin) {
+        center += ((h + l) / 2) * w;
+        dev += ((h - l) / 2) * fabs(w);
+      } else {
+        sl += (w > 0 ? w * l : 0.0) + (w < 0 ? w * h : 0.0);
+      }
+      mag += finite_abs(fmax(fabs(l), fabs(h))) * finite_abs(w);
+    }
+    lower = fin ? center - dev : sl;
+  }
+  return nan_lo(widen(lower, rounding_error(mag, wt), -1));
 }
 
 // ------------------------------------------------------------------ powers (BoundPow)
@@ -1232,6 +1265,7 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
           }
           lbv = fmax(lbv, fb);
         }
+        if (wk.lb_ibp) lbv = fmax(lbv, wk.lb_ibp[(size_t)bx.b * S + s]);   // IBP pass of the bounding glue
         wk.lb[(size_t)bx.b * S + s] = lbv;
         if (wk.lbias) wk.lbias[(size_t)bx.b * S + s] = bad ? -INFINITY : tot - ctx.row(side, R_ROOT)[s];
         ctx.row(side, R_VAL)[s] = bad ? NAN : tot;    // the lA rows of bad rows are cleared below
@@ -1342,6 +1376,17 @@ __global__ void __launch_bounds__(NT, 768 / NT) crown_megakernel(DevProgram Pg, 
           break;
         }
         case ST_RELAX: relax_node<NT>(bx, a); break;
+        case ST_IBPOUT: {
+          if (wk.lb_ibp) {
+            const int32_t* nd = node_rec(&P, a);
+            const int wt = nd[N_W], S = hdr[H_S];
+            const double* Cb = wk.C ? wk.C + (size_t)b * S * wt : nullptr;
+            for (int s = threadIdx.x; s < S; s += NT)
+              wk.lb_ibp[(size_t)b * S + s] = spec_row_lower(Cb, wt, (const double*)bx.lo, (const double*)bx.hi,
+                                                            nd[N_CUR], s);
+          }
+          break;
+        }
         case ST_PASS: case ST_FINAL: run_pass<NT>(bx, a, sm, sops, wk); break;
         case ST_COMPARE: compare_node<NT>(bx, a, tmp_lo, tmp_hi, st[3] != 0); break;
         default: break;

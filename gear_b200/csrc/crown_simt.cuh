@@ -481,6 +481,7 @@ __device__ void simt_run_pass(const SBox& bx, int pid, const Work& wk, bool live
           }
           lbv = fmax(lbv, fb);
         }
+        if (wk.lb_ibp) lbv = fmax(lbv, wk.lb_ibp[(size_t)bx.b * S + s]);   // IBP pass of the bounding glue
         if (live && side == 0) {
           wk.lb[(size_t)bx.b * S + s] = lbv;
           if (wk.lbias) wk.lbias[(size_t)bx.b * S + s] = bad ? -INFINITY : tot - rroot[s];
@@ -571,6 +572,16 @@ __global__ void __launch_bounds__(SIMT_T, 8) crown_simt_kernel(DevProgram Pg, Wo
           break;
         }
         case ST_RELAX: simt_relax_node(bx, a); break;
+        case ST_IBPOUT: {
+          if (wk.lb_ibp && live) {
+            const int32_t* nd = node_rec(&Pg, a);
+            const int wt = nd[N_W], S = hdr[H_S];
+            const double* Cb = wk.C ? wk.C + (size_t)b * S * wt : nullptr;
+            for (int s = 0; s < S; ++s)
+              wk.lb_ibp[(size_t)b * S + s] = spec_row_lower(Cb, wt, bx.lo, bx.hi, nd[N_CUR], s);
+          }
+          break;
+        }
         case ST_PASS: case ST_FINAL: simt_run_pass(bx, a, wk, live); break;
         case ST_COMPARE: {
           const int32_t* nd = node_rec(&Pg, a);

@@ -204,9 +204,26 @@ extern "C" int64_t gear_crown_workspace_bytes(const gear_dag* dag, int64_t batch
   return slots_for(dag, batch) * dag->slot_doubles * (int64_t)sizeof(double);
 }
 
+static int crown_lower_impl(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
+                            const double* C, double* lb, double* lA, double* lbias, double* lb_ibp, void* workspace,
+                            int64_t workspace_bytes, void* stream);
+
 extern "C" int gear_crown_lower(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
                                 const double* C, double* lb, double* lA, double* lbias, void* workspace,
                                 int64_t workspace_bytes, void* stream) {
+  return crown_lower_impl(dag, x_L, x_U, batch, C, lb, lA, lbias, nullptr, workspace, workspace_bytes, stream);
+}
+
+extern "C" int gear_crown_lower_ibp(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
+                                    const double* C, double* lb, double* lA, double* lbias, double* lb_ibp,
+                                    void* workspace, int64_t workspace_bytes, void* stream) {
+  if (!lb_ibp) return fail(GEAR_E_INVALID, "gear_crown_lower_ibp: %s", "lb_ibp is required");
+  return crown_lower_impl(dag, x_L, x_U, batch, C, lb, lA, lbias, lb_ibp, workspace, workspace_bytes, stream);
+}
+
+static int crown_lower_impl(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
+                            const double* C, double* lb, double* lA, double* lbias, double* lb_ibp, void* workspace,
+                            int64_t workspace_bytes, void* stream) {
   g_launches = 0;
   if (!dag || !x_L || !x_U || !lb || batch < 0) return fail(GEAR_E_INVALID, "gear_crown_lower: %s", "bad arguments");
   if (batch == 0) return GEAR_OK;
@@ -222,6 +239,7 @@ extern "C" int gear_crown_lower(const gear_dag* dag, const double* x_L, const do
   wk.lb = lb;
   wk.lA = lA;
   wk.lbias = lbias;
+  wk.lb_ibp = lb_ibp;
   wk.scratch = (double*)workspace;
   wk.slot_doubles = dag->slot_doubles;
   wk.B = batch;
@@ -291,6 +309,7 @@ extern "C" int gear_crown_lower_static(const gear_dag* dag, const double* x_L, c
   wk.lb = lb;
   wk.lA = lA;
   wk.lbias = lbias;
+  wk.lb_ibp = nullptr;
   wk.scratch = (double*)scratch;   // the kernel writes every scratch word before reading it: no clearing
   wk.slot_doubles = dag->slot_doubles;
   wk.B = batch;

@@ -17,7 +17,9 @@ enum NodeField {
   N_WIN, N_INS, N_FOLD, N_INEXACT, N_WT_OFF, NODE_REC
 };
 
-enum StepType { ST_IBP = 0, ST_MAG = 1, ST_RELAX = 2, ST_PASS = 3, ST_COMPARE = 4, ST_FOLD = 5, ST_FINAL = 6 };
+// ST_IBPOUT: the specification rows over the output's plain IBP interval, into Work.lb_ibp
+enum StepType { ST_IBP = 0, ST_MAG = 1, ST_RELAX = 2, ST_PASS = 3, ST_COMPARE = 4, ST_FOLD = 5, ST_FINAL = 6,
+                ST_IBPOUT = 7 };
 constexpr int STEP_REC = 4;
 
 enum PassField {

@@ -106,8 +106,11 @@ class CrownEngine:
         return self._workspace_bytes(int(_lib.lib().gear_crown_workspace_bytes(self.handle, batch)), device)
 
     def lower(self, x_L: torch.Tensor, x_U: torch.Tensor, C: Optional[torch.Tensor] = None,
-              return_A: bool = True, out=None):
-        """lb (B, S), lA (B, S, n) or None, lbias (B, S) -- all float64 on x_L's device."""
+              return_A: bool = True, out=None, lb_ibp: Optional[torch.Tensor] = None):
+        """lb (B, S), lA (B, S, n) or None, lbias (B, S) -- all float64 on x_L's device.
+
+        lb_ibp (B, S): when given, it receives the rows' bounds over the output's plain IBP
+        interval and lb is the larger of that and CROWN's (the bounding glue's IBP pass)."""
         B = x_L.shape[0]
         dev = x_L.device
         if dev.type != "cuda":
@@ -127,18 +130,23 @@ class CrownEngine:
         else:
             lb, lA, lbias = out
         dag = self._select(x_L, x_U, C, lb, lA, lbias) if self.mode == "auto" else self._dags[next(iter(self._dags))]
-        self._launch(dag, x_L, x_U, C, lb, lA, lbias)
+        self._launch(dag, x_L, x_U, C, lb, lA, lbias, lb_ibp)
         return lb, (lA if return_A else None), lbias
 
-    def _launch(self, dag, x_L, x_U, C, lb, lA, lbias):
+    def _launch(self, dag, x_L, x_U, C, lb, lA, lbias, lb_ibp=None):
         B = x_L.shape[0]
         L = _lib.lib()
         nbytes = int(L.gear_crown_workspace_bytes(dag.handle, B))
         ws = self._workspace_bytes(nbytes, x_L.device)
         stream = torch.cuda.current_stream(x_L.device).cuda_stream
-        st = L.gear_crown_lower(dag.handle, x_L.data_ptr(), x_U.data_ptr(), B,
-                                C.data_ptr() if self.dense_c else None,
-                                lb.data_ptr(), lA.data_ptr(), lbias.data_ptr(), ws.data_ptr(), ws.numel(), stream)
+        cptr = C.data_ptr() if self.dense_c else None
+        if lb_ibp is None:
+            st = L.gear_crown_lower(dag.handle, x_L.data_ptr(), x_U.data_ptr(), B, cptr, lb.data_ptr(), lA.data_ptr(),
+                                    lbias.data_ptr(), ws.data_ptr(), ws.numel(), stream)
+        else:
+            st = L.gear_crown_lower_ibp(dag.handle, x_L.data_ptr(), x_U.data_ptr(), B, cptr, lb.data_ptr(),
+                                        lA.data_ptr(), lbias.data_ptr(), lb_ibp.data_ptr(), ws.data_ptr(), ws.numel(),
+                                        stream)
         _lib.check(st, "gear_crown_lower")
 
     def _select(self, x_L, x_U, C, lb, lA, lbias):

@@ -48,7 +48,7 @@ N_KIND, N_W, N_NIN, N_IN0, N_IN1, N_CUR, N_PLANE, N_CVEC, N_MAP0, N_MAP1, N_W_OF
 
 # ---- steps
 MODES = {"cta": 0, "simt": 1}          # ExecMode in gear_program.h
-ST = {"ibp": 0, "mag": 1, "relax": 2, "pass": 3, "compare": 4, "fold": 5, "final": 6}
+ST = {"ibp": 0, "mag": 1, "relax": 2, "pass": 3, "compare": 4, "fold": 5, "final": 6, "ibpout": 7}
 STEP_REC = 4
 
 PASS_REC = 24
@@ -200,6 +200,9 @@ class Program:
         self.steps.append((ST["mag"], 0, 0, 0))
         for nd in g.nodes[1:]:
             self.steps.append((ST["ibp"], nd.id, 1, 0))      # b = 1: also write the magnitude
+        # the specification rows over the plain IBP interval of the output (the IBP bound of the
+        # bounding glue's IBP pass; written only when the caller asks for it)
+        self.steps.append((ST["ibpout"], self.t, 0, 0))
         self.relaxed = set()
         self._check_prior(self.t, final=True)
         # interval of the final node for the undefined-row fallback

@@ -174,6 +174,14 @@ int gear_constrained_lower(const double* x_L, const double* x_U, int64_t batch, 
                            const double* A, const double* b, int K, int max_rows, double* lb, uint8_t* infeasible,
                            void* workspace, int64_t ws_bytes, void* stream);
 
+/* gear_crown_lower with the IBP pass of the bounding glue (get_lower_bound_with_ibp_enhancement,
+ * complete_verifier/input_split/bounding.py:789-948): lb_ibp (batch, S) receives every row's bound
+ * over the output's plain interval (IBP from the box), and lb the larger of that and the CROWN bound.
+ * lA and lbias are CROWN's. */
+int gear_crown_lower_ibp(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
+                         const double* C, double* lb, double* lA, double* lbias, double* lb_ibp,
+                         void* workspace, int64_t workspace_bytes, void* stream);
+
 /* gear_crown_lower without a workspace argument, for callers that cannot allocate device
  * memory (a solver host that owns a fixed device-memory plan and gives this library no
  * allocator, or a loop that must not pay cudaMalloc's implicit synchronisation). It has no

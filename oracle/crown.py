@@ -991,9 +991,16 @@ def ibp_output(graph, xL, xU, C=None):
     lo, hi = iv[graph.output]
     if C is None:
         return lo, hi
-    mid, rad = (lo + hi) / 2, (hi - lo) / 2
-    center = np.einsum("bsw,bw->bs", C, mid)
-    dev = np.einsum("bsw,bw->bs", np.abs(C), rad)
+    # BoundLinear._bound_box (operators/linear.py:621-653)
+    if np.isfinite(lo).all() and np.isfinite(hi).all():
+        mid, rad = (lo + hi) / 2, (hi - lo) / 2
+        center = np.einsum("bsw,bw->bs", C, mid)
+        dev = np.einsum("bsw,bw->bs", np.abs(C), rad)
+        low, up = center - dev, center + dev
+    else:
+        with np.errstate(invalid="ignore"):
+            low = (np.where(C > 0, C * lo[:, None], 0.0) + np.where(C < 0, C * hi[:, None], 0.0)).sum(-1)
+            up = (np.where(C > 0, C * hi[:, None], 0.0) + np.where(C < 0, C * lo[:, None], 0.0)).sum(-1)
     mag = np.einsum("bsw,bw->bs", finite_abs(C), finite_abs(np.maximum(np.abs(lo), np.abs(hi))))
     err = rounding_error(mag, C.shape[-1])
-    return widen(center - dev, err, -1), widen(center + dev, err, 1)
+    return _nan_to_inf(widen(low, err, -1), widen(up, err, 1))

@@ -114,3 +114,27 @@ def test_gpu_bounds_of_a_lowered_node_program():
     lb, _, Ab = b.compute_bounds(x=(x,), method="CROWN", bound_upper=False, return_A=True)
     assert torch.equal(la, lb)
     assert torch.equal(Aa["/y"]["/x"]["lA"], Ab["/y"]["/x"]["lA"])
+
+
+@pytest.mark.parametrize("key", ["quad_exp_n10_0_eye", "dense_q_n200_0_eye", "quad_exp_n10_1_dense", "pow_ops_0_eye"])
+def test_gpu_ibp_pass_matches_reference(key):
+    """gear_crown_lower_ibp: lb_ibp equals the reference's IBP pass (fixtures, 1e-13) and lb is
+    the larger of it and the CROWN bound."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    from test_ibp_pass import model_graph
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "ibp_out.npz"))
+    _, g = model_graph(key)
+    dense = key.endswith("dense")
+    C = torch.tensor(d[key + "_C"], device="cuda")
+    eng = CrownEngine(g, spec_rows=C.shape[1], dense_c=dense, mode="cta")
+    xL, xU = torch.tensor(d[key + "_xL"], device="cuda"), torch.tensor(d[key + "_xU"], device="cuda")
+    lb_ibp = torch.empty(xL.shape[0], C.shape[1], dtype=torch.float64, device="cuda")
+    lb, _, _ = eng.lower(xL, xU, C if dense else None, lb_ibp=lb_ibp)
+    plain, _, _ = eng.lower(xL, xU, C if dense else None)
+    torch.cuda.synchronize()
+    ref = d[key + "_lb"]
+    got = lb_ibp.cpu().numpy()
+    assert np.max(np.abs(got - ref) / np.maximum(1.0, np.abs(ref))) < 1e-13
+    assert torch.equal(lb, torch.maximum(plain, lb_ibp))
