@@ -151,6 +151,40 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+# ---------------------------------------------------------------- branch and bound to the gap
+def bab_to_gap(instances, dev, rel_gap=1e-4, batch=2048):
+    """Branch and bound (select, CROWN, prune, SB branch, split on the device) to a relative gap
+    on quad_exp_n10 instances 0..instances-1: wall time to the gap per instance (host loop
+    included), p50 / p99, and subdomains bounded per second over all runs."""
+    import torch
+    from gear_b200 import graph, problems
+    from gear_b200.bab import BaB
+    times, bounded, iters, gaps = [], 0, [], []
+    for inst in range(-1, instances):
+        m = problems.make_instance("quad_exp_n10", max(inst, 0))
+        lo, hi = problems.root_box("quad_exp_n10")
+        g = graph.trace(m, lo.repeat(2, 1))
+        m = m.to(dev)
+        torch.cuda.synchronize(dev)
+        t = time.perf_counter()
+        bb = BaB(g, lo, hi, batch=batch, model=m, device=str(dev))
+        P, D, gap = bb.run(rel_gap=rel_gap, max_iterations=5000, time_limit=60)
+        torch.cuda.synchronize(dev)
+        dt = time.perf_counter() - t
+        if inst < 0:
+            continue                                        # warm-up run (module load)
+        times.append(dt)
+        bounded += bb.stats.bounded
+        iters.append(bb.stats.iterations)
+        gaps.append(gap)
+    q = sorted(times)
+    p99 = q[min(len(q) - 1, int(round(0.99 * (len(q) - 1))))]
+    return {"workload": "quad_exp_n10 (config-1 family)", "instances": instances, "rel_gap": rel_gap,
+            "batch": batch, "time_to_gap_s": {"p50": statistics.median(times), "p99": p99, "max": max(times)},
+            "closed": sum(1 for gp in gaps if gp <= rel_gap), "iterations_median": statistics.median(iters),
+            "subdomains_per_s": bounded / sum(times), "timing": "wall clock, host loop included"}
+
+
 # ---------------------------------------------------------------- GPU leg
 def main():
     ap = argparse.ArgumentParser()
@@ -161,6 +195,9 @@ def main():
     ap.add_argument("--impl", default="gear", choices=["gear", "reference"])
     ap.add_argument("--cpu-per-core", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--bab-instances", type=int, default=8,
+                    help="also run branch and bound to relative gap 1e-4 on this many quad_exp_n10 instances "
+                         "(time to gap, p50 / p99); 0 skips it")
     ap.add_argument("--workload", default=WORKLOAD, help="benchmark workload (profiling of other shapes)")
     ap.add_argument("--cta-threads", type=int, default=128, help="threads per CTA of --mode cta")
     ap.add_argument("--mode", default="auto", choices=["auto", "cta", "simt"],
@@ -292,6 +329,8 @@ def main():
                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * B * n * 8,
                        "d2h_bytes_per_step": B * S * 8},
                "clocks": clk.summary()}
+        if args.bab_instances > 0:
+            res["bab"] = bab_to_gap(args.bab_instances, dev)
         if world == 1 and not args.no_cpu_baseline:
             try:
                 res["cpu_baseline"] = cpu_baseline(per_core=args.cpu_per_core, workload=args.workload)

@@ -143,7 +143,8 @@ class BaB:
     g_k(x) <= rhs_k (rhs given already relaxed by the instance's feasibility tolerance)."""
 
     def __init__(self, graph: Graph, lo: torch.Tensor, hi: torch.Tensor, rhs: Optional[torch.Tensor] = None,
-                 device="cuda", batch: int = 4096, sb_coeff_thresh: float = 1e-3,
+                 device="cuda", batch: int = 4096, sb_coeff_thresh: float = 1e-3, engine: Optional[CrownEngine] = None,
+                 engine_mode: str = "auto", cta_threads: int = 128,
                  sb_min_width_ratio: float = 1e-3, model: Optional[torch.nn.Module] = None,
                  constrained: bool = False, max_constraint_rows: int = 16, clip: bool = False,
                  clip_iterations: int = 1, ibp_enhancement: bool = True):
@@ -160,7 +161,16 @@ class BaB:
         reference)."""
         self.device = torch.device(device)
         self.graph = graph
-        self.engine = CrownEngine(graph)
+        # an engine can be shared between runs on the same graph (its kernel choice is kept)
+        self.engine = engine if engine is not None else CrownEngine(graph, mode=engine_mode, cta_threads=cta_threads)
+        if self.engine.mode == "auto":
+            # pick the kernel once, at the full batch, on sub-boxes of the root box
+            gen = torch.Generator(device="cpu").manual_seed(0)
+            r0, r1 = lo.reshape(1, -1).cpu(), hi.reshape(1, -1).cpu()
+            c = r0 + (r1 - r0) * torch.rand(batch, r0.shape[1], generator=gen, dtype=torch.float64)
+            w = (r1 - r0) * torch.rand(batch, r0.shape[1], generator=gen, dtype=torch.float64) * 0.25
+            sl, su = torch.maximum(r0, c - w), torch.minimum(r1, c + w)
+            self.engine.freeze(sl.to(self.device), su.to(self.device))
         self.n = self.engine.n
         self.S = self.engine.S
         self.batch = batch
@@ -206,13 +216,12 @@ class BaB:
             y = self.model(x.to(self.device, torch.float64))
         feas = (y[:, 1:] <= self.rhs).all(1) if y.shape[1] > 1 else torch.ones(y.shape[0], dtype=torch.bool,
                                                                                 device=self.device)
-        if bool(feas.any()):
-            obj = torch.where(feas, y[:, 0], torch.full_like(y[:, 0], math.inf))
-            i = int(torch.argmin(obj))
-            v = float(obj[i])
-            if v < self.incumbent:
-                self.incumbent = v
-                self.x_best = x[i].detach().clone()
+        obj = torch.where(feas, y[:, 0], torch.full_like(y[:, 0], math.inf))
+        best = obj.min(0)
+        v = float(best.values)                # the one host read of the incumbent update
+        if v < self.incumbent:
+            self.incumbent = v
+            self.x_best = x[best.indices].detach().clone()
 
     def dual_bound(self) -> float:
         d = self.queue.min_key()

@@ -204,6 +204,43 @@ __device__ __forceinline__ bool before(double ka, int64_t ia, double kb, int64_t
   return ka > kb || (ka == kb && ia < ib);
 }
 
+// The whole bitonic network in one CTA for N2 <= SORT_SMEM_MAX: slots and their keys staged in
+// shared memory, every (k, j) stage separated by a barrier; same comparator as bitonic_step.
+constexpr int SORT_SMEM_MAX = 8192;
+constexpr int SORT_THREADS = 1024;
+__global__ void __launch_bounds__(SORT_THREADS) bitonic_smem(int32_t* idx, const double* key, const int64_t* id,
+                                                            int N2) {
+  extern __shared__ unsigned char sort_sm[];
+  double* k_s = reinterpret_cast<double*>(sort_sm);
+  int64_t* id_s = reinterpret_cast<int64_t*>(k_s + N2);
+  int32_t* ix_s = reinterpret_cast<int32_t*>(id_s + N2);
+  for (int i = threadIdx.x; i < N2; i += SORT_THREADS) {
+    const int32_t a = idx[i];
+    ix_s[i] = a;
+    k_s[i] = a >= 0 ? key[a] : 0.0;
+    id_s[i] = a >= 0 ? id[a] : 0;
+  }
+  __syncthreads();
+  for (int k = 2; k <= N2; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int t = threadIdx.x; t < (N2 >> 1); t += SORT_THREADS) {
+        const int i = (t / j) * 2 * j + (t % j), l = i + j;
+        const int32_t a = ix_s[i], b = ix_s[l];
+        const bool a_pad = a < 0, b_pad = b < 0;
+        const bool a_first = (a_pad || b_pad) ? !a_pad : before(k_s[i], id_s[i], k_s[l], id_s[l]);
+        const bool up = (i & k) == 0;
+        if (up ? !a_first : a_first) {
+          ix_s[i] = b; ix_s[l] = a;
+          const double tk = k_s[i]; k_s[i] = k_s[l]; k_s[l] = tk;
+          const int64_t ti = id_s[i]; id_s[i] = id_s[l]; id_s[l] = ti;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int i = threadIdx.x; i < N2; i += SORT_THREADS) idx[i] = ix_s[i];
+}
+
 __global__ void bitonic_step(int32_t* idx, const double* key, const int64_t* id, int64_t N2, int64_t N, int j,
                              int k) {
   int64_t i = (int64_t)blockIdx.x * BT + threadIdx.x;

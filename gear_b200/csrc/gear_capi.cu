@@ -407,11 +407,20 @@ extern "C" int gear_queue_order(const double* key, const int64_t* id, const int3
   cudaMemsetAsync(order, 0xff, n2 * sizeof(int32_t), st);             // padding = -1
   cudaMemcpyAsync(order, slots, count * sizeof(int32_t), cudaMemcpyDeviceToDevice, st);
   int launches = 0;
-  for (int64_t k = 2; k <= n2; k <<= 1)
-    for (int64_t j = k >> 1; j > 0; j >>= 1) {
-      bitonic_step<<<grid_for(n2), BT, 0, st>>>(order, key, id, n2, count, (int)j, (int)k);
-      ++launches;
-    }
+  if (n2 <= SORT_SMEM_MAX) {
+    // the whole network in one CTA (one launch instead of log2(n2)(log2(n2)+1)/2)
+    const size_t smem = (size_t)n2 * (sizeof(double) + sizeof(int64_t) + sizeof(int32_t));
+    cudaError_t ea = cudaFuncSetAttribute(bitonic_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (ea != cudaSuccess) return cuda_fail(ea, "cudaFuncSetAttribute");
+    bitonic_smem<<<1, SORT_THREADS, smem, st>>>(order, key, id, (int)n2);
+    launches = 1;
+  } else {
+    for (int64_t k = 2; k <= n2; k <<= 1)
+      for (int64_t j = k >> 1; j > 0; j >>= 1) {
+        bitonic_step<<<grid_for(n2), BT, 0, st>>>(order, key, id, n2, count, (int)j, (int)k);
+        ++launches;
+      }
+  }
   g_launches = launches;
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_queue_order");

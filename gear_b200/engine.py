@@ -93,9 +93,23 @@ class CrownEngine:
     def variant(self, batch: int) -> str:
         """Name of the kernel variant used for this batch size ("simt", "cta64", ...)."""
         v = self._choice.get(self._bucket(batch))
+        if self.mode == "fixed":
+            return self._fixed.name
         if self.mode != "auto":
             return self._dags[next(iter(self._dags))].name
         return None if v is None else self._dag(*v).name
+
+    def freeze(self, x_L: torch.Tensor, x_U: torch.Tensor, C: Optional[torch.Tensor] = None):
+        """Time the variants once on these boxes and use the fastest for every later batch size
+        (a caller whose batches vary, like a branch-and-bound loop, pays the timing once)."""
+        if self.mode != "auto":
+            return self.variant(x_L.shape[0])
+        self.lower(x_L, x_U, C)
+        choice = self._choice[self._bucket(x_L.shape[0])]
+        self._fixed = self._dag(*choice)
+        self.handle, self.prog = self._fixed.handle, self._fixed.prog
+        self.mode = "fixed"
+        return self._fixed.name
 
     @staticmethod
     def _bucket(batch):
@@ -129,7 +143,12 @@ class CrownEngine:
             lbias = torch.empty(B, self.S, dtype=torch.float64, device=dev)
         else:
             lb, lA, lbias = out
-        dag = self._select(x_L, x_U, C, lb, lA, lbias) if self.mode == "auto" else self._dags[next(iter(self._dags))]
+        if self.mode == "auto":
+            dag = self._select(x_L, x_U, C, lb, lA, lbias)
+        elif self.mode == "fixed":
+            dag = self._fixed
+        else:
+            dag = self._dags[next(iter(self._dags))]
         self._launch(dag, x_L, x_U, C, lb, lA, lbias, lb_ibp)
         return lb, (lA if return_A else None), lbias
 

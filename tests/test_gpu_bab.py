@@ -105,3 +105,27 @@ def test_constrained_concretisation_bab_is_sound_and_not_slower():
     y = m(x.cuda()).cpu()
     feas = (y[:, 1:] <= 0).all(1)
     assert Dd <= float(y[feas, 0].min()) + 1e-9
+
+
+@pytest.mark.parametrize("N", [3000, 8192, 10000])
+def test_queue_order_single_and_multi_launch(N):
+    """gear_queue_order: one shared-memory CTA up to 8192 slots, the multi-launch network
+    beyond; both give (key desc, insertion id asc), ties included."""
+    from gear_b200 import _lib
+    g = np.random.default_rng(N)
+    key = np.round(g.normal(size=N), 1)                 # many ties
+    key[::97] = -np.inf
+    ids = g.permutation(N).astype(np.int64)
+    slots = g.permutation(N).astype(np.int32)[: N - 5]   # a subset of the slots is active
+    n = slots.size
+    n2 = 1 << (n - 1).bit_length()
+    k_t = torch.tensor(key, device="cuda")
+    i_t = torch.tensor(ids, device="cuda")
+    s_t = torch.tensor(slots, device="cuda")
+    order = torch.empty(n2, dtype=torch.int32, device="cuda")
+    st = torch.cuda.current_stream().cuda_stream
+    _lib.check(_lib.lib().gear_queue_order(k_t.data_ptr(), i_t.data_ptr(), s_t.data_ptr(), n, order.data_ptr(), n2, st),
+               "gear_queue_order")
+    torch.cuda.synchronize()
+    ref = slots[np.lexsort((ids[slots], -key[slots]))]
+    assert np.array_equal(order[:n].cpu().numpy(), ref)
