@@ -40,6 +40,9 @@ constexpr double TIE_TOL = 1e-12;               // McCormick tie tolerance (see 
 constexpr double STEP_PRE = 0.01;
 // The box-per-CTA kernel is instantiated for 64, 128 and 256 threads per CTA (template
 // parameter NT of every function below that splits work over the CTA); the program picks one.
+#ifndef GEAR_CTA_MINB
+#define GEAR_CTA_MINB 768      // resident threads per SM the register budget is sized for
+#endif
 
 // sin/cos table offsets (gear_b200/tables.py SIN_TABLE_ORDER)
 constexpr int T_DL = 0, T_DU = SIN_N_PRE, T_XLLD = 2 * SIN_N_PRE, T_XLLC = T_XLLD + SIN_N_TB,
@@ -1316,7 +1319,7 @@ __device__ void compare_node(const Box& bx, int v, double* tmp_lo, double* tmp_h
 
 
 template <int NT>
-__global__ void __launch_bounds__(NT, 768 / NT) crown_megakernel(DevProgram Pg, Work wk) {
+__global__ void __launch_bounds__(NT, GEAR_CTA_MINB / NT) crown_megakernel(DevProgram Pg, Work wk) {
   extern __shared__ double sm[];
   const int32_t* hdr = Pg.hdr;
   // shared memory: [pass working set | node table | op records of the running pass]

@@ -53,6 +53,7 @@ template <int NT>
 cudaError_t cta_occupancy_t(int smem_bytes, int* bps) {
   cudaError_t e = cudaFuncSetAttribute(gear::crown_megakernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
   if (e != cudaSuccess) return e;
+
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, gear::crown_megakernel<NT>, NT, smem_bytes);
 }
 static cudaError_t cta_occupancy(int threads, int smem_bytes, int* bps) {
