@@ -53,6 +53,11 @@ template <int NT>
 cudaError_t cta_occupancy_t(int smem_bytes, int* bps) {
   cudaError_t e = cudaFuncSetAttribute(gear::crown_megakernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
   if (e != cudaSuccess) return e;
+#ifdef GEAR_CTA_CARVEOUT
+  // shared-memory share of the unified L1 (percent) for builds that fix it
+  e = cudaFuncSetAttribute(gear::crown_megakernel<NT>, cudaFuncAttributePreferredSharedMemoryCarveout, GEAR_CTA_CARVEOUT);
+  if (e != cudaSuccess) return e;
+#endif
 
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, gear::crown_megakernel<NT>, NT, smem_bytes);
 }
