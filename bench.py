@@ -151,6 +151,24 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+# ---------------------------------------------------------------- replicas (N > 1)
+def rank_boxes(workload, batch, rank):
+    """This rank's boxes: every rank bounds its own seeded sub-boxes of instance 0 (replicas,
+    no exchange of boxes between ranks)."""
+    from gear_b200 import problems
+    return problems.make_boxes(workload, batch, 0, seed_offset=500 + 7919 * rank)
+
+
+def max_over_ranks(value, world, device):
+    """The slowest rank's value (timing is the max over ranks); identity for one rank."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ---------------------------------------------------------------- branch and bound to the gap
 def bab_to_gap(instances, dev, rel_gap=1e-4, batch=2048):
     """Branch and bound (select, CROWN, prune, SB branch, split on the device) to a relative gap
@@ -222,7 +240,7 @@ def main():
     from gear_b200 import _lib
     B = args.batch
     model = problems.make_instance(args.workload, 0)
-    lo, hi = problems.make_boxes(args.workload, B, 0, seed_offset=500 + 7919 * rank)
+    lo, hi = rank_boxes(args.workload, B, rank)
     bm = BoundedModule(model, lo[:2], device=str(dev), bound_opts={"gear_mode": args.mode,
                                                                   "gear_cta_threads": args.cta_threads})
     S = bm.final_node_width()
@@ -260,10 +278,7 @@ def main():
         torch.cuda.synchronize()
         barrier()
     ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms, world, dev)
     value = B * args.steps * world / (ms_max / 1000.0)
 
     # end to end through the public API: pinned host boxes in, lb back to the host
@@ -288,10 +303,7 @@ def main():
         e2e_step()
     f1.record()
     torch.cuda.synchronize()
-    te = torch.tensor([f0.elapsed_time(f1)], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = B * e_steps * world / (float(te.item()) / 1000.0)
+    e2e_value = B * e_steps * world / (max_over_ranks(f0.elapsed_time(f1), world, dev) / 1000.0)
 
     if rank == 0:
         peak, peak_kind = _peaks()
