@@ -435,7 +435,15 @@ struct Box {
   const double* xL;  // this box's input box (n)
   const double* xU;
   int64_t b;
+  int open;        // some coordinate has a non-finite centre or radius (box_open)
 };
+
+// The concretisation A x0 + |A| eps is a dense product over every input coordinate
+// (concretize_bounds.py), so one coordinate with a non-finite centre or radius makes every
+// row NaN or infinite (0 * inf included): all rows of the box are discarded.
+__device__ __forceinline__ int box_open(double l, double h) {
+  return !(isfinite((h + l) / 2.0) && isfinite((h - l) / 2.0));
+}
 
 __device__ __forceinline__ const int32_t* node_rec(const DevProgram* P, int v) { return P->nodes + v * NODE_REC; }
 
@@ -1250,7 +1258,7 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
     for (int s = tid; s < S; s += NT) {
       double val = ctx.row(side, R_VAL)[s], er = ctx.row(side, R_ERR)[s];
       double tot = val + sign * (er + (fabs(val) + er) * RE1);
-      const bool bad = isnan(tot) || tot == -sign * INFINITY;
+      const bool bad = bx.open || isnan(tot) || tot == -sign * INFINITY;
       if (bad) tot = sign * INFINITY;
       if (final) {
         double lbv = tot;
@@ -1349,8 +1357,14 @@ __global__ void __launch_bounds__(NT, GEAR_CTA_MINB / NT) crown_megakernel(DevPr
     bx.b = b;
     bx.xL = wk.xL + (size_t)b * n;
     bx.xU = wk.xU + (size_t)b * n;
-    for (int j = threadIdx.x; j < n; j += NT) { bx.lo[j] = bx.xL[j]; bx.hi[j] = bx.xU[j]; }
-    __syncthreads();
+    int open = 0;
+    for (int j = threadIdx.x; j < n; j += NT) {
+      const double l = bx.xL[j], h = bx.xU[j];
+      bx.lo[j] = l;
+      bx.hi[j] = h;
+      open |= box_open(l, h);
+    }
+    bx.open = __syncthreads_or(open);
     for (int si = 0; si < nsteps; ++si) {
 #ifdef GEAR_STEP_PROFILE
       long long t_step = clock64();

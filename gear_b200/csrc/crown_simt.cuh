@@ -34,6 +34,7 @@ struct SBox {
   const DevProgram* P;
   SView lo, hi, mag, planes, fold, pres_lo, pres_hi, tmp_lo, tmp_hi, buf, rows;
   int64_t b;
+  int open;        // some input coordinate has a non-finite centre or radius (box_open)
 };
 
 __device__ __forceinline__ int64_t simt_items(const int32_t* hdr) {
@@ -464,7 +465,7 @@ __device__ void simt_run_pass(const SBox& bx, int pid, const Work& wk, bool live
     for (int s = 0; s < S; ++s) {
       double val = rval[s], er = rerr[s];
       double tot = val + sign * (er + (fabs(val) + er) * RE1);
-      const bool bad = isnan(tot) || tot == -sign * INFINITY;
+      const bool bad = bx.open || isnan(tot) || tot == -sign * INFINITY;
       if (bad) tot = sign * INFINITY;
       if (final) {
         double lbv = tot;
@@ -546,6 +547,8 @@ __global__ void __launch_bounds__(SIMT_T, 8) crown_simt_kernel(DevProgram Pg, Wo
       }
     }
     __syncthreads();
+    bx.open = 0;
+    for (int j = 0; j < n; ++j) bx.open |= box_open(bx.lo[j], bx.hi[j]);
     for (int si = 0; si < nsteps; ++si) {
 #ifdef GEAR_STEP_PROFILE
       long long t_step = clock64();

@@ -231,8 +231,9 @@ static int crown_lower_impl(const gear_dag* dag, const double* x_L, const double
                             const double* C, double* lb, double* lA, double* lbias, double* lb_ibp, void* workspace,
                             int64_t workspace_bytes, void* stream) {
   g_launches = 0;
-  if (!dag || !x_L || !x_U || !lb || batch < 0) return fail(GEAR_E_INVALID, "gear_crown_lower: %s", "bad arguments");
-  if (batch == 0) return GEAR_OK;
+  if (!dag || batch < 0) return fail(GEAR_E_INVALID, "gear_crown_lower: %s", "bad arguments");
+  if (batch == 0) return GEAR_OK;             // empty arrays may come with null pointers
+  if (!x_L || !x_U || !lb) return fail(GEAR_E_INVALID, "gear_crown_lower: %s", "bad arguments");
   if (!workspace || workspace_bytes < gear_crown_workspace_bytes(dag, batch))
     return fail(GEAR_E_WORKSPACE, "gear_crown_lower: %s", "workspace too small");
   if (dag->hdr[gear::H_RETA] == 0 && lA) return fail(GEAR_E_INVALID, "gear_crown_lower: %s", "program built without A");
@@ -338,7 +339,7 @@ extern "C" int64_t gear_bab_workspace_bytes(int64_t batch) {
 extern "C" int gear_bab_prune(const double* lb, const double* thr, int64_t batch, int S, uint8_t* keep, int32_t* kept,
                               int32_t* n_kept, double* disc_min, void* workspace, int64_t ws_bytes, void* stream) {
   using namespace gear::bab;
-  if (!lb || !thr || !keep || !kept || !n_kept || !disc_min || batch < 0 || S < 1)
+  if (!n_kept || !disc_min || batch < 0 || S < 1 || (batch > 0 && (!lb || !thr || !keep || !kept)))
     return fail(GEAR_E_INVALID, "gear_bab_prune: %s", "bad arguments");
   if (!workspace || ws_bytes < gear_bab_workspace_bytes(batch))
     return fail(GEAR_E_WORKSPACE, "gear_bab_prune: %s", "workspace too small");
@@ -491,7 +492,8 @@ extern "C" int gear_bab_child_keys(const double* lb, const double* lA, const dou
 extern "C" int gear_bab_compact(const uint8_t* keep, int64_t batch, int32_t* kept, int32_t* n_kept, void* workspace,
                                 int64_t ws_bytes, void* stream) {
   using namespace gear::bab;
-  if (!keep || !kept || !n_kept || batch < 0) return fail(GEAR_E_INVALID, "gear_bab_compact: %s", "bad arguments");
+  if (!n_kept || batch < 0 || (batch > 0 && (!keep || !kept)))
+    return fail(GEAR_E_INVALID, "gear_bab_compact: %s", "bad arguments");
   if (!workspace || ws_bytes < gear_bab_workspace_bytes(batch))
     return fail(GEAR_E_WORKSPACE, "gear_bab_compact: %s", "workspace too small");
   cudaStream_t st = (cudaStream_t)stream;

@@ -129,8 +129,9 @@ class CrownEngine:
         dev = x_L.device
         if dev.type != "cuda":
             raise _lib.GearError("inputs must be CUDA tensors")
-        x_L = x_L.reshape(B, -1).to(torch.float64).contiguous()
-        x_U = x_U.reshape(B, -1).to(torch.float64).contiguous()
+        w = -1 if B else self.n                     # an empty batch has no width to infer
+        x_L = x_L.reshape(B, w).to(torch.float64).contiguous()
+        x_U = x_U.reshape(B, w).to(torch.float64).contiguous()
         if x_L.shape[1] != self.n:
             raise ValueError(f"input width {x_L.shape[1]} != {self.n}")
         if self.dense_c:
@@ -143,6 +144,8 @@ class CrownEngine:
             lbias = torch.empty(B, self.S, dtype=torch.float64, device=dev)
         else:
             lb, lA, lbias = out
+        if B == 0:
+            return lb, (lA if return_A else None), lbias
         if self.mode == "auto":
             dag = self._select(x_L, x_U, C, lb, lA, lbias)
         elif self.mode == "fixed":

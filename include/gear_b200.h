@@ -76,7 +76,8 @@ int64_t gear_crown_workspace_bytes(const gear_dag* dag, int64_t batch);
  *                                     in this buffer; optional for a box-per-thread one)
  *   lbias     (batch, S) float64 or NULL      bias of that plane (lb minus the
  *                                            concretised A term)
- * `stream` is a cudaStream_t (NULL: the legacy default stream). Asynchronous. */
+ * `stream` is a cudaStream_t (NULL: the legacy default stream). Asynchronous. With batch 0
+ * nothing is launched and the array pointers may be NULL. */
 int gear_crown_lower(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
                      const double* C, double* lb, double* lA, double* lbias,
                      void* workspace, int64_t workspace_bytes, void* stream);
@@ -90,7 +91,8 @@ int64_t gear_bab_workspace_bytes(int64_t batch);
 /* Prune (solving mode): keep[b] = 0 when some row proves box b done (lb_j > thr_j on a finite
  * row, lb_0 >= thr_0, or lb_0 = +inf with a finite thr_0). kept[0..n_kept) lists the kept boxes
  * in order; disc_min (one double, in/out) is lowered to the smallest finite thr_0 of the
- * discarded boxes. lb, thr (batch, S). */
+ * discarded boxes. lb, thr (batch, S). With batch 0 only n_kept is written (0) and the
+ * array pointers may be NULL. */
 int gear_bab_prune(const double* lb, const double* thr, int64_t batch, int S, uint8_t* keep, int32_t* kept,
                    int32_t* n_kept, double* disc_min, void* workspace, int64_t ws_bytes, void* stream);
 
@@ -138,7 +140,8 @@ int gear_bab_child_keys(const double* lb, const double* lA, const double* lbias,
                         const double* child_hi, const int32_t* kept, int64_t n_kept, int S, int n,
                         double* child_key, void* stream);
 
-/* kept[0..n_kept) = the indices b with keep[b] != 0, in order. Workspace: gear_bab_workspace_bytes. */
+/* kept[0..n_kept) = the indices b with keep[b] != 0, in order. Workspace: gear_bab_workspace_bytes.
+ * With batch 0 only n_kept is written (0) and keep / kept may be NULL. */
 int gear_bab_compact(const uint8_t* keep, int64_t batch, int32_t* kept, int32_t* n_kept, void* workspace,
                      int64_t ws_bytes, void* stream);
 
