@@ -203,6 +203,165 @@ def bab_to_gap(instances, dev, rel_gap=1e-4, batch=2048):
             "subdomains_per_s": bounded / sum(times), "timing": "wall clock, host loop included"}
 
 
+def mixed_setup(instances=512, workers=None):
+    """Instances 0..instances-1 of the mixed family, traced, compiled in a process pool and
+    uploaded into one MultiEngine: (instances, graphs, engine, compile seconds)."""
+    import torch
+    from gear_b200 import graph, problems
+    from gear_b200.engine import MultiEngine
+    from gear_b200.program import compile_many
+    t0 = time.perf_counter()
+    insts = [problems.mixed_instance(k) for k in range(instances)]
+    graphs = [graph.trace(m, torch.zeros(2, m.n, dtype=torch.float64)) for m in insts]
+    me = MultiEngine(graphs, programs=compile_many(graphs, kw=dict(mode="cta", cta_threads=256),
+                                                   simt_items_max=8192, workers=workers))
+    return insts, graphs, me, time.perf_counter() - t0
+
+
+def mixed_batch(dev, setup, boxes=256, steps=2, warmup=1, plain=True):
+    """The uneven batch: instances 0..instances-1 of the mixed family (n log-uniform in [5, 500],
+    depth 3-12, m = n // 4), `boxes` sub-boxes each. Certified subdomain bounds per second
+    (device time, CUDA events) of (a) every instance in one persistent launch per kernel variant
+    (MultiEngine), (b) the same programs launched alone, one launch per instance back to back on
+    one stream, and (c) the plain form, one instance at a time with one launch per schedule step
+    and per op. Results of (a) are compared bit for bit with (b) and (c)."""
+    import torch
+    from gear_b200 import _lib, problems
+    from gear_b200.engine import _Dag
+    from gear_b200.program import compile_many
+    insts, graphs, me, compile_s = setup
+    instances = len(insts)
+    bx = [tuple(t.to(dev) for t in problems.mixed_boxes(m, boxes, k)) for k, m in enumerate(insts)]
+    total = instances * boxes
+    outs = me.outputs([boxes] * instances, dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps, warm):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / reps
+
+    packed_ms = timed(lambda: me.lower(bx, out=outs), steps, warmup)
+    me.record_groups(True)
+    me.lower(bx, out=outs)
+    group_ms = me.group_ms()
+    me.record_groups(False)
+    # one launch per instance through gear_crown_lower, same programs
+    L = _lib.lib()
+    ws_bytes = max(int(L.gear_crown_workspace_bytes(d.handle, boxes)) for d in me.dags)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    alone = me.outputs([boxes] * instances, dev)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+
+    def alone_step():
+        for i, d in enumerate(me.dags):
+            lb, lA, lbias = alone[i]
+            _lib.check(L.gear_crown_lower(d.handle, bx[i][0].data_ptr(), bx[i][1].data_ptr(), boxes, None,
+                                          lb.data_ptr(), lA.data_ptr(), lbias.data_ptr(), ws.data_ptr(), ws_bytes,
+                                          stream), "gear_crown_lower")
+    alone_ms = timed(alone_step, steps, warmup)
+    same = all(torch.equal(a[0], b[0]) and torch.equal(a[1], b[1]) for a, b in zip(outs, alone))
+    del ws
+    res = {"workload": "mixed family (n log-uniform [5, 500], depth 3-12, m = n // 4)", "instances": instances,
+           "boxes_per_instance": boxes, "groups": me.group_names(), "group_ms": group_ms,
+           "launches_per_call": me.launches(),
+           "packed_ms": packed_ms, "packed_subdomains_per_s": total / (packed_ms / 1000.0),
+           "alone_ms": alone_ms, "alone_subdomains_per_s": total / (alone_ms / 1000.0),
+           "packed_vs_alone": alone_ms / packed_ms, "bitwise_equal_alone": same}
+    if plain:
+        t1 = time.perf_counter()
+        pprogs = compile_many(graphs, kw=dict(mode="cta", cta_threads=128, smem_limit=0))
+        pdags = [_Dag.from_program(p) for p in pprogs]
+        compile_s += time.perf_counter() - t1
+        pws_bytes = max(int(L.gear_crown_plain_workspace_bytes(d.handle, boxes)) for d in pdags)
+        pws = torch.empty(pws_bytes, dtype=torch.uint8, device=dev)
+        pl = me.outputs([boxes] * instances, dev)
+        launches = [0]
+
+        def plain_step():
+            launches[0] = 0
+            for i, d in enumerate(pdags):
+                lb, lA, lbias = pl[i]
+                _lib.check(L.gear_crown_lower_plain(d.handle, bx[i][0].data_ptr(), bx[i][1].data_ptr(), boxes, None,
+                                                    lb.data_ptr(), lA.data_ptr(), lbias.data_ptr(), pws.data_ptr(),
+                                                    pws_bytes, stream), "gear_crown_lower_plain")
+                launches[0] += int(L.gear_last_launch_count())
+        plain_ms = timed(plain_step, 1, 0)
+        res.update({"plain_ms": plain_ms, "plain_subdomains_per_s": total / (plain_ms / 1000.0),
+                    "plain_launches_per_call": launches[0], "packed_vs_plain": plain_ms / packed_ms,
+                    "bitwise_equal_plain": all(torch.equal(a[0], b[0]) for a, b in zip(outs, pl))})
+        del pws
+    res.update({"compile_s": compile_s, "timing": f"CUDA events; packed and alone {steps} calls after {warmup} "
+                "warm-up, plain 1 call (its kernels already loaded)"})
+    return res
+
+
+def mixed_bab(dev, setup, batch=256, rel_gap=1e-4, time_limit=60.0):
+    """Branch and bound on the uneven batch, every instance at once (MultiBaB: one packed CROWN
+    launch per kernel variant per iteration): wall time to the relative gap per instance (host
+    loop included) over the instances that reach it within the time limit, and subdomains
+    bounded per second over the run."""
+    import torch
+    from gear_b200.bab import MultiBaB
+    insts, graphs, me, _ = setup
+    instances = len(insts)
+    roots = [(torch.full((1, m.n), -2.0, dtype=torch.float64), torch.full((1, m.n), 2.0, dtype=torch.float64))
+             for m in insts]
+    models = [m.to(dev) for m in insts]
+    mb = MultiBaB(graphs, roots, models, batch=batch, engine=me, device=str(dev))
+    torch.cuda.synchronize(dev)
+    t = time.perf_counter()
+    res = mb.run(rel_gap=rel_gap, time_limit=time_limit)
+    torch.cuda.synchronize(dev)
+    wall = time.perf_counter() - t
+    ttg = sorted(r["time_to_gap"] for r in res if r["time_to_gap"] is not None)
+    q = (lambda p: ttg[min(len(ttg) - 1, int(round(p * (len(ttg) - 1))))]) if ttg else (lambda p: None)
+    closed_n = [insts[i].n for i, r in enumerate(res) if r["time_to_gap"] is not None]
+    return {"workload": "mixed family (n log-uniform [5, 500], depth 3-12, m = n // 4)", "instances": instances,
+            "batch_per_instance": batch, "rel_gap": rel_gap, "time_limit_s": time_limit, "wall_s": wall,
+            "iterations": mb.iterations, "closed": len(ttg), "closed_max_n": max(closed_n) if closed_n else None,
+            "time_to_gap_s": {"p50": q(0.5), "p99": q(0.99), "max": ttg[-1] if ttg else None},
+            "subdomains_per_s": mb.bounded / wall, "bounded": mb.bounded,
+            "timing": "wall clock from the first iteration, host loop included"}
+
+
+def plain_gpu(dev, workload, lo, hi, fused_value, steps=3, warmup=1):
+    """The plain GPU form on the headline workload (PlainEngine: one launch per schedule step
+    and per op, box state through global memory), the same boxes: subdomains/s and the fused
+    path's multiple of it."""
+    import torch
+    from gear_b200 import graph, problems
+    from gear_b200.engine import PlainEngine
+    m = problems.make_instance(workload, 0)
+    pe = PlainEngine(graph.trace(m, lo[:2]))
+    xl, xu = lo.to(dev), hi.to(dev)
+    B = lo.shape[0]
+    out = (torch.empty(B, pe.S, dtype=torch.float64, device=dev),
+           torch.empty(B, pe.S, pe.n, dtype=torch.float64, device=dev),
+           torch.empty(B, pe.S, dtype=torch.float64, device=dev))
+    for _ in range(warmup):
+        pe.lower(xl, xu, out=out)
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        pe.lower(xl, xu, out=out)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / steps
+    value = B / (ms / 1000.0)
+    return {"value": value, "unit": UNIT, "ms_per_step": ms, "launches_per_step": pe.launches,
+            "fused_vs_plain": fused_value / value,
+            "form": "same device code, one launch per schedule step and per op of each CROWN pass, "
+                    "box state in global memory between launches"}, out
+
+
 # ---------------------------------------------------------------- GPU leg
 def main():
     ap = argparse.ArgumentParser()
@@ -216,6 +375,14 @@ def main():
     ap.add_argument("--bab-instances", type=int, default=8,
                     help="also run branch and bound to relative gap 1e-4 on this many quad_exp_n10 instances "
                          "(time to gap, p50 / p99); 0 skips it")
+    ap.add_argument("--mixed-instances", type=int, default=512,
+                    help="also bound the uneven batch of this many mixed-family instances in one launch per "
+                         "kernel variant against one launch per instance; 0 skips it")
+    ap.add_argument("--mixed-boxes", type=int, default=256, help="sub-boxes per mixed-family instance")
+    ap.add_argument("--mixed-bab-seconds", type=float, default=60.0,
+                    help="time limit of branch and bound on the uneven batch (all instances at once); 0 skips it")
+    ap.add_argument("--no-plain", dest="plain", action="store_false",
+                    help="skip the plain GPU form (one launch per step and per op) on the workload")
     ap.add_argument("--workload", default=WORKLOAD, help="benchmark workload (profiling of other shapes)")
     ap.add_argument("--cta-threads", type=int, default=128, help="threads per CTA of --mode cta")
     ap.add_argument("--mode", default="auto", choices=["auto", "cta", "simt"],
@@ -341,8 +508,18 @@ def main():
                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * B * n * 8,
                        "d2h_bytes_per_step": B * S * 8},
                "clocks": clk.summary()}
+        if args.plain:
+            pg, pout = plain_gpu(dev, args.workload, lo, hi, value)
+            pg["bitwise_equal"] = bool(torch.equal(pout[0], lb) and torch.equal(pout[1], lA))
+            res["plain_gpu"] = pg
+            del pout
         if args.bab_instances > 0:
             res["bab"] = bab_to_gap(args.bab_instances, dev)
+        if args.mixed_instances > 0:
+            setup = mixed_setup(args.mixed_instances)
+            res["mixed"] = mixed_batch(dev, setup, args.mixed_boxes)
+            if args.mixed_bab_seconds > 0:
+                res["mixed_bab"] = mixed_bab(dev, setup, time_limit=args.mixed_bab_seconds)
         if world == 1 and not args.no_cpu_baseline:
             try:
                 res["cpu_baseline"] = cpu_baseline(per_core=args.cpu_per_core, workload=args.workload)

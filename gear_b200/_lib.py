@@ -13,6 +13,13 @@ class GearError(RuntimeError):
     pass
 
 
+class LowerArgs(ctypes.Structure):
+    """gear_lower_args: one instance of a gear_crown_lower_multi call."""
+    _fields_ = [("dag", ctypes.c_void_p), ("x_L", ctypes.c_void_p), ("x_U", ctypes.c_void_p),
+                ("batch", ctypes.c_int64), ("C", ctypes.c_void_p), ("lb", ctypes.c_void_p),
+                ("lA", ctypes.c_void_p), ("lbias", ctypes.c_void_p), ("lb_ibp", ctypes.c_void_p)]
+
+
 def lib():
     """Load the in-tree extension; raise if it is missing (there is no CPU fallback)."""
     global _LIB
@@ -73,6 +80,14 @@ def lib():
         L.gear_dual_lower_bound.argtypes = [vp, vp, vp, vp, i32, i64, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp,
                                             i32, vp, vp, vp, vp]
         L.gear_dual_lower_bound.restype = i32
+        L.gear_crown_plain_workspace_bytes.argtypes = [vp, i64]
+        L.gear_crown_plain_workspace_bytes.restype = i64
+        L.gear_crown_lower_plain.argtypes = [vp, vp, vp, i64, vp, vp, vp, vp, vp, i64, vp]
+        L.gear_crown_lower_plain.restype = i32
+        L.gear_crown_multi_workspace_bytes.argtypes = [ctypes.POINTER(LowerArgs), i32]
+        L.gear_crown_multi_workspace_bytes.restype = i64
+        L.gear_crown_lower_multi.argtypes = [ctypes.POINTER(LowerArgs), i32, vp, i64, vp]
+        L.gear_crown_lower_multi.restype = i32
         _LIB = L
     return _LIB
 
@@ -99,4 +114,5 @@ EXPORTED = ("gear_dag_create", "gear_dag_destroy", "gear_crown_workspace_bytes",
             "gear_bab_branch", "gear_bab_split", "gear_queue_order", "gear_gather_rows", "gear_scatter_rows",
             "gear_crown_lower_static", "gear_crown_static_scratch_bytes", "gear_constrained_workspace_bytes",
             "gear_constrained_lower", "gear_clip_domains", "gear_bab_child_keys", "gear_bab_compact",
-            "gear_dual_lower_bound", "gear_crown_lower_ibp")
+            "gear_dual_lower_bound", "gear_crown_lower_ibp", "gear_crown_multi_workspace_bytes",
+            "gear_crown_lower_multi", "gear_crown_plain_workspace_bytes", "gear_crown_lower_plain")

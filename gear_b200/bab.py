@@ -135,6 +135,12 @@ class DomainQueue:
             return math.inf
         return float(self.key[self.active.long(), 0].min())
 
+    def min_key_tensor(self) -> torch.Tensor:
+        """min_key() as a (1,) device tensor (no host read)."""
+        if len(self) == 0:
+            return torch.full((1,), math.inf, dtype=torch.float64, device=self.device)
+        return self.key[self.active.long(), 0].min().reshape(1)
+
 
 class BaB:
     """Branch and bound to a relative gap on one NLP instance (x in [lo, hi]).
@@ -208,20 +214,29 @@ class BaB:
             self._ws = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
         return self._ws
 
-    def update_incumbent(self, x: torch.Tensor):
-        """Primal points: evaluate the model (float64) and keep the best feasible objective."""
+    def incumbent_candidate(self, x: torch.Tensor):
+        """Best feasible objective among the primal points x (model in float64), on the device:
+        (value (1,) tensor, +inf if none, and its point), without a host read."""
         if self.model is None or x.numel() == 0:
-            return
+            return None
         with torch.no_grad():
             y = self.model(x.to(self.device, torch.float64))
         feas = (y[:, 1:] <= self.rhs).all(1) if y.shape[1] > 1 else torch.ones(y.shape[0], dtype=torch.bool,
                                                                                 device=self.device)
         obj = torch.where(feas, y[:, 0], torch.full_like(y[:, 0], math.inf))
         best = obj.min(0)
-        v = float(best.values)                # the one host read of the incumbent update
-        if v < self.incumbent:
-            self.incumbent = v
-            self.x_best = x[best.indices].detach().clone()
+        return best.values.reshape(1), x[best.indices]
+
+    def accept_incumbent(self, value: float, point: torch.Tensor):
+        if value < self.incumbent:
+            self.incumbent = value
+            self.x_best = point.detach().clone()
+
+    def update_incumbent(self, x: torch.Tensor):
+        """Primal points: evaluate the model (float64) and keep the best feasible objective."""
+        c = self.incumbent_candidate(x)
+        if c is not None:
+            self.accept_incumbent(float(c[0]), c[1])      # the one host read of the incumbent update
 
     def dual_bound(self) -> float:
         d = self.queue.min_key()
@@ -235,21 +250,20 @@ class BaB:
             return 0.0 if D > 0 else math.inf
         return (P - D) / max(1.0, abs(P), abs(D))
 
-    def step(self):
-        """One iteration; returns the number of domains bounded."""
-        q = self.queue
-        if len(q) == 0:
-            return 0
-        popped = q.pop(self.batch)
+    def select(self):
+        """Pop the next batch (thresholds at the current incumbent): [lo, hi, key, thr, (cuts)]."""
+        popped = self.queue.pop(self.batch)
+        popped[3][:, 0] = self.incumbent
+        return popped
+
+    def prune_branch(self, popped, lb, lA, lbias):
+        """Prune against the thresholds and pick split variables on the device (no host read):
+        the state finish() needs, with the survivor count in state["nk"]."""
         lo, hi, key, thr = popped[:4]
-        B = lo.shape[0]
-        thr[:, 0] = self.incumbent          # thresholds follow the current incumbent
-        self.update_incumbent((lo + hi) / 2)
         thr[:, 0] = self.incumbent
-        lb_ibp = torch.empty(B, self.S, dtype=torch.float64, device=self.device) if self.ibp_enhancement else None
-        lb, lA, lbias = self.engine.lower(lo, hi, lb_ibp=lb_ibp)
         if self.constrained:
             self._constrained_objective(lo, hi, lb, lA, lbias, popped[4], popped[5])
+        B = lo.shape[0]
         L = _lib.lib()
         stream = torch.cuda.current_stream(self.device).cuda_stream
         keep = torch.empty(B, dtype=torch.uint8, device=self.device)
@@ -262,7 +276,16 @@ class BaB:
         _lib.check(L.gear_bab_branch(_p(lA), _p(lo), _p(hi), _p(lb), _p(thr), B, self.S, self.n,
                                      _p(self.root_width), self.coeff_thresh, self.min_width_ratio, _p(split_idx),
                                      _p(ws), ws.numel(), stream), "gear_bab_branch")
-        K = int(nk.item())                   # the one host read per iteration
+        return {"popped": popped, "lb": lb, "lA": lA, "lbias": lbias, "kept": kept, "nk": nk,
+                "split_idx": split_idx, "B": B}
+
+    def finish(self, st, K: int):
+        """Split the K survivors (K = st["nk"], read by the caller) and push the children."""
+        lo, hi, key, thr = st["popped"][:4]
+        lb, lA, lbias, kept, split_idx, B = st["lb"], st["lA"], st["lbias"], st["kept"], st["split_idx"], st["B"]
+        q = self.queue
+        L = _lib.lib()
+        stream = torch.cuda.current_stream(self.device).cuda_stream
         self.stats.iterations += 1
         self.stats.bounded += B
         self.stats.pruned += B - K
@@ -309,6 +332,19 @@ class BaB:
                     out.append(g)
                 fields = out
             q.push(*fields)
+
+    def step(self):
+        """One iteration; returns the number of domains bounded."""
+        if len(self.queue) == 0:
+            return 0
+        popped = self.select()
+        lo, hi = popped[0], popped[1]
+        B = lo.shape[0]
+        self.update_incumbent((lo + hi) / 2)
+        lb_ibp = torch.empty(B, self.S, dtype=torch.float64, device=self.device) if self.ibp_enhancement else None
+        lb, lA, lbias = self.engine.lower(lo, hi, lb_ibp=lb_ibp)
+        st = self.prune_branch(popped, lb, lA, lbias)
+        self.finish(st, int(st["nk"].item()))        # the one host read per iteration
         return B
 
     def _cuts(self, lA, lbias, thr, parents):
@@ -351,3 +387,114 @@ class BaB:
             if g <= rel_gap or time.perf_counter() - t0 > time_limit:
                 break
         return self.incumbent, self.dual_bound(), self.gap()
+
+
+class _Shape:
+    """Stands in for a CrownEngine where only the widths are needed (the bounds come from a
+    shared MultiEngine)."""
+    mode = "fixed"
+
+    def __init__(self, n, S):
+        self.n, self.S = n, S
+
+
+class MultiBaB:
+    """Branch and bound on many instances at once (the uneven batch).
+
+    Every iteration pops a batch from each open instance's queue, bounds all of them in one
+    persistent CROWN launch per kernel variant (MultiEngine), then prunes, branches and splits
+    each instance with the device kernels of BaB. Host reads are batched over the instances:
+    one for all incumbent candidates, one for all survivor counts, one for all dual bounds per
+    iteration. Each instance's search is the one BaB runs for it alone (same batch order, same
+    bounds: the packed launch is bit-identical to a launch per instance)."""
+
+    def __init__(self, graphs, roots, models=None, rhs=None, batch: int = 256, programs=None, engine=None,
+                 device="cuda", ibp_enhancement: bool = True, sb_coeff_thresh: float = 1e-3,
+                 sb_min_width_ratio: float = 1e-3):
+        from .engine import MultiEngine
+        self.device = torch.device(device)
+        self.engine = engine if engine is not None else MultiEngine(graphs, programs=programs)
+        self.ibp_enhancement = ibp_enhancement
+        N = len(graphs)
+        models = models if models is not None else [None] * N
+        rhs = rhs if rhs is not None else [None] * N
+        self.babs = [BaB(graphs[i], roots[i][0], roots[i][1], rhs=rhs[i], device=device, batch=batch,
+                         engine=_Shape(self.engine.n[i], self.engine.S[i]), model=models[i],
+                         ibp_enhancement=ibp_enhancement, sb_coeff_thresh=sb_coeff_thresh,
+                         sb_min_width_ratio=sb_min_width_ratio) for i in range(N)]
+        self.iterations = 0
+        self.bounded = 0
+
+    def step(self, active):
+        """One iteration over the instances in `active`; returns the number of domains bounded."""
+        dev = self.device
+        popped = {i: self.babs[i].select() for i in active if len(self.babs[i].queue)}
+        cands = {i: self.babs[i].incumbent_candidate((p[0] + p[1]) / 2) for i, p in popped.items()}
+        keys = [i for i, c in cands.items() if c is not None]
+        if keys:
+            vals = torch.cat([cands[i][0] for i in keys]).tolist()        # one host read
+            for i, v in zip(keys, vals):
+                self.babs[i].accept_incumbent(v, cands[i][1])
+        boxes, ibp = [], []
+        for i, b in enumerate(self.babs):
+            if i in popped:
+                boxes.append((popped[i][0], popped[i][1]))
+                ibp.append(torch.empty(popped[i][0].shape[0], b.S, dtype=torch.float64, device=dev)
+                           if self.ibp_enhancement else None)
+            else:
+                e = torch.empty(0, b.n, dtype=torch.float64, device=dev)
+                boxes.append((e, e))
+                ibp.append(None)
+        outs = self.engine.lower(boxes, lb_ibp=ibp)
+        sts = {i: self.babs[i].prune_branch(popped[i], *outs[i]) for i in popped}
+        if sts:
+            Ks = torch.cat([sts[i]["nk"] for i in sts]).tolist()          # one host read
+            for i, k in zip(sts, Ks):
+                self.babs[i].finish(sts[i], int(k))
+        B = sum(p[0].shape[0] for p in popped.values())
+        self.iterations += 1
+        self.bounded += B
+        return B
+
+    def gaps(self, idx):
+        """Relative gaps of the instances in idx (one host read)."""
+        if not idx:
+            return []
+        D = torch.cat([torch.minimum(self.babs[i].queue.min_key_tensor(), self.babs[i].disc_min) for i in idx]).tolist()
+        out = []
+        for i, d in zip(idx, D):
+            P = self.babs[i].incumbent
+            if not math.isfinite(P):
+                out.append(math.inf)
+            elif not math.isfinite(d):
+                out.append(0.0 if d > 0 else math.inf)
+            else:
+                out.append((P - d) / max(1.0, abs(P), abs(d)))
+        return out
+
+    def run(self, rel_gap: float = 1e-4, time_limit: float = 60.0, max_iterations: int = 10000):
+        """Iterate until every instance reaches the gap (or empties its queue), or a limit.
+        Returns per instance: incumbent, dual bound, gap, wall time to the gap (None if not
+        reached), iterations it took part in."""
+        N = len(self.babs)
+        t0 = time.perf_counter()
+        active = list(range(N))
+        reached = [None] * N
+        rounds = [0] * N
+        last = [math.inf] * N
+        while active and self.iterations < max_iterations and time.perf_counter() - t0 < time_limit:
+            self.step(active)
+            for i in active:
+                rounds[i] += 1
+            gaps = self.gaps(active)
+            now = time.perf_counter() - t0
+            nxt = []
+            for i, g in zip(active, gaps):
+                last[i] = g
+                if g <= rel_gap or len(self.babs[i].queue) == 0:
+                    reached[i] = now if g <= rel_gap else None
+                else:
+                    nxt.append(i)
+            active = nxt
+        return [{"P": b.incumbent, "gap": last[i], "time_to_gap": reached[i], "iterations": rounds[i],
+                 "bounded": b.stats.bounded} for i, b in enumerate(self.babs)]

@@ -903,8 +903,17 @@ __device__ __forceinline__ void gemv_row(const double* V, const int32_t* vcols, 
     }
 }
 
-template <int NT>
-__device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops, const Work& wk) {
+// One CROWN pass. phase bit 1: clear the row arrays and set the initial A at the pass's target;
+// ops [op_lo, op_hi) of the pass then run; phase bit 2: concretise and write the outputs. The
+// fused kernels run everything in one call; the plain form calls each phase and each op in a
+// launch of its own (the working set then lives in global memory).
+template <int NT, bool WHOLE = true>
+__device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops, const Work& wk, int op_lo_ = 0,
+                         int op_hi_ = 1 << 30, int phase_ = 3) {
+  // WHOLE: every phase and every op (compile-time constants for the fused kernels)
+  const int op_lo = WHOLE ? 0 : op_lo_;
+  const int op_hi = WHOLE ? (1 << 30) : op_hi_;
+  const int phase = WHOLE ? 3 : phase_;
   constexpr int NWARP = NT / 32;
   const DevProgram* P = bx.P;
   const int32_t* pr = P->passes + pid * PASS_REC;
@@ -928,6 +937,7 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
   const double fbox = ((double)n + 16) * EPS * 4;                             // box dot products
   const int32_t* tnd = node_rec(P, t);
 
+  if (phase & 1) {
   for (int k = tid; k < sides * ctx.nrows * S; k += NT) ctx.rows[k] = 0.0;
   // initial A at t
   {
@@ -945,6 +955,7 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
     }
   }
   __syncthreads();
+  }
 
   const int op0 = pr[P_OP0], nop = pr[P_NOP];
   // this pass's op records in shared memory (decoded once per box instead of per access)
@@ -955,7 +966,8 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
   long long t_op = clock64();
   extern __device__ unsigned long long g_op_cycles[];
 #endif
-  for (int oi = 0; oi < nop; ++oi) {
+  const int op_end = min(nop, op_hi);
+  for (int oi = op_lo; oi < op_end; ++oi) {
     const int32_t* op = sops + oi * OP_REC;
     const int kind = op[O_KIND], v = op[O_V], slot = op[O_SLOT];
     const int32_t* vnd = node_rec(P, v);
@@ -1196,6 +1208,7 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
     }
 #endif
   }
+  if (!(phase & 2)) return;
 #ifdef GEAR_STEP_PROFILE
   if (tid == 0) t_op = clock64();
 #endif
@@ -1326,23 +1339,11 @@ __device__ void compare_node(const Box& bx, int v, double* tmp_lo, double* tmp_h
 }
 
 
-template <int NT>
-__global__ void __launch_bounds__(NT, GEAR_CTA_MINB / NT) crown_megakernel(DevProgram Pg, Work wk) {
-  extern __shared__ double sm[];
-  const int32_t* hdr = Pg.hdr;
-  // shared memory: [pass working set | node table | op records of the running pass]
-  const int pass_doubles = hdr[H_SMEM] - ((hdr[H_NNODES] * NODE_REC + hdr[H_MAXOPS] * OP_REC + 1) / 2 + 2);
-  int32_t* snodes = reinterpret_cast<int32_t*>(sm + pass_doubles);
-  int32_t* sops = snodes + hdr[H_NNODES] * NODE_REC;
-  for (int k = threadIdx.x; k < hdr[H_NNODES] * NODE_REC; k += NT) snodes[k] = __ldg(Pg.nodes + k);
-  __syncthreads();
-  DevProgram P = Pg;
-  P.nodes = snodes;
+// Lay out the box's arrays in a scratch slot (and the pass working set, when the program keeps
+// it in global memory).
+__device__ __forceinline__ void cta_slot(Box& bx, double*& tmp_lo, double*& tmp_hi, double*& work, const int32_t* hdr,
+                                         double* sm, double* slot) {
   const int arena = hdr[H_ARENA], planes_w = hdr[H_PLANES], fold_w = hdr[H_FOLDW], maxw = hdr[H_MAXW];
-  const int n = hdr[H_N];
-  double* slot = wk.scratch + (size_t)blockIdx.x * wk.slot_doubles;
-  Box bx;
-  bx.P = &P;
   bx.lo = slot;
   bx.hi = slot + arena;
   bx.mag = slot + 2 * (size_t)arena;
@@ -1350,69 +1351,209 @@ __global__ void __launch_bounds__(NT, GEAR_CTA_MINB / NT) crown_megakernel(DevPr
   bx.fold = bx.planes + planes_w;
   bx.pres_lo = bx.fold + fold_w;
   bx.pres_hi = bx.pres_lo + maxw;
-  double* tmp_lo = bx.pres_hi + maxw;
-  double* tmp_hi = tmp_lo + maxw;
-  const int nsteps = hdr[H_NSTEPS];
-  for (int64_t b = blockIdx.x; b < wk.B; b += gridDim.x) {
-    bx.b = b;
-    bx.xL = wk.xL + (size_t)b * n;
-    bx.xU = wk.xU + (size_t)b * n;
-    int open = 0;
-    for (int j = threadIdx.x; j < n; j += NT) {
-      const double l = bx.xL[j], h = bx.xU[j];
+  tmp_lo = bx.pres_hi + maxw;
+  tmp_hi = tmp_lo + maxw;
+  work = hdr[H_PASS_GLOBAL] > 0 ? slot + cta_slot_fixed(hdr) : sm;
+}
+
+// Bind a program to this CTA: copy its node records into shared memory (after the pass working
+// set; P.nodes then points there) and lay out the box's arrays in the CTA's scratch slot.
+// Returns the shared-memory area for the running pass's op records. Every thread calls it; it
+// ends with a barrier.
+template <int NT>
+__device__ __forceinline__ int32_t* cta_bind(DevProgram& P, Box& bx, double*& tmp_lo, double*& tmp_hi, double*& work,
+                                             const DevProgram& Pg, double* sm, double* slot) {
+  const int32_t* hdr = Pg.hdr;
+  // shared memory: [pass working set | node table | op records of the running pass]; a working
+  // set too large for shared memory sits at the end of the scratch slot instead
+  const int pass_doubles = hdr[H_SMEM] - ((hdr[H_NNODES] * NODE_REC + hdr[H_MAXOPS] * OP_REC + 1) / 2 + 2);
+  int32_t* snodes = reinterpret_cast<int32_t*>(sm + pass_doubles);
+  __syncthreads();                                   // the previous program's last reads are done
+  for (int k = threadIdx.x; k < hdr[H_NNODES] * NODE_REC; k += NT) snodes[k] = __ldg(Pg.nodes + k);
+  __syncthreads();
+  P = Pg;
+  P.nodes = snodes;
+  bx.P = &P;
+  cta_slot(bx, tmp_lo, tmp_hi, work, hdr, sm, slot);
+  return snodes + hdr[H_NNODES] * NODE_REC;
+}
+
+// Point the box at box b of wk; with load, copy its input box into the input node's interval.
+// Every thread calls it; it ends with a barrier.
+template <int NT>
+__device__ __forceinline__ void cta_load(Box& bx, const int32_t* hdr, const Work& wk, int64_t b, bool load) {
+  const int n = hdr[H_N];
+  bx.b = b;
+  bx.xL = wk.xL + (size_t)b * n;
+  bx.xU = wk.xU + (size_t)b * n;
+  int open = 0;
+  for (int j = threadIdx.x; j < n; j += NT) {
+    const double l = bx.xL[j], h = bx.xU[j];
+    if (load) {
       bx.lo[j] = l;
       bx.hi[j] = h;
-      open |= box_open(l, h);
     }
-    bx.open = __syncthreads_or(open);
-    for (int si = 0; si < nsteps; ++si) {
-#ifdef GEAR_STEP_PROFILE
-      long long t_step = clock64();
-#endif
-      const int32_t* st = P.steps + si * STEP_REC;
-      const int type = st[0], a = st[1];
-      switch (type) {
-        case ST_FOLD: fold_node<NT>(bx, a, sm); break;
-        case ST_IBP: {
-          const int32_t* nd = node_rec(&P, a);
-          ibp_node<NT>(bx, a, tmp_lo, tmp_hi);
-          __syncthreads();
-          const bool with_mag = st[2] != 0;
-          for (int j = threadIdx.x; j < nd[N_W]; j += NT) {
-            bx.lo[nd[N_CUR] + j] = tmp_lo[j];
-            bx.hi[nd[N_CUR] + j] = tmp_hi[j];
-            if (with_mag) bx.mag[nd[N_CUR] + j] = magnitude(tmp_lo[j], tmp_hi[j]);
-          }
-          break;
-        }
-        case ST_MAG: {
-          const int32_t* nd = node_rec(&P, a);
-          for (int j = threadIdx.x; j < nd[N_W]; j += NT) {
-            bx.mag[nd[N_CUR] + j] = magnitude(bx.lo[nd[N_CUR] + j], bx.hi[nd[N_CUR] + j]);
-          }
-          break;
-        }
-        case ST_RELAX: relax_node<NT>(bx, a); break;
-        case ST_IBPOUT: {
-          if (wk.lb_ibp) {
-            const int32_t* nd = node_rec(&P, a);
-            const int wt = nd[N_W], S = hdr[H_S];
-            const double* Cb = wk.C ? wk.C + (size_t)b * S * wt : nullptr;
-            for (int s = threadIdx.x; s < S; s += NT)
-              wk.lb_ibp[(size_t)b * S + s] = spec_row_lower(Cb, wt, (const double*)bx.lo, (const double*)bx.hi,
-                                                            nd[N_CUR], s);
-          }
-          break;
-        }
-        case ST_PASS: case ST_FINAL: run_pass<NT>(bx, a, sm, sops, wk); break;
-        case ST_COMPARE: compare_node<NT>(bx, a, tmp_lo, tmp_hi, st[3] != 0); break;
-        default: break;
-      }
+    open |= box_open(l, h);
+  }
+  bx.open = __syncthreads_or(open);
+}
+
+// Schedule step si of the bound program for the current box (a CROWN pass: ops [op_lo, op_hi)
+// and the phases of run_pass).
+template <int NT, bool WHOLE = true>
+__device__ __forceinline__ void cta_step(const DevProgram& P, Box& bx, double* tmp_lo, double* tmp_hi, int32_t* sops,
+                                         const Work& wk, double* work, int si, int op_lo = 0, int op_hi = 1 << 30,
+                                         int phase = 3) {
+  const int32_t* hdr = P.hdr;
+  const int64_t b = bx.b;
+  const int32_t* st = P.steps + si * STEP_REC;
+  const int type = st[0], a = st[1];
+  switch (type) {
+    case ST_FOLD: fold_node<NT>(bx, a, work); break;
+    case ST_IBP: {
+      const int32_t* nd = node_rec(&P, a);
+      ibp_node<NT>(bx, a, tmp_lo, tmp_hi);
       __syncthreads();
-#ifdef GEAR_STEP_PROFILE
-      if (threadIdx.x == 0 && si < 8192) atomicAdd(&g_step_cycles[si], (unsigned long long)(clock64() - t_step));
-#endif
+      const bool with_mag = st[2] != 0;
+      for (int j = threadIdx.x; j < nd[N_W]; j += NT) {
+        bx.lo[nd[N_CUR] + j] = tmp_lo[j];
+        bx.hi[nd[N_CUR] + j] = tmp_hi[j];
+        if (with_mag) bx.mag[nd[N_CUR] + j] = magnitude(tmp_lo[j], tmp_hi[j]);
+      }
+      break;
     }
+    case ST_MAG: {
+      const int32_t* nd = node_rec(&P, a);
+      for (int j = threadIdx.x; j < nd[N_W]; j += NT) {
+        bx.mag[nd[N_CUR] + j] = magnitude(bx.lo[nd[N_CUR] + j], bx.hi[nd[N_CUR] + j]);
+      }
+      break;
+    }
+    case ST_RELAX: relax_node<NT>(bx, a); break;
+    case ST_IBPOUT: {
+      if (wk.lb_ibp) {
+        const int32_t* nd = node_rec(&P, a);
+        const int wt = nd[N_W], S = hdr[H_S];
+        const double* Cb = wk.C ? wk.C + (size_t)b * S * wt : nullptr;
+        for (int s = threadIdx.x; s < S; s += NT)
+          wk.lb_ibp[(size_t)b * S + s] = spec_row_lower(Cb, wt, (const double*)bx.lo, (const double*)bx.hi,
+                                                        nd[N_CUR], s);
+      }
+      break;
+    }
+    case ST_PASS: case ST_FINAL:
+      if (WHOLE) run_pass<NT, true>(bx, a, work, sops, wk);
+      else run_pass<NT, false>(bx, a, work, sops, wk, op_lo, op_hi, phase);
+      break;
+    case ST_COMPARE: compare_node<NT>(bx, a, tmp_lo, tmp_hi, st[3] != 0); break;
+    default: break;
+  }
+}
+
+// The whole schedule for box b of wk on the bound program.
+template <int NT>
+__device__ __forceinline__ void cta_box(const DevProgram& P, Box& bx, double* tmp_lo, double* tmp_hi, int32_t* sops,
+                                        const Work& wk, int64_t b, double* work) {
+  const int nsteps = P.hdr[H_NSTEPS];
+  cta_load<NT>(bx, P.hdr, wk, b, true);
+  for (int si = 0; si < nsteps; ++si) {
+#ifdef GEAR_STEP_PROFILE
+    long long t_step = clock64();
+#endif
+    cta_step<NT>(P, bx, tmp_lo, tmp_hi, sops, wk, work, si);
+    __syncthreads();
+#ifdef GEAR_STEP_PROFILE
+    if (threadIdx.x == 0 && si < 8192) atomicAdd(&g_step_cycles[si], (unsigned long long)(clock64() - t_step));
+#endif
+  }
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT, GEAR_CTA_MINB / NT) crown_megakernel(DevProgram Pg, Work wk) {
+  extern __shared__ double sm[];
+  DevProgram P;
+  Box bx;
+  double *tmp_lo, *tmp_hi, *work;
+  int32_t* sops = cta_bind<NT>(P, bx, tmp_lo, tmp_hi, work, Pg, sm, wk.scratch + (size_t)blockIdx.x * wk.slot_doubles);
+  for (int64_t b = blockIdx.x; b < wk.B; b += gridDim.x) cta_box<NT>(P, bx, tmp_lo, tmp_hi, sops, wk, b, work);
+}
+
+// ------------------------------------------------------------------ the plain (unfused) form
+// One schedule step of every box per launch, and within a CROWN pass one launch for its initial
+// A, one per op (one node's backward step into one input) and one for its concretisation: the
+// unfused baseline the fused kernels are measured against, on the same device code. Each box has
+// a scratch slot of its own (its state crosses launches through global memory; the program is
+// compiled with its pass working set there). Step -1 loads the boxes.
+template <int NT>
+__global__ void __launch_bounds__(NT, GEAR_CTA_MINB / NT)
+crown_plain_kernel(DevProgram Pg, Work wk, int si, int op_lo, int op_hi, int phase) {
+  extern __shared__ double sm[];
+  DevProgram P;
+  Box bx;
+  double *tmp_lo, *tmp_hi, *work;
+  int32_t* sops = cta_bind<NT>(P, bx, tmp_lo, tmp_hi, work, Pg, sm, wk.scratch + (size_t)blockIdx.x * wk.slot_doubles);
+  for (int64_t b = blockIdx.x; b < wk.B; b += gridDim.x) {
+    cta_slot(bx, tmp_lo, tmp_hi, work, Pg.hdr, sm, wk.scratch + (size_t)b * wk.slot_doubles);
+    cta_load<NT>(bx, Pg.hdr, wk, b, si < 0);
+    if (si >= 0) cta_step<NT, false>(P, bx, tmp_lo, tmp_hi, sops, wk, work, si, op_lo, op_hi, phase);
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ several programs, one launch
+// One instance of a multi-instance launch: its program and its boxes / outputs (the Work's
+// scratch fields are unused: the launch's slots are sized for the largest program).
+struct MultiItem {
+  DevProgram P;
+  Work wk;
+};
+
+// Index of the instance owning work item g: the last i with start[i] <= g (start ascending,
+// start[0] = 0).
+__device__ __forceinline__ int multi_owner(const int64_t* start, int count, long long g) {
+  int lo = 0, hi = count - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (start[mid] <= g) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Boxes of many instances (different programs and widths) in one persistent launch. Work item g
+// is box g - start[i] of instance i; CTAs take items from a device counter, so instances of
+// uneven cost balance over the SMs (the caller orders them by cost, largest first). A CTA
+// rebinds its shared-memory node table only when the instance changes.
+template <int NT>
+__global__ void __launch_bounds__(NT, GEAR_CTA_MINB / NT)
+crown_multi_megakernel(const MultiItem* __restrict__ items, int count, const int64_t* __restrict__ start,
+                       unsigned long long* next, double* scratch, int64_t slot_doubles) {
+  extern __shared__ double sm[];
+  __shared__ long long s_g;
+  __shared__ int s_i;
+  DevProgram P;
+  Box bx;
+  double *tmp_lo = nullptr, *tmp_hi = nullptr, *work = nullptr;
+  int32_t* sops = nullptr;
+  double* slot = scratch + (size_t)blockIdx.x * slot_doubles;
+  const long long total = start[count];
+  int cur = -1;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const long long g = (long long)atomicAdd(next, 1ull);
+      s_g = g;
+      s_i = g < total ? multi_owner(start, count, g) : 0;
+    }
+    __syncthreads();
+    const long long g = s_g;
+    const int i = s_i;
+    __syncthreads();                                 // s_g, s_i are rewritten by the next fetch
+    if (g >= total) break;
+    if (i != cur) {
+      sops = cta_bind<NT>(P, bx, tmp_lo, tmp_hi, work, items[i].P, sm, slot);
+      cur = i;
+    }
+    cta_box<NT>(P, bx, tmp_lo, tmp_hi, sops, items[i].wk, g - start[i], work);   // Work read in place
   }
 }
 

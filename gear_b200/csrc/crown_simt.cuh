@@ -506,14 +506,12 @@ __device__ void simt_run_pass(const SBox& bx, int pid, const Work& wk, bool live
   }
 }
 
-__global__ void __launch_bounds__(SIMT_T, 8) crown_simt_kernel(DevProgram Pg, Work wk) {
-  const int32_t* hdr = Pg.hdr;
-  const int64_t items = simt_items(hdr);
-  const int arena = hdr[H_ARENA], maxw = hdr[H_MAXW], n = hdr[H_N];
-  const int64_t ntiles = (wk.B + SIMT_T - 1) / SIMT_T;
-  double* tile = wk.scratch + (size_t)blockIdx.x * items * SIMT_T + threadIdx.x;
-  SBox bx;
-  bx.P = &Pg;
+// Lay out the box-interleaved views of one program in this CTA's scratch region.
+__device__ __forceinline__ void simt_bind(SBox& bx, const DevProgram* Pg, double* cta_base) {
+  const int32_t* hdr = Pg->hdr;
+  const int arena = hdr[H_ARENA], maxw = hdr[H_MAXW];
+  double* tile = cta_base + threadIdx.x;
+  bx.P = Pg;
   int64_t o = 0;
   bx.lo = SView{tile + o * SIMT_T}; o += arena;
   bx.hi = SView{tile + o * SIMT_T}; o += arena;
@@ -526,85 +524,129 @@ __global__ void __launch_bounds__(SIMT_T, 8) crown_simt_kernel(DevProgram Pg, Wo
   bx.tmp_hi = SView{tile + o * SIMT_T}; o += maxw;
   bx.buf = SView{tile + o * SIMT_T}; o += hdr[H_SIMT_BUF];
   bx.rows = SView{tile + o * SIMT_T};
+}
+
+// Tile ti (boxes ti*SIMT_T ...) of wk: the whole schedule, one box per thread.
+__device__ __forceinline__ void simt_tile(SBox& bx, const Work& wk, int64_t ti, double* cta_base) {
+  const DevProgram& Pg = *bx.P;
+  const int32_t* hdr = Pg.hdr;
+  const int arena = hdr[H_ARENA], n = hdr[H_N];
   const int nsteps = hdr[H_NSTEPS];
-  for (int64_t ti = blockIdx.x; ti < ntiles; ti += gridDim.x) {
-    const int64_t b_real = ti * SIMT_T + threadIdx.x;
-    const bool live = b_real < wk.B;
-    const int64_t b = live ? b_real : wk.B - 1;   // a tail thread repeats the last box, writes nothing
-    bx.b = b;
-    // the tile's input boxes are consecutive rows of (B, n): read them coalesced, write them
-    // box-interleaved into the input node's interval slots (arena offset 0)
-    __syncthreads();
-    {
-      const int64_t b0 = ti * SIMT_T;
-      const int nb = (int)min((int64_t)SIMT_T, wk.B - b0);
-      double* base = wk.scratch + (size_t)blockIdx.x * items * SIMT_T;
-      for (int k = threadIdx.x; k < SIMT_T * n; k += SIMT_T) {
-        const int bb = k / n, j = k - bb * n;
-        const int64_t src = (b0 + min(bb, nb - 1)) * n + j;
-        base[(int64_t)j * SIMT_T + bb] = wk.xL[src];
-        base[((int64_t)arena + j) * SIMT_T + bb] = wk.xU[src];
+  const int64_t b_real = ti * SIMT_T + threadIdx.x;
+  const bool live = b_real < wk.B;
+  const int64_t b = live ? b_real : wk.B - 1;   // a tail thread repeats the last box, writes nothing
+  bx.b = b;
+  // the tile's input boxes are consecutive rows of (B, n): read them coalesced, write them
+  // box-interleaved into the input node's interval slots (arena offset 0)
+  __syncthreads();
+  {
+    const int64_t b0 = ti * SIMT_T;
+    const int nb = (int)min((int64_t)SIMT_T, wk.B - b0);
+    double* base = cta_base;
+    for (int k = threadIdx.x; k < SIMT_T * n; k += SIMT_T) {
+      const int bb = k / n, j = k - bb * n;
+      const int64_t src = (b0 + min(bb, nb - 1)) * n + j;
+      base[(int64_t)j * SIMT_T + bb] = wk.xL[src];
+      base[((int64_t)arena + j) * SIMT_T + bb] = wk.xU[src];
+    }
+  }
+  __syncthreads();
+  bx.open = 0;
+  for (int j = 0; j < n; ++j) bx.open |= box_open(bx.lo[j], bx.hi[j]);
+  for (int si = 0; si < nsteps; ++si) {
+#ifdef GEAR_STEP_PROFILE
+    long long t_step = clock64();
+#endif
+    const int32_t* st = Pg.steps + si * STEP_REC;
+    const int type = st[0], a = st[1];
+    switch (type) {
+      case ST_FOLD: simt_fold_node(bx, a); break;
+      case ST_IBP: {
+        const int32_t* nd = node_rec(&Pg, a);
+        simt_ibp_node(bx, a, bx.tmp_lo, bx.tmp_hi);
+        const bool with_mag = st[2] != 0;
+        for (int j = 0; j < nd[N_W]; ++j) {
+          double l = bx.tmp_lo[j], h = bx.tmp_hi[j];
+          bx.lo[nd[N_CUR] + j] = l;
+          bx.hi[nd[N_CUR] + j] = h;
+          if (with_mag) bx.mag[nd[N_CUR] + j] = magnitude(l, h);
+        }
+        break;
       }
+      case ST_MAG: {
+        const int32_t* nd = node_rec(&Pg, a);
+        for (int j = 0; j < nd[N_W]; ++j) bx.mag[nd[N_CUR] + j] = magnitude(bx.lo[nd[N_CUR] + j], bx.hi[nd[N_CUR] + j]);
+        break;
+      }
+      case ST_RELAX: simt_relax_node(bx, a); break;
+      case ST_IBPOUT: {
+        if (wk.lb_ibp && live) {
+          const int32_t* nd = node_rec(&Pg, a);
+          const int wt = nd[N_W], S = hdr[H_S];
+          const double* Cb = wk.C ? wk.C + (size_t)b * S * wt : nullptr;
+          for (int s = 0; s < S; ++s)
+            wk.lb_ibp[(size_t)b * S + s] = spec_row_lower(Cb, wt, bx.lo, bx.hi, nd[N_CUR], s);
+        }
+        break;
+      }
+      case ST_PASS: case ST_FINAL: simt_run_pass(bx, a, wk, live); break;
+      case ST_COMPARE: {
+        const int32_t* nd = node_rec(&Pg, a);
+        simt_ibp_node(bx, a, bx.tmp_lo, bx.tmp_hi);
+        const bool with_mag = st[3] != 0;
+        for (int j = 0; j < nd[N_W]; ++j) {
+          double l = nan_lo(bx.pres_lo[j]), h = nan_hi(bx.pres_hi[j]);
+          double lo_ = fmax(l, bx.tmp_lo[j]), hi_ = fmin(h, bx.tmp_hi[j]);
+          bx.lo[nd[N_CUR] + j] = lo_;
+          bx.hi[nd[N_CUR] + j] = hi_;
+          if (with_mag) bx.mag[nd[N_CUR] + j] = magnitude(lo_, hi_);
+        }
+        break;
+      }
+      default: break;
+    }
+#ifdef GEAR_STEP_PROFILE
+    if (threadIdx.x == 0 && si < 8192) atomicAdd(&g_step_cycles[si], (unsigned long long)(clock64() - t_step));
+#endif
+  }
+}
+
+__global__ void __launch_bounds__(SIMT_T, 8) crown_simt_kernel(DevProgram Pg, Work wk) {
+  const int64_t items = simt_items(Pg.hdr);
+  const int64_t ntiles = (wk.B + SIMT_T - 1) / SIMT_T;
+  double* cta_base = wk.scratch + (size_t)blockIdx.x * items * SIMT_T;
+  SBox bx;
+  simt_bind(bx, &Pg, cta_base);
+  for (int64_t ti = blockIdx.x; ti < ntiles; ti += gridDim.x) simt_tile(bx, wk, ti, cta_base);
+}
+
+// Tiles of many instances in one persistent launch (work item g: tile g - start[i] of instance
+// i, taken from a device counter; slots sized for the largest program).
+__global__ void __launch_bounds__(SIMT_T, 8)
+crown_multi_simt_kernel(const MultiItem* __restrict__ items, int count, const int64_t* __restrict__ start,
+                        unsigned long long* next, double* scratch, int64_t slot_doubles) {
+  __shared__ long long s_g;
+  __shared__ int s_i;
+  double* cta_base = scratch + (size_t)blockIdx.x * slot_doubles;
+  const long long total = start[count];
+  int cur = -1;
+  SBox bx;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const long long g = (long long)atomicAdd(next, 1ull);
+      s_g = g;
+      s_i = g < total ? multi_owner(start, count, g) : 0;
     }
     __syncthreads();
-    bx.open = 0;
-    for (int j = 0; j < n; ++j) bx.open |= box_open(bx.lo[j], bx.hi[j]);
-    for (int si = 0; si < nsteps; ++si) {
-#ifdef GEAR_STEP_PROFILE
-      long long t_step = clock64();
-#endif
-      const int32_t* st = Pg.steps + si * STEP_REC;
-      const int type = st[0], a = st[1];
-      switch (type) {
-        case ST_FOLD: simt_fold_node(bx, a); break;
-        case ST_IBP: {
-          const int32_t* nd = node_rec(&Pg, a);
-          simt_ibp_node(bx, a, bx.tmp_lo, bx.tmp_hi);
-          const bool with_mag = st[2] != 0;
-          for (int j = 0; j < nd[N_W]; ++j) {
-            double l = bx.tmp_lo[j], h = bx.tmp_hi[j];
-            bx.lo[nd[N_CUR] + j] = l;
-            bx.hi[nd[N_CUR] + j] = h;
-            if (with_mag) bx.mag[nd[N_CUR] + j] = magnitude(l, h);
-          }
-          break;
-        }
-        case ST_MAG: {
-          const int32_t* nd = node_rec(&Pg, a);
-          for (int j = 0; j < nd[N_W]; ++j) bx.mag[nd[N_CUR] + j] = magnitude(bx.lo[nd[N_CUR] + j], bx.hi[nd[N_CUR] + j]);
-          break;
-        }
-        case ST_RELAX: simt_relax_node(bx, a); break;
-        case ST_IBPOUT: {
-          if (wk.lb_ibp && live) {
-            const int32_t* nd = node_rec(&Pg, a);
-            const int wt = nd[N_W], S = hdr[H_S];
-            const double* Cb = wk.C ? wk.C + (size_t)b * S * wt : nullptr;
-            for (int s = 0; s < S; ++s)
-              wk.lb_ibp[(size_t)b * S + s] = spec_row_lower(Cb, wt, bx.lo, bx.hi, nd[N_CUR], s);
-          }
-          break;
-        }
-        case ST_PASS: case ST_FINAL: simt_run_pass(bx, a, wk, live); break;
-        case ST_COMPARE: {
-          const int32_t* nd = node_rec(&Pg, a);
-          simt_ibp_node(bx, a, bx.tmp_lo, bx.tmp_hi);
-          const bool with_mag = st[3] != 0;
-          for (int j = 0; j < nd[N_W]; ++j) {
-            double l = nan_lo(bx.pres_lo[j]), h = nan_hi(bx.pres_hi[j]);
-            double lo_ = fmax(l, bx.tmp_lo[j]), hi_ = fmin(h, bx.tmp_hi[j]);
-            bx.lo[nd[N_CUR] + j] = lo_;
-            bx.hi[nd[N_CUR] + j] = hi_;
-            if (with_mag) bx.mag[nd[N_CUR] + j] = magnitude(lo_, hi_);
-          }
-          break;
-        }
-        default: break;
-      }
-#ifdef GEAR_STEP_PROFILE
-      if (threadIdx.x == 0 && si < 8192) atomicAdd(&g_step_cycles[si], (unsigned long long)(clock64() - t_step));
-#endif
+    const long long g = s_g;
+    const int i = s_i;
+    __syncthreads();
+    if (g >= total) break;
+    if (i != cur) {
+      simt_bind(bx, &items[i].P, cta_base);          // program and Work read in place
+      cur = i;
     }
+    simt_tile(bx, items[i].wk, g - start[i], cta_base);
   }
 }
 

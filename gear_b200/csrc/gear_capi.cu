@@ -8,6 +8,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "../../include/gear_b200.h"
 #include "crown_kernel.cuh"
@@ -46,6 +47,8 @@ struct gear_dag {
   int mode = 0;           // gear::ExecMode
   int threads = 0;        // threads per CTA
   int64_t boxes_per_slot = 1;
+  std::vector<int32_t> steps;    // host copies of the step and pass records (the plain form's
+  std::vector<int32_t> passes;   // launch sequence)
 };
 
 // box-per-CTA kernel instances: dynamic shared-memory limit and resident CTAs per SM
@@ -95,6 +98,8 @@ extern "C" int gear_dag_create(const int32_t* header, int64_t header_len, const 
   gear_dag* d = new (std::nothrow) gear_dag();
   if (!d) return fail(GEAR_E_NOMEM, "gear_dag_create: %s", "host allocation");
   memcpy(d->hdr, header, sizeof(d->hdr));
+  d->steps.assign(steps, steps + n_steps_ints);
+  if (passes && n_passes_ints > 0) d->passes.assign(passes, passes + n_passes_ints);
   // one device block: doubles first (8-byte aligned), then int arrays
   size_t nd = (size_t)n_dbl, ni = (size_t)(header_len + n_nodes_ints + n_steps_ints + n_passes_ints + n_ops_ints + n_int);
   size_t bytes = nd * sizeof(double) + ni * sizeof(int32_t) + 64;
@@ -146,8 +151,7 @@ extern "C" int gear_dag_create(const int32_t* header, int64_t header_len, const 
     // per-CTA scratch: lo, hi, mag arenas; planes; fold vectors; 4 node-wide temporaries
     d->threads = header[H_CTA_THREADS];
     d->boxes_per_slot = 1;
-    d->slot_doubles = 3 * (int64_t)header[H_ARENA] + header[H_PLANES] + header[H_FOLDW] + 4 * (int64_t)header[H_MAXW] + 8;
-    d->slot_doubles = (d->slot_doubles + 31) / 32 * 32;
+    d->slot_doubles = cta_slot_fixed(header) + header[H_PASS_GLOBAL];
     d->smem_bytes = header[H_SMEM] * (int)sizeof(double);
     if (d->smem_bytes > (int)prop.sharedMemPerBlockOptin) {
       cudaFree(d->dev);
@@ -322,6 +326,270 @@ extern "C" int gear_crown_lower_static(const gear_dag* dag, const double* x_L, c
   wk.B = batch;
   wk.status = nullptr;
   return launch_crown(dag, wk, slots, (cudaStream_t)stream);
+}
+
+// ------------------------------------------------------------------ the plain (unfused) form
+namespace {
+template <int NT>
+cudaError_t plain_launch_t(const gear::DevProgram& P, const gear::Work& wk, unsigned grid, int smem, int si, int op_lo,
+                           int op_hi, int phase, cudaStream_t st) {
+  gear::crown_plain_kernel<NT><<<grid, NT, smem, st>>>(P, wk, si, op_lo, op_hi, phase);
+  return cudaGetLastError();
+}
+template <int NT>
+cudaError_t plain_prepare_t(int smem, int* bps) {
+  cudaError_t e = cudaFuncSetAttribute(gear::crown_plain_kernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, gear::crown_plain_kernel<NT>, NT, smem);
+}
+bool plain_ok(const gear_dag* d) {
+  return d && d->mode == gear::MODE_CTA && d->hdr[gear::H_PASS_GLOBAL] > 0;
+}
+}  // namespace
+
+extern "C" int64_t gear_crown_plain_workspace_bytes(const gear_dag* dag, int64_t batch) {
+  if (!plain_ok(dag) || batch < 0) return -1;
+  return batch * dag->slot_doubles * (int64_t)sizeof(double);
+}
+
+extern "C" int gear_crown_lower_plain(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
+                                      const double* C, double* lb, double* lA, double* lbias, void* workspace,
+                                      int64_t workspace_bytes, void* stream) {
+  g_launches = 0;
+  if (!dag || batch < 0) return fail(GEAR_E_INVALID, "gear_crown_lower_plain: %s", "bad arguments");
+  if (!plain_ok(dag))
+    return fail(GEAR_E_INVALID, "gear_crown_lower_plain: %s",
+                "needs a box-per-CTA program compiled with its pass working set in global memory");
+  if (batch == 0) return GEAR_OK;
+  if (!x_L || !x_U || !lb || !lA) return fail(GEAR_E_INVALID, "gear_crown_lower_plain: %s", "bad arguments");
+  if (!workspace || workspace_bytes < gear_crown_plain_workspace_bytes(dag, batch))
+    return fail(GEAR_E_WORKSPACE, "gear_crown_lower_plain: %s", "workspace too small");
+  gear::Work wk;
+  wk.xL = x_L;
+  wk.xU = x_U;
+  wk.C = C;
+  wk.lb = lb;
+  wk.lA = lA;
+  wk.lbias = lbias;
+  wk.lb_ibp = nullptr;
+  wk.scratch = (double*)workspace;
+  wk.slot_doubles = dag->slot_doubles;   // one slot per box
+  wk.B = batch;
+  wk.status = nullptr;
+  cudaStream_t st = (cudaStream_t)stream;
+  int bps = 0;
+  cudaError_t e = cudaErrorInvalidValue;
+  switch (dag->threads) {
+    case 64: e = plain_prepare_t<64>(dag->smem_bytes, &bps); break;
+    case 128: e = plain_prepare_t<128>(dag->smem_bytes, &bps); break;
+    case 256: e = plain_prepare_t<256>(dag->smem_bytes, &bps); break;
+    default: break;
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "crown_plain_kernel setup");
+  int64_t grid = (int64_t)dag->num_sms * (bps > 0 ? bps : 1);
+  if (grid > batch) grid = batch;
+  int launches = 0;
+  auto go = [&](int si, int op_lo, int op_hi, int phase) -> cudaError_t {
+    ++launches;
+    switch (dag->threads) {
+      case 64: return plain_launch_t<64>(dag->P, wk, (unsigned)grid, dag->smem_bytes, si, op_lo, op_hi, phase, st);
+      case 128: return plain_launch_t<128>(dag->P, wk, (unsigned)grid, dag->smem_bytes, si, op_lo, op_hi, phase, st);
+      default: return plain_launch_t<256>(dag->P, wk, (unsigned)grid, dag->smem_bytes, si, op_lo, op_hi, phase, st);
+    }
+  };
+  e = go(-1, 0, 0, 0);
+  const int nsteps = dag->hdr[gear::H_NSTEPS];
+  for (int si = 0; si < nsteps && e == cudaSuccess; ++si) {
+    const int type = dag->steps[(size_t)si * gear::STEP_REC], a = dag->steps[(size_t)si * gear::STEP_REC + 1];
+    if (type == gear::ST_PASS || type == gear::ST_FINAL) {
+      const int nop = dag->passes[(size_t)a * gear::PASS_REC + gear::P_NOP];
+      e = go(si, 0, 0, 1);
+      for (int oi = 0; oi < nop && e == cudaSuccess; ++oi) e = go(si, oi, oi + 1, 0);
+      if (e == cudaSuccess) e = go(si, 0, 0, 2);
+    } else {
+      e = go(si, 0, 0, 0);
+    }
+  }
+  g_launches = launches;
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "crown_plain_kernel launch");
+}
+
+// ------------------------------------------------------------------ many instances, one launch
+namespace {
+template <int NT>
+cudaError_t multi_cta_occupancy_t(int smem_bytes, int* bps) {
+  cudaError_t e = cudaFuncSetAttribute(gear::crown_multi_megakernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       smem_bytes);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, gear::crown_multi_megakernel<NT>, NT, smem_bytes);
+}
+
+struct MultiPlan {
+  int mode = 0, threads = 0, smem = 0, device = 0, count = 0;   // count: instances with boxes
+  int64_t total = 0;          // work items: boxes (box per CTA) or tiles of SIMT_T boxes
+  int64_t slot_doubles = 0;   // the largest program's slot
+  int64_t slots = 1;          // CTAs of the launch
+  int64_t items_off = 0, start_off = 0, scratch_off = 0, bytes = 0;
+};
+
+inline int64_t align256(int64_t v) { return (v + 255) / 256 * 256; }
+
+int multi_plan(const gear_lower_args* a, int32_t count, MultiPlan& pl) {
+  if (count < 0 || (count > 0 && !a)) return fail(GEAR_E_INVALID, "gear_crown_lower_multi: %s", "bad arguments");
+  bool first = true;
+  int num_sms = 0;
+  for (int32_t i = 0; i < count; ++i) {
+    const gear_dag* d = a[i].dag;
+    if (!d || a[i].batch < 0) return fail(GEAR_E_INVALID, "gear_crown_lower_multi: %s", "bad instance arguments");
+    if (a[i].batch > 0 && (!a[i].x_L || !a[i].x_U || !a[i].lb))
+      return fail(GEAR_E_INVALID, "gear_crown_lower_multi: %s", "bad instance arguments");
+    if (d->hdr[gear::H_RETA] == 0 && a[i].lA)
+      return fail(GEAR_E_INVALID, "gear_crown_lower_multi: %s", "program built without A");
+    if (d->hdr[gear::H_RETA] != 0 && d->hdr[gear::H_X_IN_LA] != 0 && !a[i].lA && a[i].batch > 0)
+      return fail(GEAR_E_INVALID, "gear_crown_lower_multi: %s", "this program accumulates A in the lA output: lA is required");
+    if (first) {
+      pl.mode = d->mode;
+      pl.threads = d->threads;
+      pl.device = d->device;
+      num_sms = d->num_sms;
+      first = false;
+    } else if (d->mode != pl.mode || d->threads != pl.threads || d->device != pl.device) {
+      return fail(GEAR_E_INVALID, "gear_crown_lower_multi: %s",
+                  "every program of one launch needs the same execution mode, threads per CTA and device");
+    }
+    if (a[i].batch == 0) continue;
+    ++pl.count;
+    pl.total += (a[i].batch + d->boxes_per_slot - 1) / d->boxes_per_slot;
+    if (d->slot_doubles > pl.slot_doubles) pl.slot_doubles = d->slot_doubles;
+    if (d->smem_bytes > pl.smem) pl.smem = d->smem_bytes;
+  }
+  if (pl.count == 0) return GEAR_OK;
+  int bps = 0;
+  cudaError_t e = cudaSuccess;
+  if (pl.mode == gear::MODE_SIMT) {
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, gear::crown_multi_simt_kernel, gear::SIMT_T, 0);
+  } else {
+    switch (pl.threads) {
+      case 64: e = multi_cta_occupancy_t<64>(pl.smem, &bps); break;
+      case 128: e = multi_cta_occupancy_t<128>(pl.smem, &bps); break;
+      case 256: e = multi_cta_occupancy_t<256>(pl.smem, &bps); break;
+      default: return fail(GEAR_E_INVALID, "gear_crown_lower_multi: %s", "threads per CTA must be 64, 128 or 256");
+    }
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "gear_crown_lower_multi occupancy");
+  if (bps < 1) bps = 1;
+  pl.slots = (int64_t)num_sms * bps;
+  if (pl.total < pl.slots) pl.slots = pl.total;
+  pl.items_off = 256;                                   // [0, 8): the work counter
+  pl.start_off = pl.items_off + align256((int64_t)pl.count * (int64_t)sizeof(gear::MultiItem));
+  pl.scratch_off = pl.start_off + align256((int64_t)(pl.count + 1) * (int64_t)sizeof(int64_t));
+  pl.bytes = pl.scratch_off + pl.slots * pl.slot_doubles * (int64_t)sizeof(double);
+  return GEAR_OK;
+}
+
+// Pinned staging for the per-launch instance table, one per device and host thread: the copy
+// from it is asynchronous, and the buffer is reused only after the previous copy has finished.
+struct Staging {
+  void* host = nullptr;
+  size_t cap = 0;
+  cudaEvent_t done = nullptr;
+};
+thread_local Staging g_staging[kMaxDevices];
+}  // namespace
+
+extern "C" int64_t gear_crown_multi_workspace_bytes(const gear_lower_args* items, int32_t count) {
+  MultiPlan pl;
+  if (multi_plan(items, count, pl) != GEAR_OK) return -1;
+  return pl.count == 0 ? 0 : pl.bytes;
+}
+
+extern "C" int gear_crown_lower_multi(const gear_lower_args* items, int32_t count, void* workspace,
+                                      int64_t workspace_bytes, void* stream) {
+  g_launches = 0;
+  MultiPlan pl;
+  int rc = multi_plan(items, count, pl);
+  if (rc != GEAR_OK) return rc;
+  if (pl.count == 0) return GEAR_OK;
+  if (!workspace || workspace_bytes < pl.bytes)
+    return fail(GEAR_E_WORKSPACE, "gear_crown_lower_multi: %s", "workspace too small");
+  if (pl.device < 0 || pl.device >= kMaxDevices)
+    return fail(GEAR_E_INVALID, "gear_crown_lower_multi: %s", "device ordinal out of range");
+  cudaStream_t st = (cudaStream_t)stream;
+  char* ws = (char*)workspace;
+  // the instance table and the work-item prefix, staged in pinned memory
+  const size_t table_bytes = (size_t)(pl.start_off - pl.items_off) + (size_t)(pl.count + 1) * sizeof(int64_t);
+  Staging& sg = g_staging[pl.device];
+  cudaError_t e = cudaSuccess;
+  if (sg.done) {
+    e = cudaEventSynchronize(sg.done);
+    if (e != cudaSuccess) return cuda_fail(e, "gear_crown_lower_multi staging");
+  }
+  if (sg.cap < table_bytes) {
+    if (sg.host) cudaFreeHost(sg.host);
+    sg.host = nullptr;
+    sg.cap = 0;
+    e = cudaHostAlloc(&sg.host, table_bytes, cudaHostAllocDefault);
+    if (e != cudaSuccess) return cuda_fail(e, "gear_crown_lower_multi staging");
+    sg.cap = table_bytes;
+  }
+  if (!sg.done) {
+    e = cudaEventCreateWithFlags(&sg.done, cudaEventDisableTiming);
+    if (e != cudaSuccess) return cuda_fail(e, "gear_crown_lower_multi staging");
+  }
+  gear::MultiItem* hitems = (gear::MultiItem*)sg.host;
+  int64_t* hstart = (int64_t*)((char*)sg.host + (pl.start_off - pl.items_off));
+  int k = 0;
+  hstart[0] = 0;
+  for (int32_t i = 0; i < count; ++i) {
+    const gear_lower_args& a = items[i];
+    if (a.batch == 0) continue;
+    gear::MultiItem& it = hitems[k];
+    it.P = a.dag->P;
+    it.wk.xL = a.x_L;
+    it.wk.xU = a.x_U;
+    it.wk.C = a.C;
+    it.wk.lb = a.lb;
+    it.wk.lA = a.lA;
+    it.wk.lbias = a.lbias;
+    it.wk.lb_ibp = a.lb_ibp;
+    it.wk.scratch = nullptr;
+    it.wk.slot_doubles = pl.slot_doubles;
+    it.wk.B = a.batch;
+    it.wk.status = nullptr;
+    hstart[k + 1] = hstart[k] + (a.batch + a.dag->boxes_per_slot - 1) / a.dag->boxes_per_slot;
+    ++k;
+  }
+  e = cudaMemsetAsync(ws, 0, sizeof(unsigned long long), st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ws + pl.items_off, sg.host, table_bytes, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaEventRecord(sg.done, st);
+  if (e != cudaSuccess) return cuda_fail(e, "gear_crown_lower_multi table upload");
+  const gear::MultiItem* ditems = (const gear::MultiItem*)(ws + pl.items_off);
+  const int64_t* dstart = (const int64_t*)(ws + pl.start_off);
+  unsigned long long* next = (unsigned long long*)ws;
+  double* scratch = (double*)(ws + pl.scratch_off);
+  const unsigned grid = (unsigned)pl.slots;
+  if (pl.mode == gear::MODE_SIMT) {
+    gear::crown_multi_simt_kernel<<<grid, gear::SIMT_T, 0, st>>>(ditems, pl.count, dstart, next, scratch,
+                                                                  pl.slot_doubles);
+  } else {
+    switch (pl.threads) {
+      case 64:
+        gear::crown_multi_megakernel<64><<<grid, 64, pl.smem, st>>>(ditems, pl.count, dstart, next, scratch,
+                                                                    pl.slot_doubles);
+        break;
+      case 128:
+        gear::crown_multi_megakernel<128><<<grid, 128, pl.smem, st>>>(ditems, pl.count, dstart, next, scratch,
+                                                                      pl.slot_doubles);
+        break;
+      default:
+        gear::crown_multi_megakernel<256><<<grid, 256, pl.smem, st>>>(ditems, pl.count, dstart, next, scratch,
+                                                                      pl.slot_doubles);
+        break;
+    }
+  }
+  g_launches = 1;
+  e = cudaGetLastError();
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "crown multi-instance launch");
 }
 
 // ------------------------------------------------------------------ branch and bound

@@ -43,8 +43,18 @@ constexpr int RED_SLOTS = 32;
 enum HeaderField {
   H_NNODES = 0, H_NSTEPS, H_NPASSES, H_NOPS, H_N, H_S, H_T, H_ARENA, H_PLANES, H_FOLDW,
   H_SMEM, H_MAXS, H_SINOFF, H_MAXW, H_RETA, H_MAXOPS, H_SIMT_BUF, H_SIMT_ROWS, H_X_IN_LA, H_MODE,
-  H_CTA_THREADS, H_R21, H_R22, H_R23, HEADER_LEN = 24
+  H_CTA_THREADS, H_PASS_GLOBAL, H_R22, H_R23, HEADER_LEN = 24
 };
+// H_PASS_GLOBAL: 0, or the doubles of a box-per-CTA program's pass working set when it is too
+// large for shared memory and lives at the end of the CTA's scratch slot instead (H_SMEM then
+// counts only the staged node table and op records).
+
+// Doubles of a box-per-CTA scratch slot before that global pass working set: interval and
+// magnitude arenas, relaxation planes, fold vectors, 4 node-wide temporaries.
+__host__ __device__ inline int64_t cta_slot_fixed(const int32_t* hdr) {
+  const int64_t d = 3 * (int64_t)hdr[H_ARENA] + hdr[H_PLANES] + hdr[H_FOLDW] + 4 * (int64_t)hdr[H_MAXW] + 8;
+  return (d + 31) / 32 * 32;
+}
 
 // execution model of a program: one box per CTA (pass working set in shared memory) or one box
 // per thread (per-box state box-interleaved in global scratch)

@@ -23,8 +23,11 @@ class _Dag:
     """One compiled program uploaded to the device (a gear_dag handle)."""
 
     def __init__(self, graph, spec_rows, dense_c, mode, cta_threads):
-        self.prog = Program(graph, spec_rows=spec_rows, dense_c=dense_c, mode=mode, cta_threads=cta_threads)
-        p = self.prog
+        self._upload(Program(graph, spec_rows=spec_rows, dense_c=dense_c, mode=mode, cta_threads=cta_threads))
+
+    def _upload(self, prog):
+        self.prog = p = prog
+        mode, cta_threads = prog.mode, prog.cta_threads
         L = _lib.lib()
         h = ctypes.c_void_p()
         arrs = [np.ascontiguousarray(a, dtype=np.int32) for a in
@@ -37,6 +40,13 @@ class _Dag:
         _lib.check(st, "gear_dag_create")
         self.handle = h
         self.name = f"{mode}{cta_threads}" if mode == "cta" else mode
+
+    @classmethod
+    def from_program(cls, prog):
+        """Upload an already compiled Program."""
+        self = cls.__new__(cls)
+        self._upload(prog)
+        return self
 
     def simt_items(self):
         p = self.prog
@@ -200,3 +210,182 @@ class CrownEngine:
             self._ws = None
             self._ws = torch.empty(max(nbytes, 8), dtype=torch.uint8, device=device)
         return self._ws
+
+
+class MultiEngine:
+    """Many instances (graphs of different widths and depths) in one kernel launch per kernel
+    variant.
+
+    ``lower(boxes)`` takes ``[(x_L_i, x_U_i), ...]`` (CUDA float64, x_L_i of shape (B_i, n_i); B_i
+    may be 0) and returns ``[(lb_i, lA_i, lbias_i), ...]``; instance i's results are the ones
+    ``CrownEngine`` gives for it alone (the same kernel code runs every box). Instances are
+    grouped by kernel variant and each group is one persistent launch: with mode "auto" an
+    instance whose per-box state fits ``simt_items_max`` doubles runs one box per thread, the
+    others one box per CTA of ``cta_threads`` threads; "cta" / "simt" put every instance in
+    that mode. Within a group, instances are handed to the launch in decreasing per-box work,
+    so the device's work counter deals the expensive boxes first."""
+
+    def __init__(self, graphs, mode: str = "auto", cta_threads: int = 256, simt_items_max: int = 8192,
+                 programs=None):
+        if not torch.cuda.is_available():
+            raise _lib.GearError("gear_b200 needs a CUDA device (no CPU fallback)")
+        if mode not in ("auto", "cta", "simt"):
+            raise ValueError(f"unknown mode {mode!r}")
+        self.graphs = list(graphs)
+        self.mode = mode
+        # programs: optional precompiled Program per instance in its variant (a compile pool)
+        self.dags = []
+        self.variants = []
+        for i, g in enumerate(self.graphs):
+            if programs is not None:
+                prog = programs[i]
+                var = (prog.mode, prog.cta_threads if prog.mode == "cta" else 0)
+            else:
+                var = ("simt", 0) if mode == "simt" else ("cta", cta_threads)
+                if mode == "auto":
+                    probe = Program(g, mode="simt")
+                    items = 3 * probe.arena_w + probe.plane_w + probe.fold_w + 4 * probe.maxw + probe.simt_buf + \
+                        probe.simt_rows
+                    var = ("simt", 0) if items <= simt_items_max else ("cta", cta_threads)
+                    prog = probe if var[0] == "simt" else None
+                else:
+                    prog = None
+                if prog is None:
+                    prog = Program(g, mode=var[0], cta_threads=var[1] if var[0] == "cta" else 128)
+            self.dags.append(_Dag.from_program(prog))
+            self.variants.append(var)
+        self.n = [d.prog.n for d in self.dags]
+        self.S = [d.prog.S for d in self.dags]
+        cost = [d.prog.alg_bytes_per_box() for d in self.dags]
+        self.groups = {}
+        for i in sorted(range(len(self.dags)), key=lambda i: (-cost[i], i)):
+            self.groups.setdefault(self.variants[i], []).append(i)
+        self._ws = {}
+        self.group_events = None
+
+    def group_names(self):
+        return {(f"cta{t}" if m == "cta" else "simt"): len(ix) for (m, t), ix in self.groups.items()}
+
+    def outputs(self, batches, device):
+        """Result tensors for these batch sizes: views into three flat buffers."""
+        tot_lb = sum(b * s for b, s in zip(batches, self.S))
+        tot_la = sum(b * s * n for b, s, n in zip(batches, self.S, self.n))
+        lb = torch.empty(max(tot_lb, 1), dtype=torch.float64, device=device)
+        lbias = torch.empty(max(tot_lb, 1), dtype=torch.float64, device=device)
+        lA = torch.empty(max(tot_la, 1), dtype=torch.float64, device=device)
+        outs, o1, o2 = [], 0, 0
+        for b, s, n in zip(batches, self.S, self.n):
+            outs.append((lb[o1:o1 + b * s].view(b, s), lA[o2:o2 + b * s * n].view(b, s, n),
+                         lbias[o1:o1 + b * s].view(b, s)))
+            o1 += b * s
+            o2 += b * s * n
+        return outs
+
+    def _args(self, idx, boxes, outs, lb_ibp=None):
+        args = (_lib.LowerArgs * len(idx))()
+        for k, i in enumerate(idx):
+            x_L, x_U = boxes[i]
+            lb, lA, lbias = outs[i]
+            B = x_L.shape[0]
+            ibp = lb_ibp[i] if lb_ibp is not None else None
+            args[k] = _lib.LowerArgs(self.dags[i].handle.value, x_L.data_ptr() if B else None,
+                                     x_U.data_ptr() if B else None, B, None, lb.data_ptr() if B else None,
+                                     lA.data_ptr() if B else None, lbias.data_ptr() if B else None,
+                                     ibp.data_ptr() if (B and ibp is not None) else None)
+        return args
+
+    def _launch(self, key, args, device):
+        L = _lib.lib()
+        nbytes = int(L.gear_crown_multi_workspace_bytes(args, len(args)))
+        if nbytes < 0:
+            _lib.check(-1, "gear_crown_multi_workspace_bytes")
+        ws = self._ws.get(key)
+        if ws is None or ws.numel() < nbytes or ws.device != device:
+            self._ws[key] = None
+            ws = self._ws[key] = torch.empty(max(nbytes, 8), dtype=torch.uint8, device=device)
+        stream = torch.cuda.current_stream(device).cuda_stream
+        _lib.check(L.gear_crown_lower_multi(args, len(args), ws.data_ptr(), ws.numel(), stream),
+                   "gear_crown_lower_multi")
+
+    def lower(self, boxes, out=None, lb_ibp=None):
+        """lb_ibp: optional list of (B_i, S_i) tensors (or None entries) receiving the rows' plain
+        IBP bounds; lb is then max(CROWN, IBP), as CrownEngine.lower(lb_ibp=...)."""
+        if len(boxes) != len(self.graphs):
+            raise ValueError(f"{len(boxes)} box sets for {len(self.graphs)} instances")
+        dev = None
+        norm = []
+        for i, (x_L, x_U) in enumerate(boxes):
+            if x_L.device.type != "cuda":
+                raise _lib.GearError("inputs must be CUDA tensors")
+            dev = x_L.device
+            B = x_L.shape[0]
+            x_L = x_L.reshape(B, self.n[i]).to(torch.float64).contiguous()
+            x_U = x_U.reshape(B, self.n[i]).to(torch.float64).contiguous()
+            norm.append((x_L, x_U))
+        if dev is None:
+            return []
+        outs = out if out is not None else self.outputs([x.shape[0] for x, _ in norm], dev)
+        for key, idx in self.groups.items():
+            if self.group_events is not None:
+                e = self.group_events.setdefault(key, (torch.cuda.Event(enable_timing=True),
+                                                       torch.cuda.Event(enable_timing=True)))
+                e[0].record()
+            self._launch(key, self._args(idx, norm, outs, lb_ibp), dev)
+            if self.group_events is not None:
+                e[1].record()
+        return outs
+
+    def group_ms(self):
+        """Device time of each group's launch in the last lower() (after record_groups())."""
+        torch.cuda.synchronize()
+        return {(f"cta{t}" if m == "cta" else "simt"): e[0].elapsed_time(e[1])
+                for (m, t), e in (self.group_events or {}).items()}
+
+    def record_groups(self, on: bool = True):
+        self.group_events = {} if on else None
+
+    def launches(self):
+        """Kernel launches per lower() call (one per variant group)."""
+        return len(self.groups)
+
+
+class PlainEngine:
+    """The plain GPU form of one instance: the same bounds as CrownEngine(mode="cta"), computed
+    unfused (gear_crown_lower_plain): one kernel launch per schedule step, and per CROWN pass one
+    launch per op plus one for its initial A and one for its concretisation, with every box's
+    state in global memory between launches. The baseline the fused launch is measured against."""
+
+    def __init__(self, graph: Graph, cta_threads: int = 128):
+        if not torch.cuda.is_available():
+            raise _lib.GearError("gear_b200 needs a CUDA device (no CPU fallback)")
+        self.dag = _Dag.from_program(Program(graph, mode="cta", cta_threads=cta_threads, smem_limit=0))
+        self.prog = self.dag.prog
+        self.n, self.S = self.prog.n, self.prog.S
+        self._ws = None
+        self.launches = 0
+
+    def lower(self, x_L: torch.Tensor, x_U: torch.Tensor, out=None):
+        B = x_L.shape[0]
+        dev = x_L.device
+        if dev.type != "cuda":
+            raise _lib.GearError("inputs must be CUDA tensors")
+        x_L = x_L.reshape(B, self.n).to(torch.float64).contiguous()
+        x_U = x_U.reshape(B, self.n).to(torch.float64).contiguous()
+        if out is None:
+            out = (torch.empty(B, self.S, dtype=torch.float64, device=dev),
+                   torch.empty(B, self.S, self.n, dtype=torch.float64, device=dev),
+                   torch.empty(B, self.S, dtype=torch.float64, device=dev))
+        if B == 0:
+            return out
+        lb, lA, lbias = out
+        L = _lib.lib()
+        nbytes = int(L.gear_crown_plain_workspace_bytes(self.dag.handle, B))
+        if self._ws is None or self._ws.numel() < nbytes or self._ws.device != dev:
+            self._ws = None
+            self._ws = torch.empty(max(nbytes, 8), dtype=torch.uint8, device=dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        _lib.check(L.gear_crown_lower_plain(self.dag.handle, x_L.data_ptr(), x_U.data_ptr(), B, None, lb.data_ptr(),
+                                            lA.data_ptr(), lbias.data_ptr(), self._ws.data_ptr(), self._ws.numel(),
+                                            stream), "gear_crown_lower_plain")
+        self.launches = int(L.gear_last_launch_count())
+        return out

@@ -99,6 +99,70 @@ class DenseAN2048(torch.nn.Module):
                 + (self.beta * y[:, :-1] * y[:, 1:]).sum(1, keepdim=True))
 
 
+class MixedFamily(torch.nn.Module):
+    """One instance of the uneven-batch family (the quad-exp family at many sizes and depths).
+
+    n = round(exp(U(ln 5, ln 500))) variables in [-2, 2]^n and depth d ~ U{3..12}: the input
+    passes through d stages cycling Mul (z <- z * z[perm] / 2), Exp (z <- exp(c z) - 1,
+    c ~ U(-1/2, 1/2)) and Sqr (z <- z^2 / 2), each mapping [-2, 2] into itself; the objective is
+    the quad-exp form on the staged vector, f = sum a_i z_i z_{i+1} + b_i exp(c_i z_i) + d_i z_i^2,
+    and m = n // 4 constraints are sums of four bilinear terms of x minus 1."""
+
+    STAGES = ("mul", "exp", "sqr")
+
+    def __init__(self, seed=4000, n=None, depth=None, terms=4):
+        super().__init__()
+        g = _gen(seed)
+        u = float(torch.rand(1, generator=g, dtype=F64))
+        dd = int(torch.randint(3, 13, (1,), generator=g))
+        self.n = n if n is not None else int(round(math.exp(math.log(5) + (math.log(500) - math.log(5)) * u)))
+        self.depth = depth if depth is not None else dd
+        n = self.n
+        self.m, self.terms = n // 4, terms
+        self.register_buffer("perm", torch.stack([torch.randperm(n, generator=g) for _ in range(self.depth)]))
+        self.register_buffer("cs", torch.rand(self.depth, n, generator=g, dtype=F64) - 0.5)
+        self.register_buffer("a", torch.randn(n - 1, generator=g, dtype=F64))
+        self.register_buffer("b", torch.randn(n, generator=g, dtype=F64))
+        self.register_buffer("c", torch.rand(n, generator=g, dtype=F64) * 2 - 1)
+        self.register_buffer("d", torch.randn(n, generator=g, dtype=F64))
+        self.register_buffer("P", torch.randint(0, n, (self.m * terms,), generator=g))
+        self.register_buffer("R", torch.randint(0, n, (self.m * terms,), generator=g))
+        self.register_buffer("W", torch.randn(self.m * terms, generator=g, dtype=F64))
+        self.box = (-2.0, 2.0)
+
+    def forward(self, x):
+        z = x
+        for t in range(self.depth):
+            kind = self.STAGES[t % 3]
+            if kind == "mul":
+                z = 0.5 * (z * z[:, self.perm[t]])
+            elif kind == "exp":
+                z = torch.exp(self.cs[t] * z) - 1.0
+            else:
+                z = 0.5 * z ** 2
+        f = ((self.a * z[:, :-1] * z[:, 1:]).sum(1, keepdim=True)
+             + (self.b * torch.exp(self.c * z)).sum(1, keepdim=True)
+             + (self.d * z ** 2).sum(1, keepdim=True))
+        if self.m == 0:
+            return f
+        bil = (self.W * x[:, self.P] * x[:, self.R]).reshape(-1, self.m, self.terms).sum(2)
+        return torch.cat([f, bil - 1.0], 1)
+
+
+def mixed_instance(k: int, **kw) -> MixedFamily:
+    """Instance k of the uneven-batch family (seed 4000 + k)."""
+    return MixedFamily(seed=4000 + k, **kw)
+
+
+def mixed_boxes(inst: MixedFamily, batch: int, k: int, seed_offset: int = 500):
+    """Sub-boxes of [-2, 2]^n for instance k: centres uniform, widths U(0.05, 1)."""
+    g = _gen(4000 + k + seed_offset)
+    n = inst.n
+    c = -2.0 + 4.0 * torch.rand(batch, n, generator=g, dtype=F64)
+    w = 0.05 + 0.95 * torch.rand(batch, n, generator=g, dtype=F64)
+    return torch.clamp(c - w / 2, min=-2.0), torch.clamp(c + w / 2, max=2.0)
+
+
 WORKLOADS = {
     "quad_exp_n10": dict(cls=QuadExpN10, index=1, n=10, width=(0.05, 1.0), kind="width", boxes=256),
     "dense_q_n200": dict(cls=DenseQN200, index=2, n=200, width=(0.0, 0.1), kind="half", boxes=4096),

@@ -28,6 +28,7 @@ The output is a handful of int32 / float64 arrays (layout constants below mirror
 """
 from __future__ import annotations
 
+import os
 from collections import deque
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional, Tuple
@@ -79,7 +80,8 @@ class PassInfo:
     final: bool
     init: int                 # 0 identity, 1 dense C
     order: List[int] = field(default_factory=list)       # BFS visit order (excl. root)
-    patterns: Dict[int, List[np.ndarray]] = field(default_factory=dict)   # node -> per-row sorted cols
+    # node -> (row ids, columns) of the A entries, ordered by row then column (unique)
+    patterns: Dict[int, Tuple[np.ndarray, np.ndarray]] = field(default_factory=dict)
 
 
 class Pools:
@@ -119,12 +121,13 @@ class Program:
     """Compiled device program for one graph and one final specification shape."""
 
     def __init__(self, graph: Graph, spec_rows: Optional[int] = None, dense_c: bool = False,
-                 return_a: bool = True, smem_limit: int = 200 * 1024, mode: str = "cta",
+                 return_a: bool = True, smem_limit: int = 232448, mode: str = "cta",
                  cta_threads: int = 128):
         """mode: "cta" runs one box per CTA with the pass working set in shared memory, and the
         final pass accumulates the input's A directly in the lA output; "simt" runs one box per
         thread with every per-box array box-interleaved in global scratch, and writes lA from the
-        pass buffers at the end."""
+        pass buffers at the end. smem_limit: bytes of shared memory one CTA may use (the sm_100
+        opt-in maximum); a box-per-CTA pass working set beyond it lives in global scratch."""
         if mode not in MODES:
             raise ProgramError(f"unknown execution mode {mode!r}")
         if cta_threads not in (64, 128, 256):
@@ -314,18 +317,25 @@ class Program:
             order.append(l)
         return order
 
-    def _contrib(self, n, slot, rows_cols):
-        """Columns of input `slot` reached from each row's columns of node n."""
+    @staticmethod
+    def _pairs(rows, cols, W):
+        """The (row, column) pairs ordered by row then column, duplicates removed (columns < W)."""
+        key = np.unique(rows * W + cols)
+        return key // W, key % W
+
+    def _contrib(self, n, slot, pat):
+        """Entries of input `slot` reached from the entries (rows, cols) of node n."""
         g = self.g
         k, a = n.kind, n.attrs
         p = n.inputs[slot]
         w_in = g[p].width
-        out = []
+        rows, cols = pat
+        W = w_in + 1
         if k in ("linear", "matmul"):
-            full = np.arange(w_in, dtype=np.int64)
-            return [full if len(c) else c for c in rows_cols]
+            r = np.unique(rows)
+            return np.repeat(r, w_in), np.tile(np.arange(w_in, dtype=np.int64), len(r))
         if k in ("neg", "sqr", "exp", "log", "sin", "cos", "pow"):
-            return rows_cols
+            return rows, cols
         if k in ("mulc", "addc", "subc", "rsubc"):
             m = a["map0"]
         elif k in ("mul", "add", "sub"):
@@ -333,24 +343,22 @@ class Program:
         elif k in MAP_KINDS:
             m = a["map"]
         elif k == "reducesum":
-            rmap = a["rmap"]
-            inv = {}
-            for i, o in enumerate(rmap):
-                inv.setdefault(int(o), []).append(i)
-            for c in rows_cols:
-                s = sorted(set(i for o in c for i in inv.get(int(o), [])))
-                out.append(np.array(s, dtype=np.int64))
-            return out
+            # every input element i with rmap[i] = o, for each entry (row, o)
+            rmap = np.asarray(a["rmap"], np.int64)
+            order = np.argsort(rmap, kind="stable")
+            first = np.searchsorted(rmap[order], cols, side="left")
+            cnt = np.searchsorted(rmap[order], cols, side="right") - first
+            base = np.repeat(first - np.concatenate([[0], np.cumsum(cnt)[:-1]]), cnt)
+            ii = order[base + np.arange(int(cnt.sum()), dtype=np.int64)]
+            return self._pairs(np.repeat(rows, cnt), ii, W)
         elif k == "concat":
             off = sum(g[q].width for q in n.inputs[:slot])
-            cm = a["cmap"] - off
-            for c in rows_cols:
-                e = cm[c]
-                out.append(np.unique(e[(e >= 0) & (e < w_in)]))
-            return out
+            e = np.asarray(a["cmap"], np.int64)[cols] - off
+            keep = (e >= 0) & (e < w_in)
+            return self._pairs(rows[keep], e[keep], W)
         else:
             raise ProgramError(k)
-        return [np.unique(m[c]) for c in rows_cols]
+        return self._pairs(rows, np.asarray(m, np.int64)[cols], W)
 
     def _add_pass(self, t, S, sides, final, init):
         g = self.g
@@ -360,9 +368,10 @@ class Program:
         if init == 0:
             if S != wt:
                 raise ProgramError("an identity specification needs one row per output element")
-            pi.patterns[t] = [np.array([s], dtype=np.int64) for s in range(S)]
+            ar = np.arange(S, dtype=np.int64)
+            pi.patterns[t] = (ar, ar.copy())
         else:
-            pi.patterns[t] = [np.arange(wt, dtype=np.int64) for _ in range(S)]
+            pi.patterns[t] = (np.repeat(np.arange(S, dtype=np.int64), wt), np.tile(np.arange(wt, dtype=np.int64), S))
         # symbolic propagation
         for v in order:
             n = g[v]
@@ -372,9 +381,11 @@ class Program:
             for slot, p in enumerate(n.inputs):
                 c = self._contrib(n, slot, pv)
                 if p not in pi.patterns:
-                    pi.patterns[p] = [np.array(x, dtype=np.int64) for x in c]
+                    pi.patterns[p] = c
                 else:
-                    pi.patterns[p] = [np.union1d(a_, b_) for a_, b_ in zip(pi.patterns[p], c)]
+                    q = pi.patterns[p]
+                    pi.patterns[p] = self._pairs(np.concatenate([q[0], c[0]]), np.concatenate([q[1], c[1]]),
+                                                 g[p].width + 1)
         self.passes.append(pi)
         return len(self.passes) - 1
 
@@ -444,7 +455,7 @@ class Program:
                     r[N_B_OFF] = P.add_dbl(a["b"])
         self.node_recs = recs
         # sin/cos tables
-        tb = tables.build()
+        tb = tables.build_cached()
         self.sin_off = P.add_dbl(np.concatenate([tb[k] for k in tables.SIN_TABLE_ORDER]))
         self.sin_lens = [len(tb[k]) for k in tables.SIN_TABLE_ORDER]
 
@@ -474,11 +485,18 @@ class Program:
         # shared memory: pass working set + staged node table + staged op records (in doubles)
         stage = (len(self.g) * NODE_REC + max_ops * OP_REC + 1) // 2 + 2
         self.smem_total = self.max_smem + stage
+        # a box-per-CTA working set beyond the opt-in shared memory of one CTA goes to the end of
+        # the CTA's scratch slot (global memory, L1/L2-cached); shared memory keeps the tables
+        self.pass_global = 0
+        if self.mode == "cta" and self.smem_total > self.smem_limit // 8:
+            self.pass_global = self.max_smem
+            self.smem_total = stage
         self.header = np.array([len(self.g), len(self.steps), len(self.passes), len(self.op_recs),
                                 self.n, self.S, self.t, self.arena_w, self.plane_w, self.fold_w,
                                 self.smem_total, self.max_S, self.sin_off, self.maxw,
                                 1 if self.return_a else 0, max_ops, self.simt_buf, self.simt_rows,
-                                1 if self.x_in_la else 0, MODES[self.mode], self.cta_threads, 0, 0, 0],
+                                1 if self.x_in_la else 0, MODES[self.mode], self.cta_threads, self.pass_global,
+                                0, 0],
                                dtype=np.int32)
 
     def _emit_pass(self, pid, pi: PassInfo):
@@ -488,11 +506,9 @@ class Program:
         pats = pi.patterns
         # entry tables per node
         rowptr, cols, nnz, lookup = {}, {}, {}, {}
-        for v, pr in pats.items():
-            lens = np.array([len(c) for c in pr], dtype=np.int64)
-            rp = np.concatenate([[0], np.cumsum(lens)])
-            cc = np.concatenate(pr) if len(pr) else np.zeros(0, np.int64)
-            rowptr[v], cols[v], nnz[v] = rp, cc, int(rp[-1])
+        for v, (pr, pc) in pats.items():
+            rp = np.concatenate([[0], np.cumsum(np.bincount(pr, minlength=S))]).astype(np.int64)
+            rowptr[v], cols[v], nnz[v] = rp, pc.astype(np.int64), int(rp[-1])
         # fold decision: root contributions only from linear/matmul-on-input ops with
         # at most one entry per row, in a non-final pass
         contributors = [v for v in pi.order if 0 in g[v].inputs and v in pats]
@@ -672,64 +688,53 @@ class Program:
         pi.nnz = nnz
 
     def _moves(self, n, slot, rowptr, cols, v, p):
-        """Pull lists: for each target entry of input p, the source entries of v."""
+        """Pull lists: for each target entry of input p, the source entries of v.
+
+        Rows are handled all at once: an entry (row s, column c) has the sort key s (W + 1) + c,
+        which orders entries by row, then column (columns ascend within a row)."""
         g = self.g
         k, a = n.kind, n.attrs
-        S = len(rowptr[v]) - 1
-        rp_u, cols_u = rowptr[p], cols[p]
+        rp_v, cols_v = np.asarray(rowptr[v], np.int64), np.asarray(cols[v], np.int64)
+        rp_u, cols_u = np.asarray(rowptr[p], np.int64), np.asarray(cols[p], np.int64)
+        S = len(rp_v) - 1
         w_in = g[p].width
-        tgt_l, src_l = [], []
+        row_v = np.repeat(np.arange(S, dtype=np.int64), np.diff(rp_v))
+        row_u = np.repeat(np.arange(S, dtype=np.int64), np.diff(rp_u))
         if k == "reducesum":
-            rmap = a["rmap"]
-            for s in range(S):
-                vc = cols[v][rowptr[v][s]:rowptr[v][s + 1]]
-                if len(vc) == 0:
-                    continue
-                pos_v = {int(c): rowptr[v][s] + j for j, c in enumerate(vc)}
-                for j in range(rp_u[s], rp_u[s + 1]):
-                    o = int(rmap[cols_u[j]])
-                    if o in pos_v:
-                        tgt_l.append(j)
-                        src_l.append([pos_v[o]])
+            W = g[v].width + 1
+            key_v = row_v * W + cols_v
+            key_u = row_u * W + np.asarray(a["rmap"], np.int64)[cols_u]
+            pos = np.searchsorted(key_v, key_u)
+            hit = pos < len(key_v)
+            hit[hit] = key_v[pos[hit]] == key_u[hit]
+            tgt = np.nonzero(hit)[0].astype(np.int64)
+            src = pos[hit].astype(np.int64)
+            sptr = np.arange(len(tgt) + 1, dtype=np.int64)
+            return tgt, sptr, src
+        if k in ("neg", "sqr", "exp", "log", "sin", "cos", "pow"):
+            m = None
+        elif k in ("mulc", "addc", "subc", "rsubc"):
+            m = a["map0"]
+        elif k in ("mul", "add", "sub"):
+            m = a["map0"] if slot == 0 else a["map1"]
+        elif k in MAP_KINDS:
+            m = a["map"]
+        elif k == "concat":
+            off = sum(g[q].width for q in n.inputs[:slot])
+            m = a["cmap"] - off
         else:
-            if k in ("neg", "sqr", "exp", "log", "sin", "cos", "pow"):
-                m = None
-            elif k in ("mulc", "addc", "subc", "rsubc"):
-                m = a["map0"]
-            elif k in ("mul", "add", "sub"):
-                m = a["map0"] if slot == 0 else a["map1"]
-            elif k in MAP_KINDS:
-                m = a["map"]
-            elif k == "concat":
-                off = sum(g[q].width for q in n.inputs[:slot])
-                m = a["cmap"] - off
-            else:
-                raise ProgramError(k)
-            for s in range(S):
-                lo, hi = rowptr[v][s], rowptr[v][s + 1]
-                if lo == hi:
-                    continue
-                vc = cols[v][lo:hi]
-                tc = vc if m is None else m[vc]
-                if k == "concat":
-                    keep = (tc >= 0) & (tc < w_in)
-                else:
-                    keep = np.ones(len(tc), bool)
-                uc = cols_u[rp_u[s]:rp_u[s + 1]]
-                idx = np.searchsorted(uc, tc[keep])
-                tj = rp_u[s] + idx
-                srcs = (lo + np.nonzero(keep)[0])
-                order = np.argsort(tj, kind="stable")
-                tj, srcs = tj[order], srcs[order]
-                uniq, start = np.unique(tj, return_index=True)
-                ends = list(start[1:]) + [len(tj)]
-                for uu, st_, en in zip(uniq, start, ends):
-                    tgt_l.append(int(uu))
-                    src_l.append(list(srcs[st_:en]))
-        tgt = np.array(tgt_l, dtype=np.int64)
-        sptr = np.concatenate([[0], np.cumsum([len(x) for x in src_l])]) if src_l else np.zeros(1, np.int64)
-        src = np.concatenate([np.array(x, dtype=np.int64) for x in src_l]) if src_l else np.zeros(0, np.int64)
-        return tgt, sptr, src
+            raise ProgramError(k)
+        tc = cols_v if m is None else np.asarray(m, np.int64)[cols_v]
+        keep = (tc >= 0) & (tc < w_in) if k == "concat" else np.ones(len(tc), bool)
+        W = w_in + 1
+        key_u = row_u * W + cols_u
+        srcs = np.nonzero(keep)[0].astype(np.int64)
+        tj = np.searchsorted(key_u, row_v[keep] * W + tc[keep]).astype(np.int64)
+        order = np.argsort(tj, kind="stable")
+        tj, srcs = tj[order], srcs[order]
+        tgt, start, counts = np.unique(tj, return_index=True, return_counts=True)
+        sptr = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        return tgt.astype(np.int64), sptr, srcs
 
     # ================================================================= info
     def alg_bytes_per_box(self) -> int:
@@ -746,3 +751,50 @@ class Program:
             lines.append(f"  pass {pid}: t={pi.t}({self.g[pi.t].kind}) S={pi.S} sides={pi.sides} final={pi.final} "
                          f"fold={pi.fold} visits={r[P_NVISIT]} smem={r[P_SMEM]} x_nnz={r[P_XNNZ]} maxrow={r[P_MAXROW]}")
         return "\n".join(lines)
+
+
+# ===================================================================== compile pools
+_KEEP = ("S", "n", "t", "mode", "cta_threads", "x_in_la", "return_a", "dense_c", "arena_w", "plane_w", "fold_w", "maxw",
+         "max_S", "max_smem", "smem_total", "pass_global", "simt_buf", "simt_rows", "sin_off", "work", "header",
+         "node_arr", "step_arr", "pass_arr", "op_arr", "int_pool", "dbl_pool")
+
+
+def stripped(prog: Program) -> Program:
+    """A copy of prog with only what the device upload and the work counters need (no graph,
+    no pass patterns): small to send between processes."""
+    out = Program.__new__(Program)
+    for k in _KEEP:
+        if hasattr(prog, k):
+            setattr(out, k, getattr(prog, k))
+    return out
+
+
+def simt_items(prog: Program) -> int:
+    """Doubles of box-per-thread scratch one box needs."""
+    return 3 * prog.arena_w + prog.plane_w + prog.fold_w + 4 * prog.maxw + prog.simt_buf + prog.simt_rows
+
+
+def _compile_job(job):
+    graph, kw, simt_items_max = job
+    if simt_items_max is not None:
+        # "auto": one box per thread when the per-box state is small, else one box per CTA
+        prog = Program(graph, mode="simt")
+        if simt_items(prog) <= simt_items_max:
+            return stripped(prog)
+    return stripped(Program(graph, **kw))
+
+
+def compile_many(graphs, kw=None, simt_items_max=None, workers=None):
+    """Programs for many graphs, compiled in a process pool ("spawn" start method, so it is
+    safe after CUDA is initialised). kw: Program keyword arguments; simt_items_max: when
+    given, a graph whose box-per-thread program needs at most this many doubles per box gets
+    that program, the others Program(graph, **kw). Returns stripped programs in order."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    kw = dict(kw or {})
+    jobs = [(g, kw, simt_items_max) for g in graphs]
+    workers = workers or min(len(jobs), os.cpu_count() or 1)
+    if workers <= 1 or len(jobs) <= 1:
+        return [_compile_job(j) for j in jobs]
+    with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+        return list(ex.map(_compile_job, jobs, chunksize=max(1, len(jobs) // (4 * workers))))

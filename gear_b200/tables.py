@@ -116,6 +116,16 @@ def build():
     return {k: v.numpy().astype(np.float64) for k, v in out.items()}
 
 
+_SIN_CACHE = {}
+
+
+def build_cached():
+    """build(), computed once per process (the tables depend on nothing)."""
+    if "t" not in _SIN_CACHE:
+        _SIN_CACHE["t"] = build()
+    return _SIN_CACHE["t"]
+
+
 SIN_TABLE_ORDER = ("d_lower", "d_upper", "xl_lower_d", "xl_lower_c", "xl_upper_d", "xl_upper_c",
                    "xu_lower_d", "xu_lower_c", "xu_upper_d", "xu_upper_c")
 

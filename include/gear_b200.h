@@ -203,6 +203,50 @@ int gear_crown_lower_static(const gear_dag* dag, const double* x_L, const double
 /* Size in bytes of gear_crown_lower_static's built-in scratch array. */
 int64_t gear_crown_static_scratch_bytes(void);
 
+/* ---------------------------------------------------------------- the plain (unfused) form
+ * The same CROWN bounds as gear_crown_lower, computed the unfused way: one kernel launch per
+ * schedule step, and inside every CROWN pass one launch per op (one node's backward step into
+ * one input) plus one for the pass's initial A and one for its concretisation; every box's
+ * state crosses launches through global memory. It is the baseline the fused launch is measured
+ * against, not a production path. The DAG must be a box-per-CTA program compiled with its pass
+ * working set in global memory (H_PASS_GLOBAL > 0, e.g. Program(..., smem_limit=0)); lA is
+ * required. Workspace: one slot per box. */
+int64_t gear_crown_plain_workspace_bytes(const gear_dag* dag, int64_t batch);
+int gear_crown_lower_plain(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
+                           const double* C, double* lb, double* lA, double* lbias, void* workspace,
+                           int64_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------- many instances, one launch
+ * One instance of a multi-instance CROWN call: the arguments gear_crown_lower takes for one
+ * DAG (same shapes and meaning; batch may be 0). The reference bounds each instance with its own
+ * compute_bounds call (bound_general.py:1275, from bounding.py:317); here the boxes of every
+ * instance go into one persistent launch. */
+typedef struct gear_lower_args {
+  const gear_dag* dag;
+  const double* x_L;
+  const double* x_U;
+  int64_t batch;
+  const double* C;
+  double* lb;
+  double* lA;
+  double* lbias;
+  double* lb_ibp;   /* NULL, or (batch, S): as in gear_crown_lower_ibp (lb = max(CROWN, IBP)) */
+} gear_lower_args;
+
+/* Workspace bytes for gear_crown_lower_multi on these instances (0 when no instance has boxes,
+ * -1 on invalid arguments; the text is in gear_last_error). */
+int64_t gear_crown_multi_workspace_bytes(const gear_lower_args* items, int32_t count);
+
+/* CROWN lower bounds of every instance's boxes in ONE kernel launch: the results of instance i
+ * are those gear_crown_lower gives for it alone (same kernel code per box). Every DAG must have
+ * the same execution mode and threads per CTA and live on the current device. CTAs take work
+ * items (boxes, or tiles of 64 boxes for box-per-thread programs) from a device counter in
+ * the given instance order, so list expensive instances first. The instance table is copied
+ * to the device from pinned memory inside the call; `items` may be reused on return.
+ * Asynchronous on `stream`. */
+int gear_crown_lower_multi(const gear_lower_args* items, int32_t count, void* workspace, int64_t workspace_bytes,
+                           void* stream);
+
 /* Number of kernel launches the last gear_crown_lower on this thread issued. */
 int gear_last_launch_count(void);
 
