@@ -1468,14 +1468,16 @@ __device__ __forceinline__ void cta_box(const DevProgram& P, Box& bx, double* tm
   }
 }
 
-template <int NT>
+// GWS: the program keeps its pass working set in global memory (H_PASS_GLOBAL > 0). A separate
+// instance per address space keeps the shared-memory one on shared loads and stores.
+template <int NT, bool GWS>
 __global__ void __launch_bounds__(NT, GEAR_CTA_MINB / NT) crown_megakernel(DevProgram Pg, Work wk) {
   extern __shared__ double sm[];
   DevProgram P;
   Box bx;
   double *tmp_lo, *tmp_hi, *work;
   int32_t* sops = cta_bind<NT>(P, bx, tmp_lo, tmp_hi, work, Pg, sm, wk.scratch + (size_t)blockIdx.x * wk.slot_doubles);
-  for (int64_t b = blockIdx.x; b < wk.B; b += gridDim.x) cta_box<NT>(P, bx, tmp_lo, tmp_hi, sops, wk, b, work);
+  for (int64_t b = blockIdx.x; b < wk.B; b += gridDim.x) cta_box<NT>(P, bx, tmp_lo, tmp_hi, sops, wk, b, GWS ? work : sm);
 }
 
 // ------------------------------------------------------------------ the plain (unfused) form
@@ -1520,11 +1522,12 @@ __device__ __forceinline__ int multi_owner(const int64_t* start, int count, long
   return lo;
 }
 
-// Boxes of many instances (different programs and widths) in one persistent launch. Work item g
+// Boxes of many instances (different programs and widths) in one persistent launch; every
+// program of one launch keeps its pass working set in the same address space (GWS). Work item g
 // is box g - start[i] of instance i; CTAs take items from a device counter, so instances of
 // uneven cost balance over the SMs (the caller orders them by cost, largest first). A CTA
 // rebinds its shared-memory node table only when the instance changes.
-template <int NT>
+template <int NT, bool GWS>
 __global__ void __launch_bounds__(NT, GEAR_CTA_MINB / NT)
 crown_multi_megakernel(const MultiItem* __restrict__ items, int count, const int64_t* __restrict__ start,
                        unsigned long long* next, double* scratch, int64_t slot_doubles) {
@@ -1553,7 +1556,7 @@ crown_multi_megakernel(const MultiItem* __restrict__ items, int count, const int
       sops = cta_bind<NT>(P, bx, tmp_lo, tmp_hi, work, items[i].P, sm, slot);
       cur = i;
     }
-    cta_box<NT>(P, bx, tmp_lo, tmp_hi, sops, items[i].wk, g - start[i], work);   // Work read in place
+    cta_box<NT>(P, bx, tmp_lo, tmp_hi, sops, items[i].wk, g - start[i], GWS ? work : sm);   // Work read in place
   }
 }
 

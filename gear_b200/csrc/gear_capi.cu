@@ -52,33 +52,42 @@ struct gear_dag {
 };
 
 // box-per-CTA kernel instances: dynamic shared-memory limit and resident CTAs per SM
-template <int NT>
+// (GWS: the program keeps its pass working set in global memory, a kernel instance of its own)
+template <int NT, bool GWS>
 cudaError_t cta_occupancy_t(int smem_bytes, int* bps) {
-  cudaError_t e = cudaFuncSetAttribute(gear::crown_megakernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+  cudaError_t e = cudaFuncSetAttribute(gear::crown_megakernel<NT, GWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       smem_bytes);
   if (e != cudaSuccess) return e;
 #ifdef GEAR_CTA_CARVEOUT
   // shared-memory share of the unified L1 (percent) for builds that fix it
-  e = cudaFuncSetAttribute(gear::crown_megakernel<NT>, cudaFuncAttributePreferredSharedMemoryCarveout, GEAR_CTA_CARVEOUT);
+  e = cudaFuncSetAttribute(gear::crown_megakernel<NT, GWS>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           GEAR_CTA_CARVEOUT);
   if (e != cudaSuccess) return e;
 #endif
 
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, gear::crown_megakernel<NT>, NT, smem_bytes);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, gear::crown_megakernel<NT, GWS>, NT, smem_bytes);
 }
-static cudaError_t cta_occupancy(int threads, int smem_bytes, int* bps) {
+static cudaError_t cta_occupancy(int threads, bool gws, int smem_bytes, int* bps) {
   switch (threads) {
-    case 64: return cta_occupancy_t<64>(smem_bytes, bps);
-    case 128: return cta_occupancy_t<128>(smem_bytes, bps);
-    case 256: return cta_occupancy_t<256>(smem_bytes, bps);
+    case 64: return gws ? cta_occupancy_t<64, true>(smem_bytes, bps) : cta_occupancy_t<64, false>(smem_bytes, bps);
+    case 128: return gws ? cta_occupancy_t<128, true>(smem_bytes, bps) : cta_occupancy_t<128, false>(smem_bytes, bps);
+    case 256: return gws ? cta_occupancy_t<256, true>(smem_bytes, bps) : cta_occupancy_t<256, false>(smem_bytes, bps);
     default: return cudaErrorInvalidValue;
   }
 }
-template <int NT>
+template <int NT, bool GWS>
 cudaError_t cta_launch_t(const gear::DevProgram& P, const gear::Work& wk, int64_t slots, int smem_bytes, cudaStream_t st) {
   // the kernel's dynamic shared-memory limit is per function: set it for this program
-  cudaError_t e = cudaFuncSetAttribute(gear::crown_megakernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+  cudaError_t e = cudaFuncSetAttribute(gear::crown_megakernel<NT, GWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       smem_bytes);
   if (e != cudaSuccess) return e;
-  gear::crown_megakernel<NT><<<(unsigned)slots, NT, smem_bytes, st>>>(P, wk);
+  gear::crown_megakernel<NT, GWS><<<(unsigned)slots, NT, smem_bytes, st>>>(P, wk);
   return cudaGetLastError();
+}
+template <int NT>
+cudaError_t cta_launch_any(const gear::DevProgram& P, const gear::Work& wk, int64_t slots, int smem_bytes, bool gws,
+                           cudaStream_t st) {
+  return gws ? cta_launch_t<NT, true>(P, wk, slots, smem_bytes, st) : cta_launch_t<NT, false>(P, wk, slots, smem_bytes, st);
 }
 
 extern "C" const char* gear_last_error(void) { return g_err.c_str(); }
@@ -158,7 +167,7 @@ extern "C" int gear_dag_create(const int32_t* header, int64_t header_len, const 
       delete d;
       return fail(GEAR_E_INVALID, "gear_dag_create: %s", "pass working set exceeds shared memory");
     }
-    e = cta_occupancy(d->threads, d->smem_bytes, &bps);
+    e = cta_occupancy(d->threads, header[H_PASS_GLOBAL] > 0, d->smem_bytes, &bps);
     if (e == cudaErrorInvalidValue) {
       cudaFree(d->dev);
       delete d;
@@ -199,10 +208,11 @@ static int launch_crown(const gear_dag* dag, const gear::Work& wk, int64_t slots
     return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "crown_simt_kernel launch");
   }
   cudaError_t e = cudaErrorInvalidValue;
+  const bool gws = dag->hdr[gear::H_PASS_GLOBAL] > 0;
   switch (dag->threads) {
-    case 64: e = cta_launch_t<64>(dag->P, wk, slots, dag->smem_bytes, stream); break;
-    case 128: e = cta_launch_t<128>(dag->P, wk, slots, dag->smem_bytes, stream); break;
-    case 256: e = cta_launch_t<256>(dag->P, wk, slots, dag->smem_bytes, stream); break;
+    case 64: e = cta_launch_any<64>(dag->P, wk, slots, dag->smem_bytes, gws, stream); break;
+    case 128: e = cta_launch_any<128>(dag->P, wk, slots, dag->smem_bytes, gws, stream); break;
+    case 256: e = cta_launch_any<256>(dag->P, wk, slots, dag->smem_bytes, gws, stream); break;
     default: break;
   }
   g_launches = 1;
@@ -416,16 +426,27 @@ extern "C" int gear_crown_lower_plain(const gear_dag* dag, const double* x_L, co
 
 // ------------------------------------------------------------------ many instances, one launch
 namespace {
-template <int NT>
+template <int NT, bool GWS>
 cudaError_t multi_cta_occupancy_t(int smem_bytes, int* bps) {
-  cudaError_t e = cudaFuncSetAttribute(gear::crown_multi_megakernel<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       smem_bytes);
+  cudaError_t e = cudaFuncSetAttribute(gear::crown_multi_megakernel<NT, GWS>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, gear::crown_multi_megakernel<NT>, NT, smem_bytes);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, gear::crown_multi_megakernel<NT, GWS>, NT, smem_bytes);
+}
+template <int NT>
+cudaError_t multi_cta_occupancy(bool gws, int smem_bytes, int* bps) {
+  return gws ? multi_cta_occupancy_t<NT, true>(smem_bytes, bps) : multi_cta_occupancy_t<NT, false>(smem_bytes, bps);
+}
+template <int NT>
+void multi_cta_launch(bool gws, unsigned grid, int smem, cudaStream_t st, const gear::MultiItem* items, int count,
+                      const int64_t* start, unsigned long long* next, double* scratch, int64_t slot_doubles) {
+  if (gws) gear::crown_multi_megakernel<NT, true><<<grid, NT, smem, st>>>(items, count, start, next, scratch, slot_doubles);
+  else gear::crown_multi_megakernel<NT, false><<<grid, NT, smem, st>>>(items, count, start, next, scratch, slot_doubles);
 }
 
 struct MultiPlan {
   int mode = 0, threads = 0, smem = 0, device = 0, count = 0;   // count: instances with boxes
+  bool gws = false;           // box-per-CTA programs with their pass working set in global memory
   int64_t total = 0;          // work items: boxes (box per CTA) or tiles of SIMT_T boxes
   int64_t slot_doubles = 0;   // the largest program's slot
   int64_t slots = 1;          // CTAs of the launch
@@ -447,15 +468,18 @@ int multi_plan(const gear_lower_args* a, int32_t count, MultiPlan& pl) {
       return fail(GEAR_E_INVALID, "gear_crown_lower_multi: %s", "program built without A");
     if (d->hdr[gear::H_RETA] != 0 && d->hdr[gear::H_X_IN_LA] != 0 && !a[i].lA && a[i].batch > 0)
       return fail(GEAR_E_INVALID, "gear_crown_lower_multi: %s", "this program accumulates A in the lA output: lA is required");
+    const bool gws = d->mode == gear::MODE_CTA && d->hdr[gear::H_PASS_GLOBAL] > 0;
     if (first) {
       pl.mode = d->mode;
       pl.threads = d->threads;
       pl.device = d->device;
+      pl.gws = gws;
       num_sms = d->num_sms;
       first = false;
-    } else if (d->mode != pl.mode || d->threads != pl.threads || d->device != pl.device) {
+    } else if (d->mode != pl.mode || d->threads != pl.threads || d->device != pl.device || gws != pl.gws) {
       return fail(GEAR_E_INVALID, "gear_crown_lower_multi: %s",
-                  "every program of one launch needs the same execution mode, threads per CTA and device");
+                  "every program of one launch needs the same execution mode, threads per CTA, pass working-set "
+                  "placement and device");
     }
     if (a[i].batch == 0) continue;
     ++pl.count;
@@ -470,9 +494,9 @@ int multi_plan(const gear_lower_args* a, int32_t count, MultiPlan& pl) {
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, gear::crown_multi_simt_kernel, gear::SIMT_T, 0);
   } else {
     switch (pl.threads) {
-      case 64: e = multi_cta_occupancy_t<64>(pl.smem, &bps); break;
-      case 128: e = multi_cta_occupancy_t<128>(pl.smem, &bps); break;
-      case 256: e = multi_cta_occupancy_t<256>(pl.smem, &bps); break;
+      case 64: e = multi_cta_occupancy<64>(pl.gws, pl.smem, &bps); break;
+      case 128: e = multi_cta_occupancy<128>(pl.gws, pl.smem, &bps); break;
+      case 256: e = multi_cta_occupancy<256>(pl.gws, pl.smem, &bps); break;
       default: return fail(GEAR_E_INVALID, "gear_crown_lower_multi: %s", "threads per CTA must be 64, 128 or 256");
     }
   }
@@ -573,18 +597,9 @@ extern "C" int gear_crown_lower_multi(const gear_lower_args* items, int32_t coun
                                                                   pl.slot_doubles);
   } else {
     switch (pl.threads) {
-      case 64:
-        gear::crown_multi_megakernel<64><<<grid, 64, pl.smem, st>>>(ditems, pl.count, dstart, next, scratch,
-                                                                    pl.slot_doubles);
-        break;
-      case 128:
-        gear::crown_multi_megakernel<128><<<grid, 128, pl.smem, st>>>(ditems, pl.count, dstart, next, scratch,
-                                                                      pl.slot_doubles);
-        break;
-      default:
-        gear::crown_multi_megakernel<256><<<grid, 256, pl.smem, st>>>(ditems, pl.count, dstart, next, scratch,
-                                                                      pl.slot_doubles);
-        break;
+      case 64: multi_cta_launch<64>(pl.gws, grid, pl.smem, st, ditems, pl.count, dstart, next, scratch, pl.slot_doubles); break;
+      case 128: multi_cta_launch<128>(pl.gws, grid, pl.smem, st, ditems, pl.count, dstart, next, scratch, pl.slot_doubles); break;
+      default: multi_cta_launch<256>(pl.gws, grid, pl.smem, st, ditems, pl.count, dstart, next, scratch, pl.slot_doubles); break;
     }
   }
   g_launches = 1;

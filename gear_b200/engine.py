@@ -253,7 +253,8 @@ class MultiEngine:
                 if prog is None:
                     prog = Program(g, mode=var[0], cta_threads=var[1] if var[0] == "cta" else 128)
             self.dags.append(_Dag.from_program(prog))
-            self.variants.append(var)
+            # a launch also needs one pass working-set placement (shared or global memory)
+            self.variants.append((var[0], var[1], bool(getattr(prog, "pass_global", 0))))
         self.n = [d.prog.n for d in self.dags]
         self.S = [d.prog.S for d in self.dags]
         cost = [d.prog.alg_bytes_per_box() for d in self.dags]
@@ -263,8 +264,13 @@ class MultiEngine:
         self._ws = {}
         self.group_events = None
 
+    @staticmethod
+    def _name(key):
+        m, t, gws = key
+        return (f"cta{t}" + ("-global" if gws else "")) if m == "cta" else "simt"
+
     def group_names(self):
-        return {(f"cta{t}" if m == "cta" else "simt"): len(ix) for (m, t), ix in self.groups.items()}
+        return {self._name(k): len(ix) for k, ix in self.groups.items()}
 
     def outputs(self, batches, device):
         """Result tensors for these batch sizes: views into three flat buffers."""
@@ -338,8 +344,7 @@ class MultiEngine:
     def group_ms(self):
         """Device time of each group's launch in the last lower() (after record_groups())."""
         torch.cuda.synchronize()
-        return {(f"cta{t}" if m == "cta" else "simt"): e[0].elapsed_time(e[1])
-                for (m, t), e in (self.group_events or {}).items()}
+        return {self._name(k): e[0].elapsed_time(e[1]) for k, e in (self.group_events or {}).items()}
 
     def record_groups(self, on: bool = True):
         self.group_events = {} if on else None
