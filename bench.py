@@ -214,7 +214,7 @@ def mixed_setup(instances=512, workers=None):
     insts = [problems.mixed_instance(k) for k in range(instances)]
     graphs = [graph.trace(m, torch.zeros(2, m.n, dtype=torch.float64)) for m in insts]
     me = MultiEngine(graphs, programs=compile_many(graphs, kw=dict(mode="cta", cta_threads=256),
-                                                   simt_items_max=8192, workers=workers))
+                                                   simt_items_max=32768, workers=workers))
     return insts, graphs, me, time.perf_counter() - t0
 
 
