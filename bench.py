@@ -331,6 +331,62 @@ def mixed_bab(dev, setup, batch=256, rel_gap=1e-4, time_limit=60.0):
             "timing": "wall clock from the first iteration, host loop included"}
 
 
+def serve(dev, seconds=10.0, rate=50.0, budget=30.0, batch=2048, rel_gap=1e-4, seed=0, round_bytes=16 << 20,
+          max_live=96):
+    """The serving loop under Poisson arrivals (rate per second for `seconds`): instances of the
+    quad-exp family with n log-uniform in [5, 2000] (two bilinear constraints), each to the
+    relative gap or its time budget (from arrival). Continuous batching (Server): requests are
+    admitted as memory allows and join the running rounds. Time to gap = finish - arrival."""
+    import math as _m
+    import torch
+    from gear_b200 import problems
+    from gear_b200.serve import Server
+    g = torch.Generator().manual_seed(5000 + seed)
+    t, arrivals = 0.0, []
+    while True:
+        t += float(-_m.log(1.0 - float(torch.rand(1, generator=g))) / rate)
+        if t > seconds:
+            break
+        arrivals.append(t)
+    ns = [int(round(_m.exp(_m.log(5) + (_m.log(2000) - _m.log(5)) * float(torch.rand(1, generator=g)))))
+          for _ in arrivals]
+    srv = Server(device=str(dev), batch=batch, rel_gap=rel_gap, time_budget=budget, round_bytes=round_bytes,
+                 max_live=max_live)
+    t0 = time.perf_counter()
+    clock = lambda: time.perf_counter() - t0
+    srv.clock = clock
+    k = 0
+    while k < len(arrivals) or not srv.idle():
+        now = clock()
+        while k < len(arrivals) and arrivals[k] <= now:
+            m = problems.QuadExpN10(n=ns[k], seed=5000 + k)
+            srv.submit(k, m, torch.full((1, ns[k]), -2.0, dtype=torch.float64),
+                       torch.full((1, ns[k]), 2.0, dtype=torch.float64), arrival=arrivals[k])
+            k += 1
+        if srv.idle():
+            time.sleep(max(0.0, min(0.01, arrivals[k] - now)) if k < len(arrivals) else 0.0)
+            continue
+        srv.step()
+    torch.cuda.synchronize(dev)
+    wall = clock()
+    done = list(srv.done.values())
+    ttg = sorted(r.finished - r.arrival for r in done if r.status == "closed")
+    tis = sorted(r.finished - r.arrival for r in done)
+    q = lambda v, p: v[min(len(v) - 1, int(round(p * (len(v) - 1))))] if v else None
+    return {"workload": "quad-exp family, n log-uniform [5, 2000], m = 2", "arrival_rate_per_s": rate,
+            "arrival_seconds": seconds, "requests": len(arrivals), "closed": len(ttg),
+            "budget_reached": sum(1 for r in done if r.status == "budget"),
+            "emptied": sum(1 for r in done if r.status == "emptied"),
+            "time_to_gap_s": {"p50": q(ttg, 0.5), "p99": q(ttg, 0.99)},
+            "time_in_system_s": {"p50": q(tis, 0.5), "p99": q(tis, 0.99)},
+            "subdomains_per_s": srv.bounded / wall, "rounds": srv.rounds, "max_concurrent": srv.max_live,
+            "rel_gap": rel_gap, "budget_s": budget, "batch_per_instance_max": batch, "round_bytes": round_bytes,
+            "max_live": max_live, "waited_out": sum(1 for r in done if r.admitted is None),
+            "closed_n_max": max((r.lo.shape[1] for r in done if r.status == "closed"), default=None),
+            "host_s": {"rounds": srv.t_round, "crown_launch_calls": srv.t_bound}, "wall_s": wall,
+            "timing": "wall clock; time to gap from each request's arrival to the round that closed it"}
+
+
 def plain_gpu(dev, workload, lo, hi, fused_value, steps=3, warmup=1):
     """The plain GPU form on the headline workload (PlainEngine: one launch per schedule step
     and per op, box state through global memory), the same boxes: subdomains/s and the fused
@@ -381,6 +437,8 @@ def main():
     ap.add_argument("--mixed-boxes", type=int, default=256, help="sub-boxes per mixed-family instance")
     ap.add_argument("--mixed-bab-seconds", type=float, default=60.0,
                     help="time limit of branch and bound on the uneven batch (all instances at once); 0 skips it")
+    ap.add_argument("--serve-seconds", type=float, default=10.0,
+                    help="run the serving loop under Poisson arrivals (50 per second) for this long; 0 skips it")
     ap.add_argument("--no-plain", dest="plain", action="store_false",
                     help="skip the plain GPU form (one launch per step and per op) on the workload")
     ap.add_argument("--workload", default=WORKLOAD, help="benchmark workload (profiling of other shapes)")
@@ -520,6 +578,8 @@ def main():
             res["mixed"] = mixed_batch(dev, setup, args.mixed_boxes)
             if args.mixed_bab_seconds > 0:
                 res["mixed_bab"] = mixed_bab(dev, setup, time_limit=args.mixed_bab_seconds)
+        if args.serve_seconds > 0:
+            res["serve"] = serve(dev, seconds=args.serve_seconds)
         if world == 1 and not args.no_cpu_baseline:
             try:
                 res["cpu_baseline"] = cpu_baseline(per_core=args.cpu_per_core, workload=args.workload)

@@ -389,6 +389,48 @@ class BaB:
         return self.incumbent, self.dual_bound(), self.gap()
 
 
+def bab_round(babs, bound, ibp_enhancement=True):
+    """One branch-and-bound iteration over several instances: select on each, the incumbent
+    candidates of all of them in one host read, one bound(popped, lb_ibp) call for all batches
+    (it returns {key: (lb, lA, lbias)}), prune and branch on each, all survivor counts in one
+    host read, then split and push on each. babs: {key: BaB}. Returns the domains bounded."""
+    popped = {k: b.select() for k, b in babs.items() if len(b.queue)}
+    if not popped:
+        return 0
+    cands = {k: babs[k].incumbent_candidate((p[0] + p[1]) / 2) for k, p in popped.items()}
+    keys = [k for k, c in cands.items() if c is not None]
+    if keys:
+        vals = torch.cat([cands[k][0] for k in keys]).tolist()            # one host read
+        for k, v in zip(keys, vals):
+            babs[k].accept_incumbent(v, cands[k][1])
+    ibp = {k: torch.empty(p[0].shape[0], babs[k].S, dtype=torch.float64, device=p[0].device)
+           for k, p in popped.items()} if ibp_enhancement else {}
+    outs = bound(popped, ibp)
+    sts = {k: babs[k].prune_branch(popped[k], *outs[k]) for k in popped}
+    Ks = torch.cat([sts[k]["nk"] for k in sts]).tolist()                  # one host read
+    for k, K in zip(sts, Ks):
+        babs[k].finish(sts[k], int(K))
+    return sum(p[0].shape[0] for p in popped.values())
+
+
+def relative_gaps(babs):
+    """{key: relative gap} of several BaB instances in one host read."""
+    keys = list(babs)
+    if not keys:
+        return {}
+    D = torch.cat([torch.minimum(babs[k].queue.min_key_tensor(), babs[k].disc_min) for k in keys]).tolist()
+    out = {}
+    for k, d in zip(keys, D):
+        P = babs[k].incumbent
+        if not math.isfinite(P):
+            out[k] = math.inf
+        elif not math.isfinite(d):
+            out[k] = 0.0 if d > 0 else math.inf
+        else:
+            out[k] = (P - d) / max(1.0, abs(P), abs(d))
+    return out
+
+
 class _Shape:
     """Stands in for a CrownEngine where only the widths are needed (the bounds come from a
     shared MultiEngine)."""
@@ -428,49 +470,28 @@ class MultiBaB:
     def step(self, active):
         """One iteration over the instances in `active`; returns the number of domains bounded."""
         dev = self.device
-        popped = {i: self.babs[i].select() for i in active if len(self.babs[i].queue)}
-        cands = {i: self.babs[i].incumbent_candidate((p[0] + p[1]) / 2) for i, p in popped.items()}
-        keys = [i for i, c in cands.items() if c is not None]
-        if keys:
-            vals = torch.cat([cands[i][0] for i in keys]).tolist()        # one host read
-            for i, v in zip(keys, vals):
-                self.babs[i].accept_incumbent(v, cands[i][1])
-        boxes, ibp = [], []
-        for i, b in enumerate(self.babs):
-            if i in popped:
-                boxes.append((popped[i][0], popped[i][1]))
-                ibp.append(torch.empty(popped[i][0].shape[0], b.S, dtype=torch.float64, device=dev)
-                           if self.ibp_enhancement else None)
-            else:
-                e = torch.empty(0, b.n, dtype=torch.float64, device=dev)
-                boxes.append((e, e))
-                ibp.append(None)
-        outs = self.engine.lower(boxes, lb_ibp=ibp)
-        sts = {i: self.babs[i].prune_branch(popped[i], *outs[i]) for i in popped}
-        if sts:
-            Ks = torch.cat([sts[i]["nk"] for i in sts]).tolist()          # one host read
-            for i, k in zip(sts, Ks):
-                self.babs[i].finish(sts[i], int(k))
-        B = sum(p[0].shape[0] for p in popped.values())
+
+        def bound(popped, ibp):
+            boxes, ibps = [], []
+            for i, b in enumerate(self.babs):
+                if i in popped:
+                    boxes.append((popped[i][0], popped[i][1]))
+                    ibps.append(ibp.get(i))
+                else:
+                    e = torch.empty(0, b.n, dtype=torch.float64, device=dev)
+                    boxes.append((e, e))
+                    ibps.append(None)
+            outs = self.engine.lower(boxes, lb_ibp=ibps)
+            return {i: outs[i] for i in popped}
+        B = bab_round({i: self.babs[i] for i in active}, bound, self.ibp_enhancement)
         self.iterations += 1
         self.bounded += B
         return B
 
     def gaps(self, idx):
         """Relative gaps of the instances in idx (one host read)."""
-        if not idx:
-            return []
-        D = torch.cat([torch.minimum(self.babs[i].queue.min_key_tensor(), self.babs[i].disc_min) for i in idx]).tolist()
-        out = []
-        for i, d in zip(idx, D):
-            P = self.babs[i].incumbent
-            if not math.isfinite(P):
-                out.append(math.inf)
-            elif not math.isfinite(d):
-                out.append(0.0 if d > 0 else math.inf)
-            else:
-                out.append((P - d) / max(1.0, abs(P), abs(d)))
-        return out
+        g = relative_gaps({i: self.babs[i] for i in idx})
+        return [g[i] for i in idx]
 
     def run(self, rel_gap: float = 1e-4, time_limit: float = 60.0, max_iterations: int = 10000):
         """Iterate until every instance reaches the gap (or empties its queue), or a limit.

@@ -17,6 +17,9 @@ VARIANTS = (("simt", 128), ("cta", 64), ("cta", 128), ("cta", 256))
 # the box-per-thread kernel keeps every per-box array in global memory: beyond this many
 # doubles per box it streams too much to compete, and "auto" does not try it
 SIMT_MAX_ITEMS = 65536
+# many-instance launches: an instance whose box-per-thread state is at most this many doubles
+# joins the box-per-thread group (measured fastest on the mixed family among 2048 ... 65536)
+SIMT_PACK_ITEMS = 32768
 
 
 class _Dag:
@@ -228,7 +231,7 @@ class MultiEngine:
     stream before lower() returns; off by default: two persistent launches that each size
     their grid for the whole GPU compete for it (measured 11% slower on the mixed family)."""
 
-    def __init__(self, graphs, mode: str = "auto", cta_threads: int = 256, simt_items_max: int = 32768,
+    def __init__(self, graphs, mode: str = "auto", cta_threads: int = 256, simt_items_max: int = SIMT_PACK_ITEMS,
                  programs=None, concurrent: bool = False):
         if not torch.cuda.is_available():
             raise _lib.GearError("gear_b200 needs a CUDA device (no CPU fallback)")
