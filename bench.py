@@ -218,7 +218,7 @@ def mixed_setup(instances=512, workers=None):
     return insts, graphs, me, time.perf_counter() - t0
 
 
-def mixed_batch(dev, setup, boxes=256, steps=2, warmup=1, plain=True):
+def mixed_batch(dev, setup, boxes=256, steps=2, warmup=1, baselines=True):
     """The uneven batch: instances 0..instances-1 of the mixed family (n log-uniform in [5, 500],
     depth 3-12, m = n // 4), `boxes` sub-boxes each. Certified subdomain bounds per second
     (device time, CUDA events) of (a) every instance in one persistent launch per kernel variant
@@ -252,6 +252,12 @@ def mixed_batch(dev, setup, boxes=256, steps=2, warmup=1, plain=True):
     me.lower(bx, out=outs)
     group_ms = me.group_ms()
     me.record_groups(False)
+    res = {"workload": "mixed family (n log-uniform [5, 500], depth 3-12, m = n // 4)", "instances": instances,
+           "boxes_per_instance": boxes, "groups": me.group_names(), "group_ms": group_ms,
+           "launches_per_call": me.launches(), "packed_ms": packed_ms,
+           "packed_subdomains_per_s": total / (packed_ms / 1000.0), "compile_s": compile_s}
+    if not baselines:
+        return res
     # one launch per instance through gear_crown_lower, same programs
     L = _lib.lib()
     ws_bytes = max(int(L.gear_crown_workspace_bytes(d.handle, boxes)) for d in me.dags)
@@ -268,13 +274,9 @@ def mixed_batch(dev, setup, boxes=256, steps=2, warmup=1, plain=True):
     alone_ms = timed(alone_step, steps, warmup)
     same = all(torch.equal(a[0], b[0]) and torch.equal(a[1], b[1]) for a, b in zip(outs, alone))
     del ws
-    res = {"workload": "mixed family (n log-uniform [5, 500], depth 3-12, m = n // 4)", "instances": instances,
-           "boxes_per_instance": boxes, "groups": me.group_names(), "group_ms": group_ms,
-           "launches_per_call": me.launches(),
-           "packed_ms": packed_ms, "packed_subdomains_per_s": total / (packed_ms / 1000.0),
-           "alone_ms": alone_ms, "alone_subdomains_per_s": total / (alone_ms / 1000.0),
-           "packed_vs_alone": alone_ms / packed_ms, "bitwise_equal_alone": same}
-    if plain:
+    res.update({"alone_ms": alone_ms, "alone_subdomains_per_s": total / (alone_ms / 1000.0),
+                "packed_vs_alone": alone_ms / packed_ms, "bitwise_equal_alone": same})
+    if baselines:
         t1 = time.perf_counter()
         pprogs = compile_many(graphs, kw=dict(mode="cta", cta_threads=128, smem_limit=0))
         pdags = [_Dag.from_program(p) for p in pprogs]
@@ -435,6 +437,8 @@ def main():
                     help="also bound the uneven batch of this many mixed-family instances in one launch per "
                          "kernel variant against one launch per instance; 0 skips it")
     ap.add_argument("--mixed-boxes", type=int, default=256, help="sub-boxes per mixed-family instance")
+    ap.add_argument("--no-mixed-baselines", dest="mixed_baselines", action="store_false",
+                    help="time only the packed launch of the uneven batch (no per-instance or plain-form runs)")
     ap.add_argument("--mixed-bab-seconds", type=float, default=60.0,
                     help="time limit of branch and bound on the uneven batch (all instances at once); 0 skips it")
     ap.add_argument("--serve-seconds", type=float, default=10.0,
@@ -575,7 +579,7 @@ def main():
             res["bab"] = bab_to_gap(args.bab_instances, dev)
         if args.mixed_instances > 0:
             setup = mixed_setup(args.mixed_instances)
-            res["mixed"] = mixed_batch(dev, setup, args.mixed_boxes)
+            res["mixed"] = mixed_batch(dev, setup, args.mixed_boxes, baselines=args.mixed_baselines)
             if args.mixed_bab_seconds > 0:
                 res["mixed_bab"] = mixed_bab(dev, setup, time_limit=args.mixed_bab_seconds)
         if args.serve_seconds > 0:

@@ -677,6 +677,11 @@ __device__ void ibp_node(const Box& bx, int v, double* olo, double* ohi) {
 // fold vectors of a linear/matmul on the input: W x0, |W| eps, |W| max(|xL|, |xU|). The box's
 // centre, radius and magnitude are staged in shared memory (`stage`, 3 win doubles); each thread
 // owns outputs j and reads column j of the transposed weights (coalesced across the threads).
+#ifndef GEAR_FOLD_UNROLL
+#define GEAR_FOLD_UNROLL 16
+#endif
+constexpr int FOLD_UNROLL = GEAR_FOLD_UNROLL;
+
 template <int NT>
 __device__ void fold_node(const Box& bx, int v, double* stage) {
   const DevProgram* P = bx.P;
@@ -698,12 +703,14 @@ __device__ void fold_node(const Box& bx, int v, double* stage) {
     const double* col = Wt + j;
     double c = 0, r = 0, t = 0;
     int i = 0;
-    for (; i + 4 <= win; i += 4) {
-      double wv[4];
+    // FOLD_UNROLL weight loads in flight per thread (one L2 round trip per FOLD_UNROLL inputs;
+    // 16 measured fastest of 4, 8, 16, 32 on dense_q_n200)
+    for (; i + FOLD_UNROLL <= win; i += FOLD_UNROLL) {
+      double wv[FOLD_UNROLL];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) wv[q] = __ldg(col + (int64_t)(i + q) * w);
+      for (int q = 0; q < FOLD_UNROLL; ++q) wv[q] = __ldg(col + (int64_t)(i + q) * w);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < FOLD_UNROLL; ++q) {
         const double aw = fabs(wv[q]);
         c += xc[i + q] * wv[q];
         r += xr[i + q] * aw;
@@ -858,6 +865,7 @@ __device__ __forceinline__ void gemv_row(const double* V, const int32_t* vcols, 
       bool ok[JB];
 #pragma unroll
       for (int q = 0; q < JB; ++q) { acc[q] = 0.0; ab[q] = 0.0; ok[q] = jb + q * estep < win; }
+
       // entries in chunks of EB: their indices and coefficients first, then EB x JB weight
       // loads in flight together, then the sums (in entry order)
       for (int e = e0; e < e1; e += EB) {
@@ -1228,13 +1236,14 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
         double bs = 0, dv = 0, be = 0;
         constexpr int XB = 8;
         // XB entries per step: index, coefficient and box loads issued before the sums
+        const bool full = e1 - e0 == n;       // a full row: entry e is column e - e0
         for (int e = e0 + rs.eoff; e < e1; e += XB * rs.estep) {
           int cq[XB];
           bool ok[XB];
 #pragma unroll
           for (int q = 0; q < XB; ++q) {
             ok[q] = e + q * rs.estep < e1;
-            cq[q] = ok[q] ? __ldg(xcols + e + q * rs.estep) : 0;
+            cq[q] = ok[q] ? (full ? e + q * rs.estep - e0 : __ldg(xcols + e + q * rs.estep)) : 0;
           }
           double aq[XB], lq[XB], hq[XB];
 #pragma unroll
