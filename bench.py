@@ -213,8 +213,10 @@ def mixed_setup(instances=512, workers=None):
     t0 = time.perf_counter()
     insts = [problems.mixed_instance(k) for k in range(instances)]
     graphs = [graph.trace(m, torch.zeros(2, m.n, dtype=torch.float64)) for m in insts]
-    me = MultiEngine(graphs, programs=compile_many(graphs, kw=dict(mode="cta", cta_threads=256),
-                                                   simt_items_max=32768, workers=workers))
+    from gear_b200.engine import PACK_SMEM_LIMIT, SIMT_PACK_ITEMS
+    me = MultiEngine(graphs, programs=compile_many(graphs, kw=dict(mode="cta", cta_threads=256,
+                                                                   smem_limit=PACK_SMEM_LIMIT),
+                                                   simt_items_max=SIMT_PACK_ITEMS, workers=workers))
     return insts, graphs, me, time.perf_counter() - t0
 
 

@@ -18,8 +18,23 @@ VARIANTS = (("simt", 128), ("cta", 64), ("cta", 128), ("cta", 256))
 # doubles per box it streams too much to compete, and "auto" does not try it
 SIMT_MAX_ITEMS = 65536
 # many-instance launches: an instance whose box-per-thread state is at most this many doubles
-# joins the box-per-thread group (measured fastest on the mixed family among 2048 ... 65536)
-SIMT_PACK_ITEMS = 32768
+# joins the box-per-thread group, and a box-per-CTA program whose pass working set exceeds
+# PACK_SMEM_LIMIT bytes keeps it in global memory (more CTAs per SM); measured fastest on the
+# mixed family over thresholds 2048-65536 and limits 16 KB-227 KB
+SIMT_PACK_ITEMS = 8192
+PACK_SMEM_LIMIT = 48 << 10
+# a many-instance launch gives every CTA the largest shared-memory size of its programs, so
+# box-per-CTA programs launch in size classes (upper bounds in bytes; 6 / 3 / 2 / 1 CTAs of
+# that size fit an SM's 228 KB)
+SMEM_CLASSES = (32 << 10, 72 << 10, 108 << 10, 232448)
+
+
+def smem_class(prog) -> int:
+    """Size class of a box-per-CTA program's dynamic shared memory (0 for other programs)."""
+    if prog.mode != "cta":
+        return 0
+    b = 8 * int(prog.smem_total)
+    return next((i for i, c in enumerate(SMEM_CLASSES) if b <= c), len(SMEM_CLASSES))
 
 
 class _Dag:
@@ -257,10 +272,12 @@ class MultiEngine:
                 else:
                     prog = None
                 if prog is None:
-                    prog = Program(g, mode=var[0], cta_threads=var[1] if var[0] == "cta" else 128)
+                    prog = Program(g, mode=var[0], cta_threads=var[1] if var[0] == "cta" else 128,
+                                   smem_limit=PACK_SMEM_LIMIT)
             self.dags.append(_Dag.from_program(prog))
-            # a launch also needs one pass working-set placement (shared or global memory)
-            self.variants.append((var[0], var[1], bool(getattr(prog, "pass_global", 0))))
+            # a launch also needs one pass working-set placement (shared or global memory); the
+            # fourth field is the shared-memory size class
+            self.variants.append((var[0], var[1], bool(getattr(prog, "pass_global", 0)), smem_class(prog)))
         self.n = [d.prog.n for d in self.dags]
         self.S = [d.prog.S for d in self.dags]
         cost = [d.prog.alg_bytes_per_box() for d in self.dags]
@@ -274,8 +291,8 @@ class MultiEngine:
 
     @staticmethod
     def _name(key):
-        m, t, gws = key
-        return (f"cta{t}" + ("-global" if gws else "")) if m == "cta" else "simt"
+        m, t, gws, sc = key
+        return (f"cta{t}" + ("-global" if gws else f"-smem{sc}")) if m == "cta" else "simt"
 
     def group_names(self):
         return {self._name(k): len(ix) for k, ix in self.groups.items()}

@@ -24,7 +24,7 @@ import torch
 
 from . import _lib, graph as _graph
 from .bab import BaB, _Shape, bab_round, relative_gaps
-from .engine import SIMT_PACK_ITEMS, _Dag
+from .engine import PACK_SMEM_LIMIT, SIMT_PACK_ITEMS, _Dag, smem_class
 from .program import Program, simt_items
 
 
@@ -44,7 +44,7 @@ class Request:
     rounds: int = 0
     bounded: int = 0
     status: str = "waiting"            # waiting, running, closed, emptied, budget
-    group: tuple = ()                  # kernel group it ran in: (mode, threads, global working set)
+    group: tuple = ()                  # kernel group: (mode, threads, global working set, smem class)
 
 
 @dataclass
@@ -131,10 +131,10 @@ class Server:
                 continue
             g = r.graph
             prog = Program(g, mode="simt")
-            group = ("simt", 0, False)
+            group = ("simt", 0, False, 0)
             if simt_items(prog) > self.simt_items_max:
-                prog = Program(g, mode="cta", cta_threads=self.cta_threads)
-                group = ("cta", self.cta_threads, prog.pass_global > 0)
+                prog = Program(g, mode="cta", cta_threads=self.cta_threads, smem_limit=PACK_SMEM_LIMIT)
+                group = ("cta", self.cta_threads, prog.pass_global > 0, smem_class(prog))
             est = self._estimate(prog.n, prog.S, prog)
             if torch.cuda.memory_allocated(self.device) + est > self.hbm_budget:
                 still.append(r)                      # no room yet: admitted when memory frees up

@@ -41,7 +41,7 @@ def test_serve_same_alone_and_in_mix():
         r = srv.done[k]
         assert r.status in ("closed", "emptied", "budget") and r.rounds > 0
         m, lo, hi = _req(k, n)
-        mode, threads, _ = r.group
+        mode, threads = r.group[:2]
         g = r.graph
         eng = CrownEngine(g, mode=mode, cta_threads=threads or 128)
         bb = BaB(g, lo, hi, batch=64, engine=eng, model=m.cuda())
