@@ -153,7 +153,7 @@ class BaB:
                  engine_mode: str = "auto", cta_threads: int = 128,
                  sb_min_width_ratio: float = 1e-3, model: Optional[torch.nn.Module] = None,
                  constrained: bool = False, max_constraint_rows: int = 16, clip: bool = False,
-                 clip_iterations: int = 1, ibp_enhancement: bool = True):
+                 clip_iterations: int = 1, ibp_enhancement: bool = True, incumbent_every: int = 1):
         """constrained: the reference's complete clipping mode's constrained concretisation
         (batch_branch_and_bound.py:422-428): every child keeps its parent's planes
         lA_j x + lbias_j <= thr_j as cut rows, and the objective row of its CROWN bound is
@@ -164,7 +164,9 @@ class BaB:
         clip_iterations rounds); children that become empty are dropped.
         ibp_enhancement: every bound is the larger of CROWN's and the plain IBP bound of the
         output (get_lower_bound_with_ibp_enhancement, bounding.py:789-948, on by default in the
-        reference)."""
+        reference).
+        incumbent_every: evaluate the model at the popped boxes' midpoints (the primal points of
+        the incumbent) on every k-th iteration only; 1 = every iteration."""
         self.device = torch.device(device)
         self.graph = graph
         # an engine can be shared between runs on the same graph (its kernel choice is kept)
@@ -189,6 +191,8 @@ class BaB:
         self.rhs = (torch.zeros(self.S - 1, dtype=torch.float64) if rhs is None else rhs.to(torch.float64)).to(self.device)
         self.incumbent = math.inf
         self.x_best = None
+        self.incumbent_every = max(1, int(incumbent_every))
+        self._bufs = {}
         self.ibp_enhancement = ibp_enhancement
         self.clip = clip
         self.clip_iterations = clip_iterations
@@ -214,10 +218,19 @@ class BaB:
             self._ws = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
         return self._ws
 
+    def _buf(self, name, n, dtype):
+        """A flat scratch tensor of at least n elements kept across iterations (every use ends
+        within the iteration that takes it; the stream orders the next one after it)."""
+        t = self._bufs.get(name)
+        if t is None or t.numel() < n or t.dtype != dtype:
+            t = self._bufs[name] = torch.empty(max(n, 1), dtype=dtype, device=self.device)
+        return t[:n]
+
     def incumbent_candidate(self, x: torch.Tensor):
         """Best feasible objective among the primal points x (model in float64), on the device:
-        (value (1,) tensor, +inf if none, and its point), without a host read."""
-        if self.model is None or x.numel() == 0:
+        (value (1,) tensor, +inf if none, and its point), without a host read. With
+        incumbent_every = k only every k-th iteration evaluates (None otherwise)."""
+        if self.model is None or x.numel() == 0 or self.stats.iterations % self.incumbent_every:
             return None
         with torch.no_grad():
             y = self.model(x.to(self.device, torch.float64))
@@ -266,13 +279,13 @@ class BaB:
         B = lo.shape[0]
         L = _lib.lib()
         stream = torch.cuda.current_stream(self.device).cuda_stream
-        keep = torch.empty(B, dtype=torch.uint8, device=self.device)
-        kept = torch.empty(B, dtype=torch.int32, device=self.device)
-        nk = torch.zeros(1, dtype=torch.int32, device=self.device)
+        keep = self._buf("keep", B, torch.uint8)
+        kept = self._buf("kept", B, torch.int32)
+        nk = self._buf("nk", 1, torch.int32)              # written by the prune (0 first)
         ws = self._ws_bytes(int(L.gear_bab_workspace_bytes(B)))
         _lib.check(L.gear_bab_prune(_p(lb), _p(thr), B, self.S, _p(keep), _p(kept), _p(nk), _p(self.disc_min),
                                     _p(ws), ws.numel(), stream), "gear_bab_prune")
-        split_idx = torch.empty(B, dtype=torch.int32, device=self.device)
+        split_idx = self._buf("split", B, torch.int32)
         _lib.check(L.gear_bab_branch(_p(lA), _p(lo), _p(hi), _p(lb), _p(thr), B, self.S, self.n,
                                      _p(self.root_width), self.coeff_thresh, self.min_width_ratio, _p(split_idx),
                                      _p(ws), ws.numel(), stream), "gear_bab_branch")
@@ -290,9 +303,9 @@ class BaB:
         self.stats.bounded += B
         self.stats.pruned += B - K
         if K > 0:
-            clo = torch.empty(2 * K, self.n, dtype=torch.float64, device=self.device)
-            chi = torch.empty_like(clo)
-            ckey = torch.empty(2 * K, self.S, dtype=torch.float64, device=self.device)
+            clo = self._buf("clo", 2 * K * self.n, torch.float64).view(2 * K, self.n)
+            chi = self._buf("chi", 2 * K * self.n, torch.float64).view(2 * K, self.n)
+            ckey = self._buf("ckey", 2 * K * self.S, torch.float64).view(2 * K, self.S)
             parents = torch.cat([kept[:K], kept[:K]])
             if not self.clip:
                 _lib.check(L.gear_bab_split(_p(lo), _p(hi), _p(kept), K, self.n, _p(split_idx), _p(lb), _p(lA),

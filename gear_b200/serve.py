@@ -68,12 +68,16 @@ class Server:
     round_bytes / (its algorithmic bytes per box) domains per round, clamped to
     [min_batch, batch]: small instances take large batches (fewer rounds to their gap) and
     large ones do not stretch every round. max_live: at most this many instances run at once
-    (a round's host work grows with the number of live instances); the others wait."""
+    (a round's host work grows with the number of live instances); the others wait. admission:
+    "fifo" admits waiting requests in arrival order, "small_first" the narrowest boxes first
+    (the quickest to close). incumbent_every: each instance evaluates its model at the popped
+    midpoints on every k-th of its rounds only (BaB(incumbent_every=k))."""
 
     def __init__(self, device="cuda", batch: int = 256, rel_gap: float = 1e-4, time_budget: float = 30.0,
                  hbm_budget: Optional[int] = None, cta_threads: int = 256, simt_items_max: int = SIMT_PACK_ITEMS,
                  ibp_enhancement: bool = True, clock=time.perf_counter, round_bytes: Optional[int] = None,
-                 min_batch: int = 16, max_live: Optional[int] = None):
+                 min_batch: int = 16, max_live: Optional[int] = None, admission: str = "fifo",
+                 incumbent_every: int = 1):
         if not torch.cuda.is_available():
             raise _lib.GearError("gear_b200 needs a CUDA device (no CPU fallback)")
         self.device = torch.device(device)
@@ -83,6 +87,10 @@ class Server:
         self.clock = clock
         self.round_bytes, self.min_batch = round_bytes, min_batch
         self.live_cap = max_live
+        if admission not in ("fifo", "small_first"):
+            raise ValueError(f"unknown admission order {admission!r}")
+        self.admission = admission
+        self.incumbent_every = incumbent_every
         self.t_bound = 0.0                 # host seconds in the CROWN launches / the rest of a round
         self.t_round = 0.0
         if hbm_budget is None:
@@ -121,7 +129,10 @@ class Server:
 
     def _admit(self, now):
         still = []
-        for r in self.waiting:
+        order = self.waiting
+        if self.admission == "small_first":
+            order = sorted(self.waiting, key=lambda r: (r.lo.shape[1], r.arrival))
+        for r in order:
             if r.arrival <= now and now - r.arrival > self.time_budget:
                 r.status, r.finished = "budget", now     # its budget ran out before a slot freed up
                 self.done[r.key] = r
@@ -145,12 +156,13 @@ class Server:
             if self.round_bytes:
                 batch = int(min(self.batch, max(self.min_batch, self.round_bytes // max(prog.alg_bytes_per_box(), 1))))
             bab = BaB(g, r.lo, r.hi, rhs=r.rhs, device=str(self.device), batch=batch,
-                      engine=_Shape(prog.n, prog.S), model=model, ibp_enhancement=self.ibp_enhancement)
+                      engine=_Shape(prog.n, prog.S), model=model, ibp_enhancement=self.ibp_enhancement,
+                      incumbent_every=self.incumbent_every)
             r.admitted = now
             r.status = "running"
             r.group = group
             self.live[r.key] = _Live(r, dag, bab, group, prog.alg_bytes_per_box(), est)
-        self.waiting = still
+        self.waiting = sorted(still, key=lambda r: r.arrival)
 
     # ------------------------------------------------------------------ one round
     def _bound(self, popped, ibp):

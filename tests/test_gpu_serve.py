@@ -23,7 +23,7 @@ def test_serve_same_alone_and_in_mix():
     sizes = [(0, 6), (1, 10), (2, 14), (3, 8), (4, 12), (5, 20)]
     # the clock advances one unit per round: a request leaves after at most 25 rounds in the
     # system (closed, emptied or at its budget), so the rounds each took part in differ
-    srv = Server(batch=64, rel_gap=1e-4, time_budget=25.0)
+    srv = Server(batch=64, rel_gap=1e-4, time_budget=25.0, admission="small_first", incumbent_every=3)
     reqs = {}
     clock = 0.0
     pending = list(sizes)
@@ -44,7 +44,7 @@ def test_serve_same_alone_and_in_mix():
         mode, threads = r.group[:2]
         g = r.graph
         eng = CrownEngine(g, mode=mode, cta_threads=threads or 128)
-        bb = BaB(g, lo, hi, batch=64, engine=eng, model=m.cuda())
+        bb = BaB(g, lo, hi, batch=64, engine=eng, model=m.cuda(), incumbent_every=3)
         for _ in range(r.rounds):
             bb.step()
         assert bb.incumbent == r.P
