@@ -144,4 +144,63 @@ class BoundedModule:
             "lA": lA, "uA": None, "lbias": lbias, "ubias": None, "unstable_idx": None}}}
         return lb, None, A
 
+    def compute_bounds_host(self, x_L: torch.Tensor, x_U: torch.Tensor, chunk: int = 16384):
+        """CROWN lower bounds (identity specification) of boxes held in HOST memory, with the
+        copies overlapped with the kernels: chunks of `chunk` boxes go host -> device on one
+        stream, are bounded on the current stream and their lb rows come back on a third, through
+        two device buffers. Returns lb (B, S) in pinned host memory, complete once the current
+        stream has been synchronised. Pinned inputs make the copies asynchronous."""
+        B = x_L.shape[0]
+        x_L = x_L.reshape(B, -1)
+        x_U = x_U.reshape(B, -1)
+        n = x_L.shape[1]
+        w = self.final_node_width()
+        eng = self._engine(w, False)
+        dev = self.device
+        lb_h = torch.empty(B, w, dtype=torch.float64, pin_memory=True)
+        if B == 0:
+            return lb_h
+        chunk = max(1, min(int(chunk), B))
+        cur = torch.cuda.current_stream(dev)
+        if getattr(self, "_copy_streams", None) is None or self._copy_streams[0].device != dev:
+            self._copy_streams = (torch.cuda.Stream(dev), torch.cuda.Stream(dev))
+        s_in, s_out = self._copy_streams
+        key = (chunk, n, w)
+        if getattr(self, "_host_bufs", None) is None or self._host_bufs[0] != key:
+            self._host_bufs = (key, [dict(L=torch.empty(chunk, n, dtype=torch.float64, device=dev),
+                                          U=torch.empty(chunk, n, dtype=torch.float64, device=dev),
+                                          lb=torch.empty(chunk, w, dtype=torch.float64, device=dev),
+                                          lA=torch.empty(chunk, w, n, dtype=torch.float64, device=dev),
+                                          lbias=torch.empty(chunk, w, dtype=torch.float64, device=dev))
+                                     for _ in range(2)])
+        bufs = self._host_bufs[1]
+        ins, done, outs = [], [], []
+        s_in.wait_stream(cur)
+        s_out.wait_stream(cur)
+        for k, a in enumerate(range(0, B, chunk)):
+            b = min(a + chunk, B)
+            m = b - a
+            buf = bufs[k % 2]
+            with torch.cuda.stream(s_in):
+                if k >= 2:
+                    s_in.wait_event(done[k - 2])          # the kernel of chunk k-2 has read this buffer
+                buf["L"][:m].copy_(x_L[a:b], non_blocking=True)
+                buf["U"][:m].copy_(x_U[a:b], non_blocking=True)
+                ins.append(torch.cuda.Event())
+                ins[-1].record(s_in)
+            cur.wait_event(ins[k])
+            if k >= 2:
+                cur.wait_event(outs[k - 2])               # chunk k-2's lb rows have left this buffer
+            eng.lower(buf["L"][:m], buf["U"][:m], None, out=(buf["lb"][:m], buf["lA"][:m], buf["lbias"][:m]))
+            done.append(torch.cuda.Event())
+            done[-1].record(cur)
+            with torch.cuda.stream(s_out):
+                s_out.wait_event(done[k])
+                lb_h[a:b].copy_(buf["lb"][:m], non_blocking=True)
+                outs.append(torch.cuda.Event())
+                outs[-1].record(s_out)
+        cur.wait_stream(s_out)
+        cur.wait_stream(s_in)
+        return lb_h
+
     __call__ = compute_bounds

@@ -138,3 +138,16 @@ def test_gpu_ibp_pass_matches_reference(key):
     got = lb_ibp.cpu().numpy()
     assert np.max(np.abs(got - ref) / np.maximum(1.0, np.abs(ref))) < 1e-13
     assert torch.equal(lb, torch.maximum(plain, lb_ibp))
+
+
+def test_compute_bounds_host_matches_device_call():
+    """The pipelined host-buffer call (chunks not dividing the batch) gives the device call's bits."""
+    m = problems.make_instance("dense_q_n200", 0)
+    lo, hi = problems.make_boxes("dense_q_n200", 1000, 0)
+    bm = BoundedModule(m, lo[:2], device="cuda", bound_opts={"gear_mode": "cta", "gear_cta_threads": 128})
+    hL, hU = lo.pin_memory(), hi.pin_memory()
+    lb_h = bm.compute_bounds_host(hL, hU, chunk=300)
+    x = BoundedTensor(lo.cuda(), PerturbationLpNorm(x_L=lo.cuda(), x_U=hi.cuda()))
+    lb_d, _ = bm.compute_bounds(x=(x,), method="CROWN", bound_upper=False)
+    torch.cuda.synchronize()
+    assert torch.equal(lb_h, lb_d.cpu())
