@@ -58,6 +58,7 @@ class DomainQueue:
         self.free: List[torch.Tensor] = []
         self.active = torch.empty(0, dtype=torch.int32, device=device)
         self.next_id = 0
+        self._pop_bufs = {}
         self._grow(max(capacity, 1))
 
     def _fields(self):
@@ -108,7 +109,8 @@ class DomainQueue:
         self.active = torch.cat([self.active, slots])
 
     def pop(self, batch: int):
-        """Sort by (objective key desc, id asc) and take the last `batch` domains."""
+        """Sort by (objective key desc, id asc) and take the last `batch` domains. The returned
+        rows live in buffers the next pop reuses."""
         N = len(self)
         b = min(batch, N)
         n2 = 1 << max(0, (N - 1).bit_length())
@@ -123,7 +125,11 @@ class DomainQueue:
         self.active = order[:N - b].contiguous()
         out = []
         for name, w in self._fields():
-            dst = torch.empty(b, w, dtype=torch.float64, device=self.device)
+            # popped rows live until the end of the iteration that pops them: reused buffers
+            buf = self._pop_bufs.get(name)
+            if buf is None or buf.numel() < b * w:
+                buf = self._pop_bufs[name] = torch.empty(max(b * w, 1), dtype=torch.float64, device=self.device)
+            dst = buf[:b * w].view(b, w)
             _lib.check(L.gear_gather_rows(_p(getattr(self, name)), _p(slots), b, w, _p(dst), stream),
                        "gear_gather_rows")
             out.append(dst)
@@ -416,7 +422,7 @@ def bab_round(babs, bound, ibp_enhancement=True):
         vals = torch.cat([cands[k][0] for k in keys]).tolist()            # one host read
         for k, v in zip(keys, vals):
             babs[k].accept_incumbent(v, cands[k][1])
-    ibp = {k: torch.empty(p[0].shape[0], babs[k].S, dtype=torch.float64, device=p[0].device)
+    ibp = {k: babs[k]._buf("lb_ibp", p[0].shape[0] * babs[k].S, torch.float64).view(p[0].shape[0], babs[k].S)
            for k, p in popped.items()} if ibp_enhancement else {}
     outs = bound(popped, ibp)
     sts = {k: babs[k].prune_branch(popped[k], *outs[k]) for k in popped}

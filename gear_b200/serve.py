@@ -179,10 +179,12 @@ class Server:
             for j, k in enumerate(keys):
                 lo, hi = popped[k][0], popped[k][1]
                 B, n = lo.shape
-                S = self.live[k].bab.S
-                lb = torch.empty(B, S, dtype=torch.float64, device=dev)
-                lA = torch.empty(B, S, n, dtype=torch.float64, device=dev)
-                lbias = torch.empty(B, S, dtype=torch.float64, device=dev)
+                bab = self.live[k].bab
+                S = bab.S
+                # the instance's own buffers, reused every round (consumed within the round)
+                lb = bab._buf("lb", B * S, torch.float64).view(B, S)
+                lA = bab._buf("lA", B * S * n, torch.float64).view(B, S, n)
+                lbias = bab._buf("lbias", B * S, torch.float64).view(B, S)
                 outs[k] = (lb, lA, lbias)
                 ib = ibp.get(k)
                 args[j] = _lib.LowerArgs(self.live[k].dag.handle.value, lo.data_ptr(), hi.data_ptr(), B, None,
