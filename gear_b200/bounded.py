@@ -151,9 +151,9 @@ class BoundedModule:
         two device buffers. Returns lb (B, S) in pinned host memory, complete once the current
         stream has been synchronised. Pinned inputs make the copies asynchronous."""
         B = x_L.shape[0]
-        x_L = x_L.reshape(B, -1)
-        x_U = x_U.reshape(B, -1)
-        n = x_L.shape[1]
+        n = self.graph[0].width
+        x_L = x_L.reshape(B, n)
+        x_U = x_U.reshape(B, n)
         w = self.final_node_width()
         eng = self._engine(w, False)
         dev = self.device

@@ -151,3 +151,15 @@ def test_compute_bounds_host_matches_device_call():
     lb_d, _ = bm.compute_bounds(x=(x,), method="CROWN", bound_upper=False)
     torch.cuda.synchronize()
     assert torch.equal(lb_h, lb_d.cpu())
+
+
+def test_compute_bounds_host_small_batch_and_empty():
+    m = problems.make_instance("quad_exp_n10", 0)
+    lo, hi = problems.make_boxes("quad_exp_n10", 37, 0)
+    bm = BoundedModule(m, lo[:2], device="cuda", bound_opts={"gear_mode": "simt"})
+    lb_h = bm.compute_bounds_host(lo.pin_memory(), hi.pin_memory(), chunk=4096)   # one partial chunk
+    x = BoundedTensor(lo.cuda(), PerturbationLpNorm(x_L=lo.cuda(), x_U=hi.cuda()))
+    lb_d, _ = bm.compute_bounds(x=(x,), method="CROWN", bound_upper=False)
+    torch.cuda.synchronize()
+    assert torch.equal(lb_h, lb_d.cpu())
+    assert bm.compute_bounds_host(lo[:0], hi[:0]).shape == (0, 3)

@@ -149,3 +149,40 @@ def test_multi_bab_matches_single_runs():
         assert bb.incumbent == res[i]["P"]
         assert bb.stats.bounded == res[i]["bounded"]
         assert bb.dual_bound() == float(torch.minimum(mb.babs[i].queue.min_key_tensor(), mb.babs[i].disc_min))
+
+
+def test_multi_ibp_pass_and_empty_groups():
+    """The IBP pass through the packed launch equals CrownEngine's, and groups whose instances
+    all have empty batches launch nothing (their outputs are empty)."""
+    graphs, boxes = _instances()
+    me = MultiEngine(graphs, mode="auto", cta_threads=128)
+    # empty every instance of one group, keep the others
+    first_group = next(iter(me.groups.values()))
+    bx, ibp = [], []
+    for i, (lo, hi) in enumerate(boxes):
+        if i in first_group:
+            lo, hi = lo[:0], hi[:0]
+        bx.append((lo.cuda(), hi.cuda()))
+        ibp.append(torch.empty(lo.shape[0], me.S[i], dtype=torch.float64, device="cuda"))
+    outs = me.lower(bx, lb_ibp=ibp)
+    torch.cuda.synchronize()
+    for i, g in enumerate(graphs):
+        B = bx[i][0].shape[0]
+        assert outs[i][0].shape == (B, me.S[i])
+        if B == 0:
+            continue
+        var = me.variants[i]
+        eng = CrownEngine(g, mode=var[0], cta_threads=var[1] or 128)
+        ib = torch.empty(B, me.S[i], dtype=torch.float64, device="cuda")
+        lb1, _, _ = eng.lower(bx[i][0], bx[i][1], lb_ibp=ib)
+        torch.cuda.synchronize()
+        assert torch.equal(outs[i][0], lb1) and torch.equal(ibp[i], ib)
+
+
+def test_plain_form_empty_batch():
+    from gear_b200.engine import PlainEngine
+    m = problems.make_instance("quad_exp_n10", 0)
+    pe = PlainEngine(_graph(m, 10))
+    e = torch.empty(0, 10, dtype=torch.float64, device="cuda")
+    lb, lA, lbias = pe.lower(e, e)
+    assert lb.shape == (0, 3) and lA.shape == (0, 3, 10)
