@@ -336,7 +336,7 @@ def mixed_bab(dev, setup, batch=256, rel_gap=1e-4, time_limit=60.0):
 
 
 def serve(dev, seconds=10.0, rate=50.0, budget=30.0, batch=2048, rel_gap=1e-4, seed=0, round_bytes=16 << 20,
-          max_live=96, admission="small_first", incumbent_every=4):
+          max_live=128, admission="small_first", incumbent_every=4, round_cap=16):
     """The serving loop under Poisson arrivals (rate per second for `seconds`): instances of the
     quad-exp family with n log-uniform in [5, 2000] (two bilinear constraints), each to the
     relative gap or its time budget (from arrival). Continuous batching (Server): requests are
@@ -355,7 +355,7 @@ def serve(dev, seconds=10.0, rate=50.0, budget=30.0, batch=2048, rel_gap=1e-4, s
     ns = [int(round(_m.exp(_m.log(5) + (_m.log(2000) - _m.log(5)) * float(torch.rand(1, generator=g)))))
           for _ in arrivals]
     srv = Server(device=str(dev), batch=batch, rel_gap=rel_gap, time_budget=budget, round_bytes=round_bytes,
-                 max_live=max_live, admission=admission, incumbent_every=incumbent_every)
+                 max_live=max_live, admission=admission, incumbent_every=incumbent_every, round_cap=round_cap)
     t0 = time.perf_counter()
     clock = lambda: time.perf_counter() - t0
     srv.clock = clock
@@ -386,7 +386,7 @@ def serve(dev, seconds=10.0, rate=50.0, budget=30.0, batch=2048, rel_gap=1e-4, s
             "subdomains_per_s": srv.bounded / wall, "rounds": srv.rounds, "max_concurrent": srv.max_live,
             "rel_gap": rel_gap, "budget_s": budget, "batch_per_instance_max": batch, "round_bytes": round_bytes,
             "max_live": max_live, "waited_out": sum(1 for r in done if r.admitted is None),
-            "admission": admission, "incumbent_every": incumbent_every,
+            "admission": admission, "incumbent_every": incumbent_every, "round_cap": round_cap,
             "closed_n_max": max((r.lo.shape[1] for r in done if r.status == "closed"), default=None),
             "host_s": {"rounds": srv.t_round, "crown_launch_calls": srv.t_bound}, "wall_s": wall,
             "timing": "wall clock; time to gap from each request's arrival to the round that closed it"}

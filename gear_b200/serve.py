@@ -71,13 +71,15 @@ class Server:
     (a round's host work grows with the number of live instances); the others wait. admission:
     "fifo" admits waiting requests in arrival order, "small_first" the narrowest boxes first
     (the quickest to close). incumbent_every: each instance evaluates its model at the popped
-    midpoints on every k-th of its rounds only (BaB(incumbent_every=k))."""
+    midpoints on every k-th of its rounds only (BaB(incumbent_every=k)). round_cap: a round
+    runs at most this many live instances, the narrowest boxes first (then by arrival); the
+    others keep their state and wait for a later round (their budget keeps running)."""
 
     def __init__(self, device="cuda", batch: int = 256, rel_gap: float = 1e-4, time_budget: float = 30.0,
                  hbm_budget: Optional[int] = None, cta_threads: int = 256, simt_items_max: int = SIMT_PACK_ITEMS,
                  ibp_enhancement: bool = True, clock=time.perf_counter, round_bytes: Optional[int] = None,
                  min_batch: int = 16, max_live: Optional[int] = None, admission: str = "fifo",
-                 incumbent_every: int = 1):
+                 incumbent_every: int = 1, round_cap: Optional[int] = None):
         if not torch.cuda.is_available():
             raise _lib.GearError("gear_b200 needs a CUDA device (no CPU fallback)")
         self.device = torch.device(device)
@@ -91,6 +93,7 @@ class Server:
             raise ValueError(f"unknown admission order {admission!r}")
         self.admission = admission
         self.incumbent_every = incumbent_every
+        self.round_cap = round_cap
         self.t_bound = 0.0                 # host seconds in the CROWN launches / the rest of a round
         self.t_round = 0.0
         if hbm_budget is None:
@@ -215,7 +218,11 @@ class Server:
         self.max_live = max(self.max_live, len(self.live))
         if not self.live:
             return 0
-        babs = {k: lv.bab for k, lv in self.live.items()}
+        keys = list(self.live)
+        if self.round_cap is not None and len(keys) > self.round_cap:
+            keys = sorted(keys, key=lambda k: (self.live[k].req.lo.shape[1], self.live[k].req.arrival))
+            keys = keys[:self.round_cap]
+        babs = {k: self.live[k].bab for k in keys}
         t0 = time.perf_counter()
         B = bab_round(babs, self._timed_bound, self.ibp_enhancement)
         self.t_round += time.perf_counter() - t0
@@ -226,14 +233,15 @@ class Server:
         for k in list(self.live):
             lv = self.live[k]
             r = lv.req
-            r.rounds += 1
-            r.gap, r.P, r.bounded = gaps[k], lv.bab.incumbent, lv.bab.stats.bounded
             status = None
-            if gaps[k] <= self.rel_gap:
-                status = "closed"
-            elif len(lv.bab.queue) == 0:
-                status = "emptied"
-            elif t - r.arrival > self.time_budget:
+            if k in babs:
+                r.rounds += 1
+                r.gap, r.P, r.bounded = gaps[k], lv.bab.incumbent, lv.bab.stats.bounded
+                if gaps[k] <= self.rel_gap:
+                    status = "closed"
+                elif len(lv.bab.queue) == 0:
+                    status = "emptied"
+            if status is None and t - r.arrival > self.time_budget:
                 status = "budget"
             if status:
                 r.status, r.finished = status, t

@@ -23,7 +23,8 @@ def test_serve_same_alone_and_in_mix():
     sizes = [(0, 6), (1, 10), (2, 14), (3, 8), (4, 12), (5, 20)]
     # the clock advances one unit per round: a request leaves after at most 25 rounds in the
     # system (closed, emptied or at its budget), so the rounds each took part in differ
-    srv = Server(batch=64, rel_gap=1e-4, time_budget=25.0, admission="small_first", incumbent_every=3)
+    srv = Server(batch=64, rel_gap=1e-4, time_budget=25.0, admission="small_first", incumbent_every=3,
+                 round_cap=3)
     reqs = {}
     clock = 0.0
     pending = list(sizes)
