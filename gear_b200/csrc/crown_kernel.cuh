@@ -915,7 +915,10 @@ __device__ __forceinline__ void gemv_row(const double* V, const int32_t* vcols, 
 // ops [op_lo, op_hi) of the pass then run; phase bit 2: concretise and write the outputs. The
 // fused kernels run everything in one call; the plain form calls each phase and each op in a
 // launch of its own (the working set then lives in global memory).
-template <int NT, bool WHOLE = true>
+// IDX: also skip the loads of identity source / target lists and row pointers (OpFlag). Used
+// by the instances whose working set is in global memory; in the shared-memory instances the
+// extra live flags cost more in register spills than the loads they save (measured).
+template <int NT, bool WHOLE = true, bool IDX = false>
 __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops, const Work& wk, int op_lo_ = 0,
                          int op_hi_ = 1 << 30, int phase_ = 3) {
   // WHOLE: every phase and every op (compile-time constants for the fused kernels)
@@ -1006,6 +1009,7 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
     const double* m1 = (kind == NK_ADD || kind == NK_SUB) ? bx.mag + node_rec(P, vnd[N_IN1])[N_CUR] : nullptr;
     const double* bvec = (kind == NK_LINEAR && vnd[N_B_OFF] >= 0) ? P->dp + vnd[N_B_OFF] : nullptr;
     const bool dense = op[O_DENSE] != 0 && !op[O_FOLD];
+    const int oflags = op[O_SINGLE];   // OpFlag bits
 
     // ---- per-row work of a non-GEMV op: bias/charges over v's row, zero u's row on its first
     //      contribution, pull the row's moves (or fold it into the concretisation)
@@ -1024,7 +1028,8 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
     // mode 0: one thread per row, 1: a warp, 2: the whole CTA (every thread calls with the same s)
     auto row_body = [&](int s, int eoff, int estep, int mode) {
       const bool lead = mode == 0 || (mode == 1 ? lane == 0 : tid == 0);
-      const int e0 = vrp[s], e1 = vrp[s + 1];
+      const bool vid = IDX && (oflags & OF_VRP_ID);
+      const int e0 = vid ? s : vrp[s], e1 = vid ? s + 1 : vrp[s + 1];
       for (int side = 0; side < sides; ++side) {
         const double* V = ctx.vals(side, op[O_VBUF]);
         if (need_a && e0 < e1) {
@@ -1099,18 +1104,18 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
           if (mode == 2) __syncthreads();
         }
         const int32_t* tptr = P->ip + op[O_TPTR];
-        const int k0 = tptr[s], k1 = tptr[s + 1];
+        const int k0 = (oflags & OF_TPTR_ID) ? s : tptr[s], k1 = (oflags & OF_TPTR_ID) ? s + 1 : tptr[s + 1];
         if (k0 == k1) continue;
         const int32_t* tgt = P->ip + op[O_TGT];
         const int32_t* sptr = P->ip + op[O_SPTR];
         const int32_t* src = P->ip + op[O_SRC];
         double pmerge = 0;
-        const bool single = op[O_SINGLE] != 0;
+        const bool single = (oflags & OF_SINGLE) != 0;
         for (int k = k0 + eoff; k < k1; k += estep) {
           double acc = 0;
           const int q0 = single ? k : __ldg(sptr + k), q1 = single ? k + 1 : __ldg(sptr + k + 1);
           for (int q = q0; q < q1; ++q) {
-            int e = __ldg(src + q);
+            int e = (IDX && (oflags & OF_SRC_ID)) ? q : __ldg(src + q);
             double a = V[e];
             int c = __ldg(vcols + e);
             double bt;
@@ -1118,7 +1123,7 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
             if (!isfinite(na)) na = 0.0;
             acc += na;
           }
-          int ti = tgt[k];
+          int ti = (IDX && (oflags & OF_TGT_ID)) ? k : tgt[k];
           U[ti] += acc;
           if (uk >= 2 && acc != 0.0) {
             int col = u_la ? ti - s * n : ucols[ti];
@@ -1409,7 +1414,7 @@ __device__ __forceinline__ void cta_load(Box& bx, const int32_t* hdr, const Work
 
 // Schedule step si of the bound program for the current box (a CROWN pass: ops [op_lo, op_hi)
 // and the phases of run_pass).
-template <int NT, bool WHOLE = true>
+template <int NT, bool WHOLE = true, bool IDX = false>
 __device__ __forceinline__ void cta_step(const DevProgram& P, Box& bx, double* tmp_lo, double* tmp_hi, int32_t* sops,
                                          const Work& wk, double* work, int si, int op_lo = 0, int op_hi = 1 << 30,
                                          int phase = 3) {
@@ -1451,8 +1456,8 @@ __device__ __forceinline__ void cta_step(const DevProgram& P, Box& bx, double* t
       break;
     }
     case ST_PASS: case ST_FINAL:
-      if (WHOLE) run_pass<NT, true>(bx, a, work, sops, wk);
-      else run_pass<NT, false>(bx, a, work, sops, wk, op_lo, op_hi, phase);
+      if (WHOLE) run_pass<NT, true, IDX>(bx, a, work, sops, wk);
+      else run_pass<NT, false, IDX>(bx, a, work, sops, wk, op_lo, op_hi, phase);
       break;
     case ST_COMPARE: compare_node<NT>(bx, a, tmp_lo, tmp_hi, st[3] != 0); break;
     default: break;
@@ -1460,7 +1465,7 @@ __device__ __forceinline__ void cta_step(const DevProgram& P, Box& bx, double* t
 }
 
 // The whole schedule for box b of wk on the bound program.
-template <int NT>
+template <int NT, bool IDX = false>
 __device__ __forceinline__ void cta_box(const DevProgram& P, Box& bx, double* tmp_lo, double* tmp_hi, int32_t* sops,
                                         const Work& wk, int64_t b, double* work) {
   const int nsteps = P.hdr[H_NSTEPS];
@@ -1469,7 +1474,7 @@ __device__ __forceinline__ void cta_box(const DevProgram& P, Box& bx, double* tm
 #ifdef GEAR_STEP_PROFILE
     long long t_step = clock64();
 #endif
-    cta_step<NT>(P, bx, tmp_lo, tmp_hi, sops, wk, work, si);
+    cta_step<NT, true, IDX>(P, bx, tmp_lo, tmp_hi, sops, wk, work, si);
     __syncthreads();
 #ifdef GEAR_STEP_PROFILE
     if (threadIdx.x == 0 && si < 8192) atomicAdd(&g_step_cycles[si], (unsigned long long)(clock64() - t_step));
@@ -1486,7 +1491,8 @@ __global__ void __launch_bounds__(NT, GEAR_CTA_MINB / NT) crown_megakernel(DevPr
   Box bx;
   double *tmp_lo, *tmp_hi, *work;
   int32_t* sops = cta_bind<NT>(P, bx, tmp_lo, tmp_hi, work, Pg, sm, wk.scratch + (size_t)blockIdx.x * wk.slot_doubles);
-  for (int64_t b = blockIdx.x; b < wk.B; b += gridDim.x) cta_box<NT>(P, bx, tmp_lo, tmp_hi, sops, wk, b, GWS ? work : sm);
+  for (int64_t b = blockIdx.x; b < wk.B; b += gridDim.x)
+    cta_box<NT, GWS>(P, bx, tmp_lo, tmp_hi, sops, wk, b, GWS ? work : sm);
 }
 
 // ------------------------------------------------------------------ the plain (unfused) form
@@ -1506,7 +1512,7 @@ crown_plain_kernel(DevProgram Pg, Work wk, int si, int op_lo, int op_hi, int pha
   for (int64_t b = blockIdx.x; b < wk.B; b += gridDim.x) {
     cta_slot(bx, tmp_lo, tmp_hi, work, Pg.hdr, sm, wk.scratch + (size_t)b * wk.slot_doubles);
     cta_load<NT>(bx, Pg.hdr, wk, b, si < 0);
-    if (si >= 0) cta_step<NT, false>(P, bx, tmp_lo, tmp_hi, sops, wk, work, si, op_lo, op_hi, phase);
+    if (si >= 0) cta_step<NT, false, true>(P, bx, tmp_lo, tmp_hi, sops, wk, work, si, op_lo, op_hi, phase);
     __syncthreads();
   }
 }
@@ -1565,7 +1571,7 @@ crown_multi_megakernel(const MultiItem* __restrict__ items, int count, const int
       sops = cta_bind<NT>(P, bx, tmp_lo, tmp_hi, work, items[i].P, sm, slot);
       cur = i;
     }
-    cta_box<NT>(P, bx, tmp_lo, tmp_hi, sops, items[i].wk, g - start[i], GWS ? work : sm);   // Work read in place
+    cta_box<NT, GWS>(P, bx, tmp_lo, tmp_hi, sops, items[i].wk, g - start[i], GWS ? work : sm);   // Work read in place
   }
 }
 

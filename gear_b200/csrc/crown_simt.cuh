@@ -377,7 +377,7 @@ __device__ void simt_run_pass(const SBox& bx, int pid, const Work& wk, bool live
       const int32_t* tgt = P->ip + op[O_TGT];
       const int32_t* sptr = P->ip + op[O_SPTR];
       const int32_t* src = P->ip + op[O_SRC];
-      const bool single = op[O_SINGLE] != 0;
+      const bool single = (op[O_SINGLE] & OF_SINGLE) != 0;
       for (int s = 0; s < S; ++s) {
         const int k0 = __ldg(tptr + s), k1 = __ldg(tptr + s + 1);
         if (k0 == k1) continue;

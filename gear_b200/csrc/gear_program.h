@@ -33,6 +33,10 @@ enum OpField {
   O_UCOLS, O_UMERGE, O_NTGT, O_TGT, O_SPTR, O_SRC, O_DENSE, O_FOLD, O_WOUT, O_VMAXROW, O_UMAXROW, O_VROWS,
   O_TPTR, O_UK, O_TMAXROW, O_SHORT, O_NSHORT, O_LONG, O_NLONG, O_SINGLE, OP_REC = 32
 };
+// bits of an op record's O_SINGLE field: every target pulls one source; the source list, the
+// target list, the target row pointers or v's row pointers are the identity (the kernel then
+// computes the index instead of loading it)
+enum OpFlag { OF_SINGLE = 1, OF_SRC_ID = 2, OF_TGT_ID = 4, OF_TPTR_ID = 8, OF_VRP_ID = 16 };
 // buffer offset marker: the input's A of a final pass accumulates in the lA output (row s at s * n)
 constexpr int ROOT_IN_LA = -2;
 // rows with at most this many entries are handled by one thread, longer rows by a warp

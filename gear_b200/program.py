@@ -61,6 +61,8 @@ OP_REC = 32
  O_UCOLS, O_UMERGE, O_NTGT, O_TGT, O_SPTR, O_SRC, O_DENSE, O_FOLD, O_WOUT, O_VMAXROW, O_UMAXROW, O_VROWS,
  O_TPTR, O_UK, O_TMAXROW, O_SHORT, O_NSHORT, O_LONG, O_NLONG, O_SINGLE) = range(32)
 ROW_THREAD_MAX = 16  # rows with at most this much work run on one thread, longer rows on a warp
+# bits of the op record's O_SINGLE field (OpFlag in gear_program.h)
+OF_SINGLE, OF_SRC_ID, OF_TGT_ID, OF_TPTR_ID, OF_VRP_ID = 1, 2, 4, 8, 16
 ROOT_IN_LA = -2     # buffer marker: the input's A of a final pass accumulates in the lA output
 
 PLANES_PER_ELEM = {"mul": 6, "sqr": 4, "exp": 4, "log": 4, "sin": 4, "cos": 4, "pow": 4}
@@ -574,6 +576,7 @@ class Program:
             k = n.kind
             for slot, p in enumerate(n.inputs):
                 r = np.full(OP_REC, -1, dtype=np.int32)
+                r[O_SINGLE] = 0                      # index-shape flags, set for pull-move ops below
                 kk = k if k not in MAP_KINDS else "map"
                 r[O_KIND] = NK[kk]
                 r[O_V] = v
@@ -629,8 +632,21 @@ class Program:
                     r[O_TGT] = P.add_int(tgt)
                     r[O_SPTR] = P.add_int(sptr)
                     r[O_SRC] = P.add_int(src)
-                    # every target pulls exactly one source: src[k] is target k's source
-                    r[O_SINGLE] = 1 if (len(src) == len(tgt)) else 0
+                    # index-shape flags (OpFlag in gear_program.h): every target pulls exactly one
+                    # source; sources, targets, target row pointers or v's row pointers that are the
+                    # identity, so the kernel computes the index instead of loading it
+                    flags = 0
+                    if len(src) == len(tgt):
+                        flags |= OF_SINGLE
+                    if len(src) and np.array_equal(src, np.arange(len(src))):
+                        flags |= OF_SRC_ID
+                    if np.array_equal(tgt, np.arange(len(tgt))):
+                        flags |= OF_TGT_ID
+                    if np.array_equal(tptr, np.arange(S + 1)):
+                        flags |= OF_TPTR_ID
+                    if np.array_equal(rowptr[v], np.arange(S + 1)):
+                        flags |= OF_VRP_ID
+                    r[O_SINGLE] = flags
                 else:
                     r[O_NTGT] = 0
                 # rows this op works on, split by length: short rows one thread, long rows one warp
