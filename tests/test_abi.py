@@ -67,3 +67,13 @@ def test_dag_create_rejects_bad_arguments(lib):
                              ctypes.c_int64(0), ctypes.byref(h))
     assert st == -1 and not h.value
     assert b"bad arguments" in lib.gear_last_error()
+
+
+def test_multi_and_plain_sizes_reject_bad_arguments(lib):
+    lib.gear_crown_multi_workspace_bytes.restype = ctypes.c_int64
+    lib.gear_crown_multi_workspace_bytes.argtypes = [ctypes.c_void_p, ctypes.c_int32]
+    assert lib.gear_crown_multi_workspace_bytes(None, -1) == -1
+    assert lib.gear_crown_multi_workspace_bytes(None, 0) == 0        # nothing to launch
+    lib.gear_crown_plain_workspace_bytes.restype = ctypes.c_int64
+    lib.gear_crown_plain_workspace_bytes.argtypes = [ctypes.c_void_p, ctypes.c_int64]
+    assert lib.gear_crown_plain_workspace_bytes(None, 1) == -1
