@@ -147,10 +147,13 @@ def test_compute_bounds_host_matches_device_call():
     bm = BoundedModule(m, lo[:2], device="cuda", bound_opts={"gear_mode": "cta", "gear_cta_threads": 128})
     hL, hU = lo.pin_memory(), hi.pin_memory()
     lb_h = bm.compute_bounds_host(hL, hU, chunk=300)
+    lb_h2 = bm.compute_bounds_host(hL.flip(0).contiguous().pin_memory(), hU.flip(0).contiguous().pin_memory(),
+                                   chunk=300)            # a second call right behind the first
     x = BoundedTensor(lo.cuda(), PerturbationLpNorm(x_L=lo.cuda(), x_U=hi.cuda()))
     lb_d, _ = bm.compute_bounds(x=(x,), method="CROWN", bound_upper=False)
     torch.cuda.synchronize()
     assert torch.equal(lb_h, lb_d.cpu())
+    assert torch.equal(lb_h2, lb_d.cpu().flip(0))
 
 
 def test_compute_bounds_host_small_batch_and_empty():
