@@ -94,7 +94,6 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- CPU leg (oracle)
 def _cpu_worker(args):
-    import numpy as np
     os.environ.setdefault("OMP_NUM_THREADS", "1")
     sys.path.insert(0, ROOT)
     from oracle.crown import CrownOracle
