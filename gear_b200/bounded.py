@@ -28,7 +28,12 @@ from . import graph as _graph
 from .engine import CrownEngine
 
 # The reference's GEAR configuration turns these on (exp_configs/NLP_solver/f3.yaml); the
-# engine always behaves as if they were set.
+# engine always behaves as if the first three were set. For 'undefined_relaxation_interval' it
+# applies the coarser row rule only: a row that touches an element whose relaxation is undefined
+# (a non-finite input interval, log of a non-positive interval, an overflowing exp) is discarded
+# and falls back to the output interval, where the reference first tries to stop just the
+# coefficients selecting the undefined side (backward_bound.py:249-292). Both are sound; they
+# differ only on boxes with such elements.
 HOT_PATH_BOUND_OPTS = {'fp_enclosure': {'affine_backward': True}, 'compare_crown_with_ibp_intermediate': True,
                        'undefined_relaxation_rows': True, 'undefined_relaxation_interval': True}
 
