@@ -199,6 +199,10 @@ class BaB:
         self.x_best = None
         self.incumbent_every = max(1, int(incumbent_every))
         self._bufs = {}
+        # the incumbent on the device: thresholds read it there, so proposing a better one needs
+        # no host read; the host copy (self.incumbent) is refreshed with the survivor count
+        self._inc_dev = torch.full((1,), math.inf, dtype=torch.float64, device=self.device)
+        self._x_best_dev = None
         self.ibp_enhancement = ibp_enhancement
         self.clip = clip
         self.clip_iterations = clip_iterations
@@ -246,40 +250,56 @@ class BaB:
         best = obj.min(0)
         return best.values.reshape(1), x[best.indices]
 
-    def accept_incumbent(self, value: float, point: torch.Tensor):
+    def propose_incumbent(self, x: torch.Tensor):
+        """Fold the best feasible point among x into the device-side incumbent (no host read)."""
+        c = self.incumbent_candidate(x)
+        if c is None:
+            return
+        val, pt = c
+        pt = pt.reshape(-1)
+        if self._x_best_dev is None:
+            self._x_best_dev = pt.clone()
+        else:
+            self._x_best_dev = torch.where(val < self._inc_dev, pt, self._x_best_dev)
+        self._inc_dev = torch.minimum(self._inc_dev, val)
+
+    def sync_incumbent(self, value: float):
+        """Host copy of the device incumbent (value read from it by the caller)."""
         if value < self.incumbent:
             self.incumbent = value
-            self.x_best = point.detach().clone()
+            self.x_best = self._x_best_dev.clone()
 
     def update_incumbent(self, x: torch.Tensor):
         """Primal points: evaluate the model (float64) and keep the best feasible objective."""
-        c = self.incumbent_candidate(x)
-        if c is not None:
-            self.accept_incumbent(float(c[0]), c[1])      # the one host read of the incumbent update
+        self.propose_incumbent(x)
+        self.sync_incumbent(float(self._inc_dev))
 
     def dual_bound(self) -> float:
-        d = self.queue.min_key()
-        return min(d, float(self.disc_min))
+        """min(open objective keys, smallest discarded threshold): one host read."""
+        return float(torch.minimum(self.queue.min_key_tensor(), self.disc_min))
 
-    def gap(self) -> float:
-        P, D = self.incumbent, self.dual_bound()
+    @staticmethod
+    def _gap(P, D):
         if not math.isfinite(P):
             return math.inf
         if not math.isfinite(D):
             return 0.0 if D > 0 else math.inf
         return (P - D) / max(1.0, abs(P), abs(D))
 
+    def gap(self) -> float:
+        return self._gap(self.incumbent, self.dual_bound())
+
     def select(self):
         """Pop the next batch (thresholds at the current incumbent): [lo, hi, key, thr, (cuts)]."""
         popped = self.queue.pop(self.batch)
-        popped[3][:, 0] = self.incumbent
+        popped[3][:, 0] = self._inc_dev
         return popped
 
     def prune_branch(self, popped, lb, lA, lbias):
         """Prune against the thresholds and pick split variables on the device (no host read):
         the state finish() needs, with the survivor count in state["nk"]."""
         lo, hi, key, thr = popped[:4]
-        thr[:, 0] = self.incumbent
+        thr[:, 0] = self._inc_dev                         # after this iteration's proposals
         if self.constrained:
             self._constrained_objective(lo, hi, lb, lA, lbias, popped[4], popped[5])
         B = lo.shape[0]
@@ -359,11 +379,13 @@ class BaB:
         popped = self.select()
         lo, hi = popped[0], popped[1]
         B = lo.shape[0]
-        self.update_incumbent((lo + hi) / 2)
+        self.propose_incumbent((lo + hi) / 2)
         lb_ibp = torch.empty(B, self.S, dtype=torch.float64, device=self.device) if self.ibp_enhancement else None
         lb, lA, lbias = self.engine.lower(lo, hi, lb_ibp=lb_ibp)
         st = self.prune_branch(popped, lb, lA, lbias)
-        self.finish(st, int(st["nk"].item()))        # the one host read per iteration
+        K, inc = torch.cat([st["nk"].to(torch.float64), self._inc_dev]).tolist()   # the iteration's host read
+        self.sync_incumbent(inc)
+        self.finish(st, int(K))
         return B
 
     def _cuts(self, lA, lbias, thr, parents):
@@ -400,35 +422,33 @@ class BaB:
         t0 = time.perf_counter()
         while len(self.queue) and self.stats.iterations < max_iterations:
             self.step()
-            g = self.gap()
-            self.stats.history.append(dict(it=self.stats.iterations, P=self.incumbent, D=self.dual_bound(),
-                                           gap=g, open=len(self.queue)))
+            D = self.dual_bound()
+            g = self._gap(self.incumbent, D)
+            self.stats.history.append(dict(it=self.stats.iterations, P=self.incumbent, D=D, gap=g,
+                                           open=len(self.queue)))
             if g <= rel_gap or time.perf_counter() - t0 > time_limit:
                 break
         return self.incumbent, self.dual_bound(), self.gap()
 
 
 def bab_round(babs, bound, ibp_enhancement=True):
-    """One branch-and-bound iteration over several instances: select on each, the incumbent
-    candidates of all of them in one host read, one bound(popped, lb_ibp) call for all batches
-    (it returns {key: (lb, lA, lbias)}), prune and branch on each, all survivor counts in one
+    """One branch-and-bound iteration over several instances: select on each, their incumbent
+    candidates folded in on the device, one bound(popped, lb_ibp) call for all batches (it returns
+    {key: (lb, lA, lbias)}), prune and branch on each, all survivor counts and incumbents in one
     host read, then split and push on each. babs: {key: BaB}. Returns the domains bounded."""
     popped = {k: b.select() for k, b in babs.items() if len(b.queue)}
     if not popped:
         return 0
-    cands = {k: babs[k].incumbent_candidate((p[0] + p[1]) / 2) for k, p in popped.items()}
-    keys = [k for k, c in cands.items() if c is not None]
-    if keys:
-        vals = torch.cat([cands[k][0] for k in keys]).tolist()            # one host read
-        for k, v in zip(keys, vals):
-            babs[k].accept_incumbent(v, cands[k][1])
+    for k, p in popped.items():
+        babs[k].propose_incumbent((p[0] + p[1]) / 2)                   # on the device
     ibp = {k: babs[k]._buf("lb_ibp", p[0].shape[0] * babs[k].S, torch.float64).view(p[0].shape[0], babs[k].S)
            for k, p in popped.items()} if ibp_enhancement else {}
     outs = bound(popped, ibp)
     sts = {k: babs[k].prune_branch(popped[k], *outs[k]) for k in popped}
-    Ks = torch.cat([sts[k]["nk"] for k in sts]).tolist()                  # one host read
-    for k, K in zip(sts, Ks):
-        babs[k].finish(sts[k], int(K))
+    vals = torch.cat([t for k in sts for t in (sts[k]["nk"].to(torch.float64), babs[k]._inc_dev)]).tolist()
+    for j, k in enumerate(sts):                                            # one host read above
+        babs[k].sync_incumbent(vals[2 * j + 1])
+        babs[k].finish(sts[k], int(vals[2 * j]))
     return sum(p[0].shape[0] for p in popped.values())
 
 
