@@ -63,6 +63,8 @@ def lib():
         L.gear_bab_split.restype = i32
         L.gear_queue_order.argtypes = [vp, vp, vp, i64, vp, i64, vp]
         L.gear_queue_order.restype = i32
+        L.gear_queue_merge.argtypes = [vp, vp, vp, i64, vp, i64, vp, vp]
+        L.gear_queue_merge.restype = i32
         L.gear_gather_rows.argtypes = [vp, vp, i64, i64, vp, vp]
         L.gear_gather_rows.restype = i32
         L.gear_scatter_rows.argtypes = [vp, vp, i64, i64, vp, vp]
@@ -115,4 +117,5 @@ EXPORTED = ("gear_dag_create", "gear_dag_destroy", "gear_crown_workspace_bytes",
             "gear_crown_lower_static", "gear_crown_static_scratch_bytes", "gear_constrained_workspace_bytes",
             "gear_constrained_lower", "gear_clip_domains", "gear_bab_child_keys", "gear_bab_compact",
             "gear_dual_lower_bound", "gear_crown_lower_ibp", "gear_crown_multi_workspace_bytes",
-            "gear_crown_lower_multi", "gear_crown_plain_workspace_bytes", "gear_crown_lower_plain")
+            "gear_crown_lower_multi", "gear_crown_plain_workspace_bytes", "gear_crown_lower_plain",
+            "gear_queue_merge")

@@ -47,7 +47,12 @@ class BaBStats:
 
 
 class DomainQueue:
-    """Device-resident pool of open subdomains (structure of arrays over slots)."""
+    """Device-resident pool of open subdomains (structure of arrays over slots).
+
+    The active slot list is kept in the reference's pop order, (objective key descending,
+    insertion id ascending): keys do not change while a domain is queued, so a push sorts only
+    the new domains and merges them in (gear_queue_merge), and a pop takes the list's tail, the
+    same batch a full sort of the open domains gives."""
 
     def __init__(self, n: int, S: int, capacity: int, device, cuts: bool = False):
         """cuts: also keep per domain the cut rows A (S, n), b (S) inherited from its parent."""
@@ -73,7 +78,8 @@ class DomainQueue:
                    hi=torch.empty(cap, self.n, dtype=torch.float64, device=dev),
                    key=torch.full((cap, self.S), math.inf, dtype=torch.float64, device=dev),
                    thr=torch.empty(cap, self.S, dtype=torch.float64, device=dev),
-                   ids=torch.zeros(cap, dtype=torch.int64, device=dev))
+                   ids=torch.zeros(cap, dtype=torch.int64, device=dev),
+                   key0=torch.full((cap,), math.inf, dtype=torch.float64, device=dev))
         if self.cuts:
             new["cutA"] = torch.empty(cap, self.S * self.n, dtype=torch.float64, device=dev)
             new["cutb"] = torch.empty(cap, self.S, dtype=torch.float64, device=dev)
@@ -104,25 +110,30 @@ class DomainQueue:
             src = vals[name].reshape(m, w).contiguous()
             _lib.check(L.gear_scatter_rows(_p(src), _p(slots), m, w, _p(getattr(self, name)), stream),
                        "gear_scatter_rows")
-        self.ids[slots.long()] = torch.arange(self.next_id, self.next_id + m, device=self.device)
+        sl = slots.long()
+        self.ids[sl] = torch.arange(self.next_id, self.next_id + m, device=self.device)
+        self.key0[sl] = key.reshape(m, self.S)[:, 0]
         self.next_id += m
-        self.active = torch.cat([self.active, slots])
+        # the new domains in pop order, merged into the ordered active list
+        n2 = 1 << max(0, (m - 1).bit_length())
+        order = torch.empty(max(n2, 1), dtype=torch.int32, device=self.device)
+        _lib.check(L.gear_queue_order(_p(self.key0), _p(self.ids), _p(slots), m, _p(order), order.numel(), stream),
+                   "gear_queue_order")
+        na = int(self.active.numel())
+        merged = torch.empty(na + m, dtype=torch.int32, device=self.device)
+        _lib.check(L.gear_queue_merge(_p(self.key0), _p(self.ids), _p(self.active) if na else None, na, _p(order), m,
+                                      _p(merged), stream), "gear_queue_merge")
+        self.active = merged
 
     def pop(self, batch: int):
-        """Sort by (objective key desc, id asc) and take the last `batch` domains. The returned
-        rows live in buffers the next pop reuses."""
+        """The last `batch` domains in (objective key desc, id asc) order: the tail of the ordered
+        active list. The returned rows live in buffers the next pop reuses."""
         N = len(self)
         b = min(batch, N)
-        n2 = 1 << max(0, (N - 1).bit_length())
-        order = torch.empty(max(n2, 1), dtype=torch.int32, device=self.device)
-        key0 = self.key[:, 0].contiguous()
         L = _lib.lib()
         stream = torch.cuda.current_stream(self.device).cuda_stream
-        _lib.check(L.gear_queue_order(_p(key0), _p(self.ids), _p(self.active), N, _p(order), order.numel(), stream),
-                   "gear_queue_order")
-        order = order[:N]
-        slots = order[N - b:].contiguous()
-        self.active = order[:N - b].contiguous()
+        slots = self.active[N - b:]
+        self.active = self.active[:N - b]
         out = []
         for name, w in self._fields():
             # popped rows live until the end of the iteration that pops them: reused buffers
@@ -137,15 +148,14 @@ class DomainQueue:
         return out
 
     def min_key(self) -> float:
-        if len(self) == 0:
-            return math.inf
-        return float(self.key[self.active.long(), 0].min())
+        return float(self.min_key_tensor())
 
     def min_key_tensor(self) -> torch.Tensor:
-        """min_key() as a (1,) device tensor (no host read)."""
+        """The smallest objective key of the open domains as a (1,) device tensor (no host
+        read): the key of the ordered list's last slot."""
         if len(self) == 0:
             return torch.full((1,), math.inf, dtype=torch.float64, device=self.device)
-        return self.key[self.active.long(), 0].min().reshape(1)
+        return self.key0[self.active[-1:].long()]
 
 
 class BaB:

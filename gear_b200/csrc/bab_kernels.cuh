@@ -241,6 +241,33 @@ __global__ void __launch_bounds__(SORT_THREADS) bitonic_smem(int32_t* idx, const
   for (int i = threadIdx.x; i < N2; i += SORT_THREADS) idx[i] = ix_s[i];
 }
 
+// Merge of two slot lists, each ordered by (key descending, id ascending), into one such list:
+// output position i takes its element from the co-rank split (merge path) found by binary search,
+// so every position is independent. Ids are unique, so the order is total and the result is the
+// one a full sort of the union gives.
+__global__ void merge_kernel(const double* key, const int64_t* id, const int32_t* a, int64_t na, const int32_t* b,
+                             int64_t nb, int32_t* out) {
+  const int64_t i = (int64_t)blockIdx.x * BT + threadIdx.x;
+  if (i >= na + nb) return;
+  // smallest j (elements taken from a among the first i outputs) with b[i-j-1] before a[j]
+  int64_t lo = i > nb ? i - nb : 0, hi = i < na ? i : na;
+  while (lo < hi) {
+    const int64_t j = (lo + hi) >> 1, k = i - j;
+    const int32_t bk = b[k - 1], aj = a[j];
+    if (before(key[bk], id[bk], key[aj], id[aj])) hi = j;
+    else lo = j + 1;
+  }
+  const int64_t j = lo, k = i - j;
+  bool take_a;
+  if (j >= na) take_a = false;
+  else if (k >= nb) take_a = true;
+  else {
+    const int32_t aj = a[j], bk = b[k];
+    take_a = before(key[aj], id[aj], key[bk], id[bk]);
+  }
+  out[i] = take_a ? a[j] : b[k];
+}
+
 __global__ void bitonic_step(int32_t* idx, const double* key, const int64_t* id, int64_t N2, int64_t N, int j,
                              int k) {
   int64_t i = (int64_t)blockIdx.x * BT + threadIdx.x;

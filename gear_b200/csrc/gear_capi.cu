@@ -716,6 +716,19 @@ extern "C" int gear_queue_order(const double* key, const int64_t* id, const int3
   return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_queue_order");
 }
 
+extern "C" int gear_queue_merge(const double* key, const int64_t* id, const int32_t* a, int64_t na, const int32_t* b,
+                                int64_t nb, int32_t* out, void* stream) {
+  using namespace gear::bab;
+  if (!key || !id || !out || na < 0 || nb < 0 || (na > 0 && !a) || (nb > 0 && !b))
+    return fail(GEAR_E_INVALID, "gear_queue_merge: %s", "bad arguments");
+  g_launches = 0;
+  if (na + nb == 0) return GEAR_OK;
+  merge_kernel<<<grid_for(na + nb), BT, 0, (cudaStream_t)stream>>>(key, id, a, na, b, nb, out);
+  g_launches = 1;
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_queue_merge");
+}
+
 extern "C" int gear_gather_rows(const double* src, const int32_t* rows, int64_t count, int64_t width, double* dst,
                                 void* stream) {
   if (!src || !rows || !dst || count < 0 || width < 1) return fail(GEAR_E_INVALID, "gear_gather_rows: %s", "bad arguments");

@@ -116,6 +116,14 @@ int gear_bab_split(const double* lo, const double* hi, const int32_t* kept, int6
 int gear_queue_order(const double* key, const int64_t* id, const int32_t* slots, int64_t count, int32_t* order,
                      int64_t order_len, void* stream);
 
+/* Merge two slot lists a (na) and b (nb), each ordered by (key[slot] descending, id[slot]
+ * ascending), into out (na + nb) in that order: the order gear_queue_order gives their union. A
+ * queue kept in this order pops its batch from the tail with no sort (the reference re-sorts its
+ * domain list, branching_domains.py:831-962); new domains are sorted (gear_queue_order) and
+ * merged in. key, id: indexed by slot. */
+int gear_queue_merge(const double* key, const int64_t* id, const int32_t* a, int64_t na, const int32_t* b, int64_t nb,
+                     int32_t* out, void* stream);
+
 /* dst[i, :] = src[rows[i], :] and dst[rows[i], :] = src[i, :] for float64 rows of `width`. */
 int gear_gather_rows(const double* src, const int32_t* rows, int64_t count, int64_t width, double* dst,
                      void* stream);

@@ -129,3 +129,30 @@ def test_queue_order_single_and_multi_launch(N):
     torch.cuda.synchronize()
     ref = slots[np.lexsort((ids[slots], -key[slots]))]
     assert np.array_equal(order[:n].cpu().numpy(), ref)
+
+
+def test_ordered_queue_pops_what_a_full_sort_pops():
+    """Pushes merged into the ordered list and pops from its tail give, batch by batch, what a
+    full sort of the open domains by (key descending, id ascending) gives; keys with many ties."""
+    from gear_b200.bab import DomainQueue
+    g = torch.Generator().manual_seed(7)
+    n, S = 3, 2
+    q = DomainQueue(n, S, 16, "cuda")
+    ref = []                                           # (key, id) of the open domains
+    next_id = 0
+    for rnd in range(12):
+        m = int(torch.randint(1, 3000, (1,), generator=g))
+        key = torch.randint(-5, 5, (m, S), generator=g).to(torch.float64) / 2
+        key[::7, 0] = float("-inf")
+        lo = torch.rand(m, n, generator=g, dtype=torch.float64)
+        q.push(lo.cuda(), (lo + 1).cuda(), key.cuda(), torch.zeros(m, S, dtype=torch.float64, device="cuda"))
+        ref += [(float(key[i, 0]), next_id + i) for i in range(m)]
+        next_id += m
+        b = int(torch.randint(1, 2500, (1,), generator=g))
+        popped = q.pop(b)
+        ref.sort(key=lambda t: (-t[0], t[1]))
+        want, ref = ref[len(ref) - min(b, len(ref)):], ref[:len(ref) - min(b, len(ref))]
+        got = popped[2][:, 0].cpu().tolist()
+        assert got == [k for k, _ in want]
+        assert len(q) == len(ref)
+        assert float(q.min_key_tensor()) == (min(k for k, _ in ref) if ref else float("inf"))
