@@ -258,7 +258,8 @@ class BaB:
                                                                                 device=self.device)
         obj = torch.where(feas, y[:, 0], torch.full_like(y[:, 0], math.inf))
         best = obj.min(0)
-        return best.values.reshape(1), x[best.indices]
+        # index_select keeps the index on the device (x[tensor] would read it on the host)
+        return best.values.reshape(1), x.index_select(0, best.indices.reshape(1)).reshape(-1)
 
     def propose_incumbent(self, x: torch.Tensor):
         """Fold the best feasible point among x into the device-side incumbent (no host read)."""
