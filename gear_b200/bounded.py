@@ -95,7 +95,8 @@ class BoundedModule:
             with torch.cuda.device(self.device):
                 eng = CrownEngine(self.graph, spec_rows=spec_rows, dense_c=dense_c,
                                   mode=self.bound_opts.get("gear_mode", "auto"),
-                                  cta_threads=int(self.bound_opts.get("gear_cta_threads", 128)))
+                                  cta_threads=int(self.bound_opts.get("gear_cta_threads", 128)),
+                                  tie_rule=self.bound_opts.get("gear_tie_rule", "reference"))
             self._engines[key] = eng
         return eng
 

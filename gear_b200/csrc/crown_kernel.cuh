@@ -36,7 +36,7 @@ constexpr double THREE_HALF_PI = 3 * PI / 2;
 constexpr double EPS = 2.220446049250313e-16;   // float64 machine epsilon
 constexpr double UNIT = EPS / 2;
 constexpr double EPSILON = 1e-12;               // operators/base.py:32
-constexpr double TIE_TOL = 1e-12;               // McCormick tie tolerance (see program.py)
+constexpr double TIE_TOL = 1e-12;               // McCormick tie tolerance of the "exact" tie rule
 constexpr double STEP_PRE = 0.01;
 // The box-per-CTA kernel is instantiated for 64, 128 and 256 threads per CTA (template
 // parameter NT of every function below that splits work over the CTA); the program picks one.
@@ -294,23 +294,39 @@ __device__ void relax_cos(const double* T, double l, double u, double* p) {
   p[3] = p[3] + p[2] * hp;
 }
 
-__device__ void relax_mul(double xl, double xu, double yl, double yu, double* p) {
-  auto amin = [&](double a, double b, double c) {
-    return a * (a >= 0 ? xl : xu) + b * (b >= 0 ? yl : yu) + c;
-  };
-  auto amax = [&](double a, double b, double c) {
-    return a * (a >= 0 ? xu : xl) + b * (b >= 0 ? yu : yl) + c;
-  };
-  double m1 = amin(yl, xl, -xl * yl), m2 = amin(yu, xu, -xu * yu);
-  double M1 = amax(yu, xl, -yu * xl), M2 = amax(yl, xu, -yl * xu);
-  double r_l = (m1 >= m2 - TIE_TOL * (fabs(m1) + fabs(m2))) ? 1.0 : 0.0;
-  double r_u = (M1 <= M2 + TIE_TOL * (fabs(M1) + fabs(M2))) ? 1.0 : 0.0;
-  p[0] = (yl - yu) * r_l + yu;
-  p[1] = (xl - xu) * r_l + xu;
-  p[2] = (yu * xu - yl * xl) * r_l - yu * xu;
-  p[3] = (yu - yl) * r_u + yl;
-  p[4] = (xl - xu) * r_u + xu;
-  p[5] = (yl * xu - yu * xl) * r_u - yl * xu;
+// Box minimum (maximum) of the plane a x + b y + c, rounded op by op in the reference's order
+// (BoundMul._affine_min_box: a * x_min + b * y_min + c, operators/bivariate.py:206-217): the
+// plane choice compares two such values, so no product may be contracted into an FMA.
+__device__ __forceinline__ double plane_min(double a, double b, double c, double xl, double xu, double yl,
+                                            double yu) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(a, a >= 0 ? xl : xu), __dmul_rn(b, b >= 0 ? yl : yu)), c);
+}
+__device__ __forceinline__ double plane_max(double a, double b, double c, double xl, double xu, double yl,
+                                            double yu) {
+  return __dadd_rn(__dadd_rn(__dmul_rn(a, a >= 0 ? xu : xl), __dmul_rn(b, b >= 0 ? yu : yl)), c);
+}
+
+// McCormick planes with the coefficient-aware pick (BoundMul._compute_coeff_aware_r,
+// operators/bivariate.py:219-250, and interpolated_relaxation :66-75). exact_ties = 0 is the
+// reference's float comparison min_p1l >= min_p2l (max_p1u <= max_p2u); exact_ties = 1 counts a
+// relative difference below TIE_TOL as a tie and picks plane 1, the exact-arithmetic outcome of
+// that comparison (the planes of a tie have the same box minimum, so the choice is then
+// independent of the last bits of the intermediate bounds).
+__device__ void relax_mul(double xl, double xu, double yl, double yu, double* p, int exact_ties) {
+  const double m1 = plane_min(yl, xl, __dmul_rn(-xl, yl), xl, xu, yl, yu);
+  const double m2 = plane_min(yu, xu, __dmul_rn(-xu, yu), xl, xu, yl, yu);
+  const double M1 = plane_max(yu, xl, __dmul_rn(-yu, xl), xl, xu, yl, yu);
+  const double M2 = plane_max(yl, xu, __dmul_rn(-yl, xu), xl, xu, yl, yu);
+  const double tl = exact_ties ? TIE_TOL * (fabs(m1) + fabs(m2)) : 0.0;
+  const double tu = exact_ties ? TIE_TOL * (fabs(M1) + fabs(M2)) : 0.0;
+  const double r_l = (m1 >= m2 - tl) ? 1.0 : 0.0;
+  const double r_u = (M1 <= M2 + tu) ? 1.0 : 0.0;
+  p[0] = __dadd_rn(__dmul_rn(__dsub_rn(yl, yu), r_l), yu);
+  p[1] = __dadd_rn(__dmul_rn(__dsub_rn(xl, xu), r_l), xu);
+  p[2] = __dsub_rn(__dmul_rn(__dsub_rn(__dmul_rn(yu, xu), __dmul_rn(yl, xl)), r_l), __dmul_rn(yu, xu));
+  p[3] = __dadd_rn(__dmul_rn(__dsub_rn(yu, yl), r_u), yl);
+  p[4] = __dadd_rn(__dmul_rn(__dsub_rn(xl, xu), r_u), xu);
+  p[5] = __dsub_rn(__dmul_rn(__dsub_rn(__dmul_rn(yl, xu), __dmul_rn(yu, xl)), r_u), __dmul_rn(yl, xu));
 }
 
 // Lower bound of specification row s over the output interval [lo, hi] (width wt), as the
@@ -747,7 +763,7 @@ __device__ void relax_node(const Box& bx, int v) {
       if (!(isfinite(xl) && isfinite(xu) && isfinite(yl) && isfinite(yu))) {
         for (int k = 0; k < 6; ++k) p[k] = NAN;
       } else {
-        relax_mul(xl, xu, yl, yu, p);
+        relax_mul(xl, xu, yl, yu, p, P->hdr[H_TIES]);
       }
     } else {
       const int32_t* a = node_rec(P, nd[N_IN0]);

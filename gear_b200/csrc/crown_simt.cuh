@@ -152,7 +152,7 @@ __device__ void simt_relax_node(const SBox& bx, int v) {
       if (!(isfinite(xl) && isfinite(xu) && isfinite(yl) && isfinite(yu))) {
         for (int k = 0; k < 6; ++k) q[k] = NAN;
       } else {
-        relax_mul(xl, xu, yl, yu, q);
+        relax_mul(xl, xu, yl, yu, q, P->hdr[H_TIES]);
       }
       for (int k = 0; k < 6; ++k) pl[6 * j + k] = q[k];
     } else {

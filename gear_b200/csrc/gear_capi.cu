@@ -304,10 +304,14 @@ extern "C" int64_t gear_crown_static_scratch_bytes(void) { return kStaticScratch
 extern "C" int gear_crown_lower_static(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
                                        const double* C, double* lb, double* lA, double* lbias, void* stream) {
   g_launches = 0;
-  if (!dag || !x_L || !x_U || !lb || batch < 0) return fail(GEAR_E_INVALID, "gear_crown_lower_static: %s", "bad arguments");
+  // the same argument checks, in the same order, as gear_crown_lower
+  if (!dag || batch < 0) return fail(GEAR_E_INVALID, "gear_crown_lower_static: %s", "bad arguments");
+  if (batch == 0) return GEAR_OK;             // empty arrays may come with null pointers
+  if (!x_L || !x_U || !lb) return fail(GEAR_E_INVALID, "gear_crown_lower_static: %s", "bad arguments");
+  if (dag->hdr[gear::H_RETA] == 0 && lA)
+    return fail(GEAR_E_INVALID, "gear_crown_lower_static: %s", "program built without A");
   if (dag->hdr[gear::H_RETA] != 0 && dag->hdr[gear::H_X_IN_LA] != 0 && !lA)
     return fail(GEAR_E_INVALID, "gear_crown_lower_static: %s", "this program accumulates A in the lA output: lA is required");
-  if (batch == 0) return GEAR_OK;
   const int64_t slot_bytes = dag->slot_doubles * (int64_t)sizeof(double);
   const int64_t max_slots = kStaticScratchBytes / slot_bytes;
   if (max_slots < 1) {

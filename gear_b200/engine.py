@@ -40,8 +40,9 @@ def smem_class(prog) -> int:
 class _Dag:
     """One compiled program uploaded to the device (a gear_dag handle)."""
 
-    def __init__(self, graph, spec_rows, dense_c, mode, cta_threads):
-        self._upload(Program(graph, spec_rows=spec_rows, dense_c=dense_c, mode=mode, cta_threads=cta_threads))
+    def __init__(self, graph, spec_rows, dense_c, mode, cta_threads, tie_rule="reference"):
+        self._upload(Program(graph, spec_rows=spec_rows, dense_c=dense_c, mode=mode, cta_threads=cta_threads,
+                             tie_rule=tie_rule))
 
     def _upload(self, prog):
         self.prog = p = prog
@@ -85,10 +86,11 @@ class CrownEngine:
 
     mode "cta" runs one box per CTA (cta_threads threads), "simt" one box per thread; both
     give the same bounds. mode "auto" times the kernel variants on the first call for each
-    batch size class (powers of two) on the caller's own boxes and keeps the fastest."""
+    batch size class (powers of two) on the caller's own boxes and keeps the fastest.
+    tie_rule: the McCormick tie rule of the compiled programs (``Program``)."""
 
     def __init__(self, graph: Graph, spec_rows: Optional[int] = None, dense_c: bool = False, mode: str = "auto",
-                 cta_threads: int = 128):
+                 cta_threads: int = 128, tie_rule: str = "reference"):
         if not torch.cuda.is_available():
             raise _lib.GearError("gear_b200 needs a CUDA device (no CPU fallback)")
         if mode not in ("auto", "cta", "simt"):
@@ -97,6 +99,7 @@ class CrownEngine:
         self.mode = mode
         self.dense_c = dense_c
         self._args = (graph, spec_rows, dense_c)
+        self.tie_rule = tie_rule
         self._dags = {}
         first = ("cta", cta_threads) if mode == "auto" else (mode, cta_threads)
         d = self._dag(*first)
@@ -111,7 +114,7 @@ class CrownEngine:
     def _dag(self, mode, threads):
         key = (mode, threads if mode == "cta" else 0)
         if key not in self._dags:
-            self._dags[key] = _Dag(*self._args, mode, threads)
+            self._dags[key] = _Dag(*self._args, mode, threads, self.tie_rule)
         return self._dags[key]
 
     def _candidates(self):
@@ -252,7 +255,7 @@ class MultiEngine:
     their grid for the whole GPU compete for it (measured 11% slower on the mixed family)."""
 
     def __init__(self, graphs, mode: str = "auto", cta_threads: int = 256, simt_items_max: int = SIMT_PACK_ITEMS,
-                 programs=None, concurrent: bool = False):
+                 programs=None, concurrent: bool = False, tie_rule: str = "reference"):
         if not torch.cuda.is_available():
             raise _lib.GearError("gear_b200 needs a CUDA device (no CPU fallback)")
         if mode not in ("auto", "cta", "simt"):
@@ -269,7 +272,7 @@ class MultiEngine:
             else:
                 var = ("simt", 0) if mode == "simt" else ("cta", cta_threads)
                 if mode == "auto":
-                    probe = Program(g, mode="simt")
+                    probe = Program(g, mode="simt", tie_rule=tie_rule)
                     items = 3 * probe.arena_w + probe.plane_w + probe.fold_w + 4 * probe.maxw + probe.simt_buf + \
                         probe.simt_rows
                     var = ("simt", 0) if items <= simt_items_max else ("cta", cta_threads)
@@ -278,7 +281,7 @@ class MultiEngine:
                     prog = None
                 if prog is None:
                     prog = Program(g, mode=var[0], cta_threads=var[1] if var[0] == "cta" else 128,
-                                   smem_limit=PACK_SMEM_LIMIT)
+                                   smem_limit=PACK_SMEM_LIMIT, tie_rule=tie_rule)
             self.dags.append(_Dag.from_program(prog))
             # a launch also needs one pass working-set placement (shared or global memory); the
             # fourth field is the shared-memory size class
@@ -408,10 +411,11 @@ class PlainEngine:
     launch per op plus one for its initial A and one for its concretisation, with every box's
     state in global memory between launches. The baseline the fused launch is measured against."""
 
-    def __init__(self, graph: Graph, cta_threads: int = 128):
+    def __init__(self, graph: Graph, cta_threads: int = 128, tie_rule: str = "reference"):
         if not torch.cuda.is_available():
             raise _lib.GearError("gear_b200 needs a CUDA device (no CPU fallback)")
-        self.dag = _Dag.from_program(Program(graph, mode="cta", cta_threads=cta_threads, smem_limit=0))
+        self.dag = _Dag.from_program(Program(graph, mode="cta", cta_threads=cta_threads, smem_limit=0,
+                                             tie_rule=tie_rule))
         self.prog = self.dag.prog
         self.n, self.S = self.prog.n, self.prog.S
         self._ws = None

@@ -67,7 +67,10 @@ ROOT_IN_LA = -2     # buffer marker: the input's A of a final pass accumulates i
 
 PLANES_PER_ELEM = {"mul": 6, "sqr": 4, "exp": 4, "log": 4, "sin": 4, "cos": 4, "pow": 4}
 
-TIE_TOL = 1e-12
+# McCormick tie rules (header field H_TIES): "reference" is the reference's float comparison of
+# the two candidate planes' box minima (bivariate.py:250); "exact" counts a relative difference
+# below 1e-12 as a tie and picks plane 1 (deterministic across summation orders)
+TIE_RULES = {"reference": 0, "exact": 1}
 
 
 class ProgramError(ValueError):
@@ -124,12 +127,20 @@ class Program:
 
     def __init__(self, graph: Graph, spec_rows: Optional[int] = None, dense_c: bool = False,
                  return_a: bool = True, smem_limit: int = 232448, mode: str = "cta",
-                 cta_threads: int = 128):
+                 cta_threads: int = 128, tie_rule: str = "reference"):
         """mode: "cta" runs one box per CTA with the pass working set in shared memory, and the
         final pass accumulates the input's A directly in the lA output; "simt" runs one box per
         thread with every per-box array box-interleaved in global scratch, and writes lA from the
         pass buffers at the end. smem_limit: bytes of shared memory one CTA may use (the sm_100
-        opt-in maximum); a box-per-CTA pass working set beyond it lives in global scratch."""
+        opt-in maximum); a box-per-CTA pass working set beyond it lives in global scratch.
+        tie_rule: how the coefficient-aware McCormick pick decides between two candidate planes
+        whose box minima are equal in exact arithmetic (x entirely negative and y entirely
+        positive, or the reverse): "reference" compares the two rounded minima as the reference
+        does (bivariate.py:250; the outcome then follows the last bits of the intermediate
+        bounds), "exact" picks plane 1, the exact-arithmetic outcome."""
+        if tie_rule not in TIE_RULES:
+            raise ProgramError(f"unknown tie rule {tie_rule!r}")
+        self.tie_rule = tie_rule
         if mode not in MODES:
             raise ProgramError(f"unknown execution mode {mode!r}")
         if cta_threads not in (64, 128, 256):
@@ -498,7 +509,7 @@ class Program:
                                 self.smem_total, self.max_S, self.sin_off, self.maxw,
                                 1 if self.return_a else 0, max_ops, self.simt_buf, self.simt_rows,
                                 1 if self.x_in_la else 0, MODES[self.mode], self.cta_threads, self.pass_global,
-                                0, 0],
+                                TIE_RULES[self.tie_rule], 0],
                                dtype=np.int32)
 
     def _emit_pass(self, pid, pi: PassInfo):
@@ -770,7 +781,7 @@ class Program:
 
 
 # ===================================================================== compile pools
-_KEEP = ("S", "n", "t", "mode", "cta_threads", "x_in_la", "return_a", "dense_c", "arena_w", "plane_w", "fold_w", "maxw",
+_KEEP = ("S", "n", "t", "mode", "cta_threads", "tie_rule", "x_in_la", "return_a", "dense_c", "arena_w", "plane_w", "fold_w", "maxw",
          "max_S", "max_smem", "smem_total", "pass_global", "simt_buf", "simt_rows", "sin_off", "work", "header",
          "node_arr", "step_arr", "pass_arr", "op_arr", "int_pool", "dbl_pool")
 
@@ -794,7 +805,7 @@ def _compile_job(job):
     graph, kw, simt_items_max = job
     if simt_items_max is not None:
         # "auto": one box per thread when the per-box state is small, else one box per CTA
-        prog = Program(graph, mode="simt")
+        prog = Program(graph, mode="simt", tie_rule=kw.get("tie_rule", "reference"))
         if simt_items(prog) <= simt_items_max:
             return stripped(prog)
     return stripped(Program(graph, **kw))

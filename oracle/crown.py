@@ -417,10 +417,11 @@ class SinRelax:
         return lw, lb + lw * hp, uw, ub + uw * hp
 
 
-TIE_TOL = 1e-12
+# tie tolerance of the "exact" McCormick tie rule (the reference's rule is tie_tol = 0)
+EXACT_TIE_TOL = 1e-12
 
 
-def relax_mul(xl, xu, yl, yu, tie_tol=TIE_TOL):
+def relax_mul(xl, xu, yl, yu, tie_tol=0.0):
     """McCormick with the coefficient-aware pick (bivariate.py:206-247, 38-77).
 
     Where both candidate planes have the same box minimum (maximum) in exact arithmetic --
@@ -578,7 +579,7 @@ def _nan_to_inf(lo, hi):
 class CrownOracle:
     """compute_bounds(method='CROWN') over a batch of boxes for a ``gear_b200.graph.Graph``."""
 
-    def __init__(self, graph, tie_tol=TIE_TOL, inject=None):
+    def __init__(self, graph, tie_tol=0.0, inject=None):
         """inject: {node id: (lo, hi)} replaces the computed bounds of those nodes (used to
         check the restatement against recorded reference intermediates)."""
         self.tie_tol = tie_tol

@@ -8,6 +8,18 @@ return_A=True) in float64 on CPU with the hot-path bound options of the referenc
 GEAR configuration (fp_enclosure.affine_backward, compare_crown_with_ibp_intermediate,
 undefined_relaxation_rows/interval, domain_aware_ops), and stores x_L, x_U, C, lb, lA,
 lbias plus the order of CROWN intermediate passes (node kind and width).
+
+Two more records per case:
+
+* ``lb_exact``, ``lA_exact``, ``lbias_exact``: the same call with the reference's McCormick
+  plane pick (BoundMul._compute_coeff_aware_r, operators/bivariate.py:219-257) decided in exact
+  arithmetic -- a relative difference of the two candidates' box minima (maxima) below 1e-12
+  counts as a tie and picks plane 1. This is the outcome of the reference's comparison
+  whenever its operands are exact; it differs from the float comparison only where the two
+  planes tie and rounding noise in the intermediate bounds decides.
+* ``lb_ulp_dev``: per row, the largest relative change of the reference's lb over three runs on
+  the boxes widened by one ulp (x_L down, x_U up, both). Rows where it exceeds 1e-5 are decided
+  by such ties: the reference itself does not determine them to that tolerance.
 """
 import os
 import sys
@@ -45,6 +57,23 @@ def _stub_modules():
     sys.modules.setdefault("graphviz", graphviz)
 
 
+def exact_tie_rule(BoundMul):
+    """A replacement for BoundMul._compute_coeff_aware_r that decides ties in exact arithmetic."""
+    tol = 1e-12
+
+    def rule(self, x_l, x_u, y_l, y_u):
+        xl, xu = x_l + torch.zeros_like(y_l), x_u + torch.zeros_like(y_u)
+        yl, yu = y_l + torch.zeros_like(x_l), y_u + torch.zeros_like(x_u)
+        m1 = BoundMul._affine_min_box(yl, xl, -xl * yl, xl, xu, yl, yu)
+        m2 = BoundMul._affine_min_box(yu, xu, -xu * yu, xl, xu, yl, yu)
+        M1 = BoundMul._affine_max_box(yu, xl, -yu * xl, xl, xu, yl, yu)
+        M2 = BoundMul._affine_max_box(yl, xu, -yl * xu, xl, xu, yl, yu)
+        r_l = (m1 >= m2 - tol * (m1.abs() + m2.abs())).to(xl.dtype)
+        r_u = (M1 <= M2 + tol * (M1.abs() + M2.abs())).to(xl.dtype)
+        return r_l, r_u
+    return rule
+
+
 def map_nodes(bm, g):
     """Pair reference Bound nodes with IR node ids by walking both DAGs from the output
     (perturbed inputs in order); the IR keeps one node per perturbed reference node."""
@@ -69,6 +98,9 @@ def main(ref_root):
     torch.set_num_threads(1)
     from auto_LiRPA import BoundedModule, BoundedTensor, PerturbationLpNorm
     import auto_LiRPA.bound_general as bg
+    from auto_LiRPA.operators.bivariate import BoundMul
+    float_rule = BoundMul._compute_coeff_aware_r
+    exact_rule = exact_tie_rule(BoundMul)
     from gear_b200 import problems, graph
     import models
 
@@ -113,12 +145,26 @@ def main(ref_root):
         bm = BoundedModule(model, torch.zeros(2, n), bound_opts=BOUND_OPTS, device='cpu')
         S = bm.final_node().output_shape[1]
         C = torch.eye(S).unsqueeze(0).expand(lo.shape[0], S, S).contiguous()
-        x = BoundedTensor((lo + hi) / 2, PerturbationLpNorm(x_L=lo, x_U=hi))
-        passes.clear()
         need = {bm.output_name[0]: {bm.input_name[0]}}
-        lb, _, A = bm.compute_bounds(x=(x,), C=C, method='CROWN', bound_upper=False,
-                                     return_A=True, needed_A_dict=need)
-        rec = A[bm.output_name[0]][bm.input_name[0]]
+
+        def bound(lo_, hi_):
+            x = BoundedTensor((lo_ + hi_) / 2, PerturbationLpNorm(x_L=lo_, x_U=hi_))
+            lb_, _, A_ = bm.compute_bounds(x=(x,), C=C, method='CROWN', bound_upper=False,
+                                           return_A=True, needed_A_dict=need)
+            return lb_.detach(), A_[bm.output_name[0]][bm.input_name[0]]
+
+        BoundMul._compute_coeff_aware_r = exact_rule
+        lb_x, rec_x = bound(lo, hi)
+        BoundMul._compute_coeff_aware_r = float_rule
+        dev = torch.zeros_like(lb_x)
+        down, up = torch.nextafter(lo, torch.tensor(-torch.inf)), torch.nextafter(hi, torch.tensor(torch.inf))
+        ulp = []
+        for plo, phi in ((down, hi), (lo, up), (down, up)):
+            ulp.append(bound(plo, phi)[0])
+        passes.clear()
+        lb, rec = bound(lo, hi)
+        for lp in ulp:
+            dev = torch.maximum(dev, (lp - lb).abs() / torch.clamp(lb.abs(), min=1.0))
         # intermediate bounds the reference kept, keyed by IR node id
         g = graph.trace(model, torch.zeros(2, n))
         inter = {}
@@ -132,9 +178,14 @@ def main(ref_root):
         out = os.path.join(HERE, f"crown_{name}_{inst}.npz")
         np.savez_compressed(out, x_L=lo.numpy(), x_U=hi.numpy(), C=C.numpy(), lb=lb.detach().numpy(),
                             lA=rec['lA'].detach().numpy(), lbias=rec['lbias'].detach().numpy(),
+                            lb_exact=lb_x.numpy(), lA_exact=rec_x['lA'].detach().numpy(),
+                            lbias_exact=rec_x['lbias'].detach().numpy(), lb_ulp_dev=dev.numpy(),
                             passes=np.array([f"{k}:{w}" for k, w in passes]), **inter)
-        print(name, inst, lb.shape, [f"{k}:{w}" for k, w in passes])
+        print(name, inst, lb.shape, [f"{k}:{w}" for k, w in passes],
+              f"rows the reference moves by > 1e-5 under one ulp: {int((dev > 1e-5).sum())}/{dev.numel()}")
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) < 2:
+        sys.exit(f"usage: python {os.path.basename(__file__)} REFERENCE_ROOT")
+    main(sys.argv[1])

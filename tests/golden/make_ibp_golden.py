@@ -57,4 +57,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) < 2:
+        sys.exit(f"usage: python {os.path.basename(__file__)} REFERENCE_ROOT")
+    main(sys.argv[1])

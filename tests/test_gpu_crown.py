@@ -1,6 +1,8 @@
-"""GPU CROWN (libgear_b200.so megakernel) against the float64 CPU oracle and the
-reference fixtures. Tolerances: 1e-9 relative against the oracle (same rounding model,
-same deterministic tie-break), soundness by sampling at the benchmark sizes."""
+"""GPU CROWN (libgear_b200.so megakernel) against the float64 CPU oracle. Tolerance: 1e-9
+relative (same rounding model). Both sides decide McCormick ties in exact arithmetic
+(tie_rule "exact"), so the comparison does not depend on the last bits of the two
+implementations' summation orders; the default rule is compared with the reference's own
+outputs in test_gpu_reference.py."""
 import numpy as np
 import pytest
 import torch
@@ -8,7 +10,7 @@ import torch
 from golden_cases import cases, load
 from gear_b200 import BoundedModule, BoundedTensor, PerturbationLpNorm, problems
 from gear_b200.engine import CrownEngine
-from oracle.crown import CrownOracle
+from oracle.crown import CrownOracle, EXACT_TIE_TOL
 
 pytestmark = pytest.mark.gpu
 RTOL = 1e-9
@@ -26,12 +28,12 @@ def _close(a, b, rtol=RTOL):
 def test_gpu_matches_oracle_on_fixture_boxes(case, threads):
     """Every box-per-CTA kernel instance (64, 128, 256 threads) against the oracle."""
     m, g, d, inject = load(case)
-    eng = CrownEngine(g, mode="cta", cta_threads=threads)
+    eng = CrownEngine(g, mode="cta", cta_threads=threads, tie_rule="exact")
     lo = torch.tensor(d["x_L"], device="cuda")
     hi = torch.tensor(d["x_U"], device="cuda")
     lb, lA, lbias = eng.lower(lo, hi)
     torch.cuda.synchronize()
-    o = CrownOracle(g)
+    o = CrownOracle(g, tie_tol=EXACT_TIE_TOL)
     olb, _, olA, olbias = o.compute_bounds(d["x_L"], d["x_U"], d["C"])
     assert _close(lb.cpu().numpy(), olb) < RTOL
     # On a degenerate box a power's relaxation is a secant over the reference's 1e-8 widening:
@@ -49,13 +51,13 @@ def test_gpu_matches_oracle_on_fixture_boxes(case, threads):
 def test_gpu_matches_oracle_random_boxes(workload, batch):
     m = problems.make_instance(workload, 0)
     lo, hi = problems.make_boxes(workload, batch, 0)
-    bm = BoundedModule(m, lo[:2], device="cuda")
+    bm = BoundedModule(m, lo[:2], device="cuda", bound_opts={"gear_tie_rule": "exact"})
     x = BoundedTensor(lo.cuda(), PerturbationLpNorm(x_L=lo.cuda(), x_U=hi.cuda()))
     S = bm.final_node_width()
     C = torch.eye(S, dtype=torch.float64).expand(batch, S, S)
     lb, _, A = bm.compute_bounds(x=(x,), C=C.cuda(), method="CROWN", bound_upper=False, return_A=True)
     rec = A[bm.output_name[0]][bm.input_name[0]]
-    o = CrownOracle(bm.graph)
+    o = CrownOracle(bm.graph, tie_tol=EXACT_TIE_TOL)
     olb, _, olA, olbias = o.compute_bounds(lo.numpy(), hi.numpy(), C.numpy())
     assert _close(lb.cpu().numpy(), olb) < RTOL
     assert _close(rec["lA"].cpu().numpy(), olA) < RTOL
@@ -83,7 +85,7 @@ def test_auto_engine_picks_a_variant_and_matches_oracle(workload, batch):
     m = problems.make_instance(workload, 0)
     lo, hi = problems.make_boxes(workload, batch, 0)
     g = graph.trace(m, lo[:2])
-    eng = CrownEngine(g, mode="auto")
+    eng = CrownEngine(g, mode="auto", tie_rule="exact")
     first = eng.lower(lo.cuda(), hi.cuda())
     second = eng.lower(lo.cuda(), hi.cuda())
     torch.cuda.synchronize()
@@ -91,7 +93,7 @@ def test_auto_engine_picks_a_variant_and_matches_oracle(workload, batch):
     assert len(eng.timings) == 1
     for a, b in zip(first, second):
         assert torch.equal(a, b)           # same variant, same arithmetic: bit-identical
-    olb, _, olA, olbias = CrownOracle(g).compute_bounds(lo.numpy(), hi.numpy())
+    olb, _, olA, olbias = CrownOracle(g, tie_tol=EXACT_TIE_TOL).compute_bounds(lo.numpy(), hi.numpy())
     assert _close(first[0].cpu().numpy(), olb) < RTOL
     assert _close(first[1].cpu().numpy(), olA) < RTOL
 

@@ -83,3 +83,36 @@ def test_empty_bab_steps():
                                   ws.numel(), st), "compact")
     torch.cuda.synchronize()
     assert int(nk.item()) == 0
+
+
+def test_static_entry_argument_checks():
+    """gear_crown_lower_static checks its arguments like gear_crown_lower: an empty batch with
+    null pointers is accepted, an lA output for a program compiled without A is rejected."""
+    from gear_b200 import _lib
+    from gear_b200.engine import _Dag
+    from gear_b200.program import Program
+    L = _lib.lib()
+    m, g = _graph()
+    st = torch.cuda.current_stream().cuda_stream
+    with_a = _Dag.from_program(Program(g, mode="cta"))
+    for fn in ("gear_crown_lower_static",):
+        assert getattr(L, fn)(with_a.handle, None, None, 0, None, None, None, None, st) == 0
+    no_a = _Dag.from_program(Program(g, mode="cta", return_a=False))
+    lo, hi = problems.make_boxes("quad_exp_n10", 4, 0)
+    xL, xU = lo.cuda(), hi.cuda()
+    lb = torch.empty(4, 3, dtype=torch.float64, device="cuda")
+    lbias = torch.empty_like(lb)
+    lA = torch.empty(4, 3, 10, dtype=torch.float64, device="cuda")
+    assert L.gear_crown_lower_static(no_a.handle, xL.data_ptr(), xU.data_ptr(), 4, None, lb.data_ptr(),
+                                     lA.data_ptr(), lbias.data_ptr(), st) == -1
+    ws = torch.empty(int(L.gear_crown_workspace_bytes(no_a.handle, 4)), dtype=torch.uint8, device="cuda")
+    assert L.gear_crown_lower(no_a.handle, xL.data_ptr(), xU.data_ptr(), 4, None, lb.data_ptr(), lA.data_ptr(),
+                              lbias.data_ptr(), ws.data_ptr(), ws.numel(), st) == -1
+    # without lA both entry points run and agree
+    assert L.gear_crown_lower_static(no_a.handle, xL.data_ptr(), xU.data_ptr(), 4, None, lb.data_ptr(),
+                                     None, lbias.data_ptr(), st) == 0
+    lb2 = torch.empty_like(lb)
+    assert L.gear_crown_lower(no_a.handle, xL.data_ptr(), xU.data_ptr(), 4, None, lb2.data_ptr(), None,
+                              lbias.data_ptr(), ws.data_ptr(), ws.numel(), st) == 0
+    torch.cuda.synchronize()
+    assert torch.equal(lb, lb2)

@@ -1,6 +1,6 @@
 """Many instances in one launch (gear_crown_lower_multi / MultiEngine): every instance's
 results are bit-identical to the same program launched alone, and agree with the oracle
-(1e-9 relative). Also the box-per-CTA program whose pass working set lives in global scratch:
+(1e-9 relative; McCormick ties decided in exact arithmetic on both sides, tie_rule "exact"). Also the box-per-CTA program whose pass working set lives in global scratch:
 identical to the shared-memory one."""
 import numpy as np
 import pytest
@@ -9,7 +9,7 @@ import torch
 from gear_b200 import _lib, graph, problems
 from gear_b200.engine import CrownEngine, MultiEngine, _Dag
 from gear_b200.program import Program
-from oracle.crown import CrownOracle
+from oracle.crown import CrownOracle, EXACT_TIE_TOL
 
 pytestmark = pytest.mark.gpu
 RTOL = 1e-9
@@ -39,7 +39,7 @@ def _instances():
 @pytest.mark.parametrize("mode", ["auto", "cta", "simt"])
 def test_multi_equals_alone_and_oracle(mode):
     graphs, boxes = _instances()
-    me = MultiEngine(graphs, mode=mode, cta_threads=128)
+    me = MultiEngine(graphs, mode=mode, cta_threads=128, tie_rule="exact")
     dev_boxes = [(lo.cuda(), hi.cuda()) for lo, hi in boxes]
     outs = me.lower(dev_boxes)
     torch.cuda.synchronize()
@@ -50,11 +50,11 @@ def test_multi_equals_alone_and_oracle(mode):
         if lo.shape[0] == 0:
             continue
         var = me.variants[i]
-        alone = CrownEngine(g, mode=var[0], cta_threads=var[1] if var[0] == "cta" else 128)
+        alone = CrownEngine(g, mode=var[0], cta_threads=var[1] if var[0] == "cta" else 128, tie_rule="exact")
         lb1, lA1, lbias1 = alone.lower(dev_boxes[i][0], dev_boxes[i][1])
         torch.cuda.synchronize()
         assert torch.equal(lb, lb1) and torch.equal(lA, lA1) and torch.equal(lbias, lbias1)
-        olb, _, olA, olbias = CrownOracle(g).compute_bounds(lo.numpy(), hi.numpy())
+        olb, _, olA, olbias = CrownOracle(g, tie_tol=EXACT_TIE_TOL).compute_bounds(lo.numpy(), hi.numpy())
         assert _close(lb.cpu().numpy(), olb) < RTOL
         assert _close(lA.cpu().numpy(), olA) < RTOL
 

@@ -1,6 +1,7 @@
 """Box-per-thread CROWN kernel (crown_simt_kernel) against the float64 CPU oracle and against
-the box-per-CTA kernel. Tolerance: 1e-9 relative (same rounding model, same tie-break; the two
-kernels sum in different orders)."""
+the box-per-CTA kernel. Tolerance: 1e-9 relative (same rounding model; the two kernels sum in
+different orders, so McCormick ties are decided in exact arithmetic, tie_rule "exact", on every
+side of these comparisons)."""
 import numpy as np
 import pytest
 import torch
@@ -8,7 +9,7 @@ import torch
 from golden_cases import cases, load
 from gear_b200 import BoundedModule, BoundedTensor, PerturbationLpNorm, problems
 from gear_b200.engine import CrownEngine
-from oracle.crown import CrownOracle
+from oracle.crown import CrownOracle, EXACT_TIE_TOL
 
 pytestmark = pytest.mark.gpu
 RTOL = 1e-9
@@ -24,12 +25,12 @@ def _close(a, b, rtol=RTOL):
 @pytest.mark.parametrize("case", cases())
 def test_simt_matches_oracle_on_fixture_boxes(case):
     m, g, d, inject = load(case)
-    eng = CrownEngine(g, mode="simt")
+    eng = CrownEngine(g, mode="simt", tie_rule="exact")
     lo = torch.tensor(d["x_L"], device="cuda")
     hi = torch.tensor(d["x_U"], device="cuda")
     lb, lA, lbias = eng.lower(lo, hi)
     torch.cuda.synchronize()
-    olb, _, olA, olbias = CrownOracle(g).compute_bounds(d["x_L"], d["x_U"], d["C"])
+    olb, _, olA, olbias = CrownOracle(g, tie_tol=EXACT_TIE_TOL).compute_bounds(d["x_L"], d["x_U"], d["C"])
     assert _close(lb.cpu().numpy(), olb) < RTOL
     # On a degenerate box a power's relaxation is a secant over the reference's 1e-8 widening:
     # its slope amplifies the last-bit difference of pow (torch on the CPU vs CUDA) by ~1e8, so
@@ -47,13 +48,14 @@ def test_simt_matches_oracle_on_fixture_boxes(case):
 def test_simt_matches_oracle_random_boxes(workload, batch):
     m = problems.make_instance(workload, 0)
     lo, hi = problems.make_boxes(workload, batch, 0)
-    bm = BoundedModule(m, lo[:2], device="cuda", bound_opts={"gear_mode": "simt"})
+    bm = BoundedModule(m, lo[:2], device="cuda", bound_opts={"gear_mode": "simt", "gear_tie_rule": "exact"})
     x = BoundedTensor(lo.cuda(), PerturbationLpNorm(x_L=lo.cuda(), x_U=hi.cuda()))
     S = bm.final_node_width()
     C = torch.eye(S, dtype=torch.float64).expand(batch, S, S)
     lb, _, A = bm.compute_bounds(x=(x,), C=C.cuda(), method="CROWN", bound_upper=False, return_A=True)
     rec = A[bm.output_name[0]][bm.input_name[0]]
-    olb, _, olA, olbias = CrownOracle(bm.graph).compute_bounds(lo.numpy(), hi.numpy(), C.numpy())
+    olb, _, olA, olbias = CrownOracle(bm.graph, tie_tol=EXACT_TIE_TOL).compute_bounds(lo.numpy(), hi.numpy(),
+                                                                                       C.numpy())
     assert _close(lb.cpu().numpy(), olb) < RTOL
     assert _close(rec["lA"].cpu().numpy(), olA) < RTOL
     assert _close(rec["lbias"].cpu().numpy(), olbias) < RTOL
@@ -80,8 +82,8 @@ def test_simt_matches_cta_kernel(workload, batch):
     from gear_b200 import graph
     g = graph.trace(m, lo[:2])
     xL, xU = lo.cuda(), hi.cuda()
-    a = CrownEngine(g, mode="cta").lower(xL, xU)
-    b = CrownEngine(g, mode="simt").lower(xL, xU)
+    a = CrownEngine(g, mode="cta", tie_rule="exact").lower(xL, xU)
+    b = CrownEngine(g, mode="simt", tie_rule="exact").lower(xL, xU)
     torch.cuda.synchronize()
     for x, y in zip(a, b):
         assert _close(y.cpu().numpy(), x.cpu().numpy()) < RTOL

@@ -3,14 +3,15 @@
 The fixtures hold the reference's compute_bounds(method='CROWN') outputs and the
 intermediate bounds it kept. With those intermediates injected (tie_tol=0, the
 reference's float comparison) the oracle must reproduce lb / lA / lbias; its own
-intermediates must match the recorded ones. With its default deterministic McCormick
-tie-break it must stay sound against sampling and match the reference wherever no tie
-decides a plane."""
+intermediates must match the recorded ones. With its own intermediates it must match the
+reference's exact-tie run on every row (tie_tol = EXACT_TIE_TOL) and the plain run on every
+row the reference determines to 1e-5 under a one-ulp change of its boxes (lb_ulp_dev), and
+stay sound against sampling."""
 import numpy as np
 import pytest
 
 from golden_cases import cases, load
-from oracle.crown import CrownOracle
+from oracle.crown import CrownOracle, EXACT_TIE_TOL
 
 
 @pytest.mark.parametrize("case", cases())
@@ -22,6 +23,29 @@ def test_oracle_matches_reference_with_injected_intermediates(case):
     assert np.all(np.abs(lb - d["lb"]) / scale < 1e-9)
     assert np.abs(lA - d["lA"]).max() <= 1e-9 * max(1.0, np.abs(d["lA"]).max())
     assert np.all(np.abs(lbias - d["lbias"]) / np.maximum(1.0, np.abs(d["lbias"])) < 1e-9)
+
+
+def _rel(a, b):
+    same_inf = np.isinf(a) & np.isinf(b) & (np.sign(a) == np.sign(b))
+    return np.where(same_inf, 0.0, np.abs(a - b) / np.maximum(1.0, np.abs(b)))
+
+
+@pytest.mark.parametrize("case", cases())
+def test_oracle_exact_ties_match_reference_exact_ties(case):
+    m, g, d, inject = load(case)
+    lb, _, lA, lbias = CrownOracle(g, tie_tol=EXACT_TIE_TOL).compute_bounds(d["x_L"], d["x_U"], d["C"])
+    assert _rel(lb, d["lb_exact"]).max() < 1e-9
+    assert _rel(lbias, d["lbias_exact"]).max() < 1e-9
+    assert np.abs(lA - d["lA_exact"]).max() <= 1e-9 * max(1.0, np.abs(d["lA_exact"]).max())
+
+
+@pytest.mark.parametrize("case", cases())
+def test_oracle_default_matches_reference_on_determined_rows(case):
+    m, g, d, inject = load(case)
+    lb, _, lA, lbias = CrownOracle(g).compute_bounds(d["x_L"], d["x_U"], d["C"])
+    stable = d["lb_ulp_dev"] <= 1e-5
+    assert _rel(lb, d["lb"])[stable].max(initial=0.0) < 1e-9
+    assert _rel(lbias, d["lbias"])[stable].max(initial=0.0) < 1e-9
 
 
 @pytest.mark.parametrize("case", cases())

@@ -42,3 +42,29 @@ def test_static_scratch_entry_matches_workspace_entry(workload, batch):
             assert np.all(np.isfinite(g_) == np.isfinite(w_))
             err = np.abs(g_ - w_) / np.maximum(1.0, np.abs(w_))
             assert float(np.nanmax(np.where(np.isfinite(w_), err, 0.0))) < RTOL
+
+
+def test_static_scratch_entry_loops_boxes_beyond_its_slots():
+    """A batch that needs more CTA scratch slots than the 64 MiB array holds: the entry runs the
+    batch on as many CTAs as fit, each taking several boxes in turn. Boxes are independent and
+    run the same code, so the results equal the workspace entry point's bit for bit."""
+    from gear_b200 import _lib, graph, problems
+    from gear_b200.engine import CrownEngine
+    L = _lib.lib()
+    m = problems.make_instance("dense_a_n2048", 0)
+    batch = 600
+    lo, hi = problems.make_boxes("dense_a_n2048", batch, 0)
+    eng = CrownEngine(graph.trace(m, lo[:2]), mode="cta", cta_threads=256)
+    # more slots than the static array holds: the capped path runs
+    assert L.gear_crown_workspace_bytes(eng.handle, batch) > L.gear_crown_static_scratch_bytes()
+    xL, xU = lo.cuda().contiguous(), hi.cuda().contiguous()
+    ref = eng.lower(xL, xU)
+    st = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):
+        out = [torch.full_like(t, np.nan) for t in ref]
+        _lib.check(L.gear_crown_lower_static(eng.handle, xL.data_ptr(), xU.data_ptr(), batch, None,
+                                             out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(), st),
+                   "gear_crown_lower_static")
+        torch.cuda.synchronize()
+        for got, want in zip(out, ref):
+            assert torch.equal(got, want)
