@@ -53,6 +53,10 @@ def lib():
         L.gear_crown_lower_static.restype = i32
         L.gear_crown_static_scratch_bytes.argtypes = []
         L.gear_crown_static_scratch_bytes.restype = i64
+        L.gear_crown_fold_vectors.argtypes = [vp, vp, vp, i64, vp, vp, vp, i64, vp]
+        L.gear_crown_fold_vectors.restype = i32
+        L.gear_crown_fold_workspace_bytes.argtypes = [vp, i64]
+        L.gear_crown_fold_workspace_bytes.restype = i64
         L.gear_bab_workspace_bytes.argtypes = [i64]
         L.gear_bab_workspace_bytes.restype = i64
         L.gear_bab_prune.argtypes = [vp, vp, i64, i32, vp, vp, vp, vp, vp, i64, vp]
@@ -118,4 +122,4 @@ EXPORTED = ("gear_dag_create", "gear_dag_destroy", "gear_crown_workspace_bytes",
             "gear_constrained_lower", "gear_clip_domains", "gear_bab_child_keys", "gear_bab_compact",
             "gear_dual_lower_bound", "gear_crown_lower_ibp", "gear_crown_multi_workspace_bytes",
             "gear_crown_lower_multi", "gear_crown_plain_workspace_bytes", "gear_crown_lower_plain",
-            "gear_queue_merge")
+            "gear_queue_merge", "gear_crown_fold_vectors", "gear_crown_fold_workspace_bytes")

@@ -96,9 +96,23 @@ class BoundedModule:
                 eng = CrownEngine(self.graph, spec_rows=spec_rows, dense_c=dense_c,
                                   mode=self.bound_opts.get("gear_mode", "auto"),
                                   cta_threads=int(self.bound_opts.get("gear_cta_threads", 128)),
-                                  tie_rule=self.bound_opts.get("gear_tie_rule", "reference"))
+                                  tie_rule=self.bound_opts.get("gear_tie_rule", "reference"),
+                                  fold_tc=self._fold_tc())
             self._engines[key] = eng
         return eng
+
+    # "auto" fold placement: dense nodes on the input with at least this many weights in all run
+    # their fold products on the tensor cores (measured on B200: 30% off a dense_a_n2048 call with
+    # 2 M weights, 4% on dense_q_n200's 50 k, where the fold is a small share of the kernel)
+    FOLD_TC_MIN_WEIGHTS = 1 << 20
+
+    def _fold_tc(self) -> bool:
+        opt = self.bound_opts.get("gear_fold_tc", "auto")
+        if opt != "auto":
+            return bool(opt)
+        weights = sum(nd.width * self.graph[0].width for nd in self.graph.nodes
+                      if nd.kind in ("linear", "matmul") and nd.inputs and nd.inputs[0] == 0)
+        return weights >= self.FOLD_TC_MIN_WEIGHTS
 
     def final_node_width(self) -> int:
         return self.graph[self.graph.output].width

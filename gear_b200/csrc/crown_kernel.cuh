@@ -61,6 +61,11 @@ struct Work {
   int64_t slot_doubles;
   int64_t B;
   int* status;
+  // fold vectors computed before the launch by the tensor-core fold (fold_tc.cuh), (B, H_FOLDW),
+  // or null; fold_fail points to its status flag (nonzero: a bounded wait expired, and every box
+  // folds on the CUDA cores instead)
+  const double* fold_ext;
+  const int* fold_fail;
 };
 
 // ------------------------------------------------------------------ small helpers
@@ -1439,7 +1444,18 @@ __device__ __forceinline__ void cta_step(const DevProgram& P, Box& bx, double* t
   const int32_t* st = P.steps + si * STEP_REC;
   const int type = st[0], a = st[1];
   switch (type) {
-    case ST_FOLD: fold_node<NT>(bx, a, work); break;
+    case ST_FOLD:
+      if (wk.fold_ext && !bx.open && *wk.fold_fail == 0) {
+        // tensor-core fold vectors of this box (a box with a non-finite centre or radius folds
+        // here, as the reference's dense product does)
+        const int32_t* nd = node_rec(&P, a);
+        const int off = nd[N_FOLD], cnt = 3 * nd[N_W];
+        const double* src = wk.fold_ext + (size_t)b * hdr[H_FOLDW] + off;
+        for (int j = threadIdx.x; j < cnt; j += NT) bx.fold[off + j] = src[j];
+      } else {
+        fold_node<NT>(bx, a, work);
+      }
+      break;
     case ST_IBP: {
       const int32_t* nd = node_rec(&P, a);
       ibp_node<NT>(bx, a, tmp_lo, tmp_hi);

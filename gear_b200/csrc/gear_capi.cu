@@ -16,6 +16,7 @@
 #include "bab_kernels.cuh"
 #include "concretize_kernels.cuh"
 #include "dual_kernels.cuh"
+#include "fold_tc.cuh"
 
 namespace {
 thread_local std::string g_err;
@@ -49,7 +50,131 @@ struct gear_dag {
   int64_t boxes_per_slot = 1;
   std::vector<int32_t> steps;    // host copies of the step and pass records (the plain form's
   std::vector<int32_t> passes;   // launch sequence)
+  // tensor-core fold (H_FOLD_TC): digit planes and row statistics of the dense nodes on the
+  // input, in one device block; the box digit planes of a batch live in the caller's workspace
+  void* tc_dev = nullptr;
+  std::vector<gear::foldtc::NodeDigits> tc_nodes;
+  int tc_k_pad = 0;
 };
+
+namespace {
+constexpr int64_t kAlign = 256;
+inline int64_t align_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
+
+// Workspace of the tensor-core fold for a batch, after the CTA slots: fold vectors (B, fold_w),
+// box statistics, centre and radius digit planes (b_pad x k_pad each), the status flag.
+struct TcLayout {
+  int64_t fold, stats, xc, xr, flag, total, b_pad, plane;
+};
+TcLayout tc_layout(const gear_dag* d, int64_t batch, int64_t base) {
+  using namespace gear::foldtc;
+  TcLayout L{};
+  L.b_pad = align_up(batch, BM);
+  L.plane = L.b_pad * d->tc_k_pad;
+  int64_t o = align_up(base, kAlign);
+  L.fold = o;  o = align_up(o + batch * d->hdr[gear::H_FOLDW] * (int64_t)sizeof(double), kAlign);
+  L.stats = o; o = align_up(o + L.b_pad * (int64_t)sizeof(BoxStat), kAlign);
+  L.xc = o;    o = align_up(o + DIGITS * L.plane, kAlign);
+  L.xr = o;    o = align_up(o + DIGITS * L.plane, kAlign);
+  L.flag = o;  o = align_up(o + (int64_t)sizeof(int), kAlign);
+  L.total = o;
+  return L;
+}
+
+// Digit planes of every dense node on the input (fold step of a box-per-CTA program), built once.
+int tc_prepare(gear_dag* d, const int32_t* nodes) {
+  using namespace gear;
+  using namespace gear::foldtc;
+  const int n_nodes = d->hdr[H_NNODES];
+  struct Pending { int v, w, K, n_pad, k_pad, woff; int64_t off; };
+  std::vector<Pending> todo;
+  int64_t bytes = 0;
+  for (int v = 0; v < n_nodes; ++v) {
+    const int32_t* nd = nodes + (int64_t)v * NODE_REC;
+    if (nd[N_FOLD] < 0) continue;
+    Pending p;
+    p.v = v;
+    p.w = nd[N_W];
+    p.K = nd[N_WIN];
+    p.n_pad = (int)align_up(p.w, BN);
+    p.k_pad = (int)align_up(p.K, BK);
+    p.woff = nd[N_W_OFF];
+    // int32 level sums: at most DIGITS - 1 pairs x k_pad x 127^2 must stay below 2^31
+    if ((int64_t)(DIGITS - 1) * p.k_pad * 127 * 127 >= (int64_t)1 << 31)
+      return fail(GEAR_E_INVALID, "gear_dag_create: %s", "tensor-core fold: input width beyond the int32 accumulator bound");
+    if (d->tc_k_pad && d->tc_k_pad != p.k_pad)
+      return fail(GEAR_E_INVALID, "gear_dag_create: %s", "tensor-core fold: dense nodes on the input of different widths");
+    d->tc_k_pad = p.k_pad;
+    p.off = bytes;
+    const int64_t plane = (int64_t)p.n_pad * p.k_pad;
+    bytes = align_up(bytes + 2 * DIGITS * plane + (int64_t)p.n_pad * (sizeof(int) + 2 * sizeof(double)) + 64, kAlign);
+    todo.push_back(p);
+  }
+  if (todo.empty()) return GEAR_OK;
+  cudaError_t e = cudaMalloc(&d->tc_dev, bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(tensor-core fold digits)");
+  for (const Pending& p : todo) {
+    char* base = (char*)d->tc_dev + p.off;
+    NodeDigits nd;
+    nd.plane = (int64_t)p.n_pad * p.k_pad;
+    int8_t* wd = (int8_t*)base;
+    int8_t* wa = wd + DIGITS * nd.plane;
+    double* wnorm = (double*)align_up((int64_t)(wa + DIGITS * nd.plane), 8);
+    double* wdelta = wnorm + p.n_pad;
+    int* we = (int*)(wdelta + p.n_pad);
+    nd.wd = wd;
+    nd.wa = wa;
+    nd.we = we;
+    nd.wnorm = wnorm;
+    nd.wdelta = wdelta;
+    nd.w = p.w;
+    nd.k_pad = p.k_pad;
+    nd.n_pad = p.n_pad;
+    nd.fold_off = (nodes + (int64_t)p.v * NODE_REC)[N_FOLD];
+    w_digits_kernel<<<p.n_pad, NT>>>(d->P.dp + p.woff, p.w, p.K, nd, wd, wa, we, wnorm, wdelta);
+    d->tc_nodes.push_back(nd);
+  }
+  e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "tensor-core fold digits");
+  e = cudaFuncSetAttribute(fold_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+  if (e != cudaSuccess) return cuda_fail(e, "fold_tc_kernel shared memory");
+  return GEAR_OK;
+}
+
+// Box digits, then one tensor-core launch per dense node: fold vectors of the batch into the
+// workspace (layout L). Returns the number of kernel launches, or a negative status.
+int tc_launch(const gear_dag* d, const double* x_L, const double* x_U, int64_t batch, char* ws, const TcLayout& L,
+              cudaStream_t stream) {
+  using namespace gear::foldtc;
+  int* flag = (int*)(ws + L.flag);
+  cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(int), stream);
+  if (e != cudaSuccess) return cuda_fail(e, "tensor-core fold status");
+  BoxStat* st = (BoxStat*)(ws + L.stats);
+  int8_t* xc = (int8_t*)(ws + L.xc);
+  int8_t* xr = (int8_t*)(ws + L.xr);
+  box_digits_kernel<<<(unsigned)L.b_pad, NT, 0, stream>>>(x_L, x_U, batch, d->hdr[gear::H_N], d->tc_k_pad, xc, xr,
+                                                         L.plane, st);
+  int launches = 1;
+  BatchDigits bt;
+  bt.xc = xc;
+  bt.xr = xr;
+  bt.plane = L.plane;
+  bt.st = st;
+  bt.fold = (double*)(ws + L.fold);
+  bt.fold_w = d->hdr[gear::H_FOLDW];
+  bt.B = batch;
+  bt.status = flag;
+  for (const NodeDigits& nd : d->tc_nodes) {
+    dim3 grid((unsigned)(nd.n_pad / BN), (unsigned)(L.b_pad / BM));
+    fold_tc_kernel<<<grid, NT, SMEM_BYTES, stream>>>(nd, bt);
+    ++launches;
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "tensor-core fold launch");
+  return launches;
+}
+}  // namespace
 
 // box-per-CTA kernel instances: dynamic shared-memory limit and resident CTAs per SM
 // (GWS: the program keeps its pass working set in global memory, a kernel instance of its own)
@@ -180,6 +305,20 @@ extern "C" int gear_dag_create(const int32_t* header, int64_t header_len, const 
   }
   if (e != cudaSuccess || bps < 1) bps = 1;
   d->blocks_per_sm = bps;
+  if (header[H_FOLD_TC] != 0) {
+    if (d->mode != MODE_CTA) {
+      cudaFree(d->dev);
+      delete d;
+      return fail(GEAR_E_INVALID, "gear_dag_create: %s", "the tensor-core fold is for box-per-CTA programs");
+    }
+    int st = tc_prepare(d, nodes);
+    if (st != GEAR_OK) {
+      if (d->tc_dev) cudaFree(d->tc_dev);
+      cudaFree(d->dev);
+      delete d;
+      return st;
+    }
+  }
   *out = d;
   return GEAR_OK;
 }
@@ -187,6 +326,7 @@ extern "C" int gear_dag_create(const int32_t* header, int64_t header_len, const 
 extern "C" int gear_dag_destroy(gear_dag* dag) {
   if (!dag) return GEAR_OK;
   if (dag->dev) cudaFree(dag->dev);
+  if (dag->tc_dev) cudaFree(dag->tc_dev);
   delete dag;
   return GEAR_OK;
 }
@@ -221,7 +361,9 @@ static int launch_crown(const gear_dag* dag, const gear::Work& wk, int64_t slots
 
 extern "C" int64_t gear_crown_workspace_bytes(const gear_dag* dag, int64_t batch) {
   if (!dag || batch < 0) return -1;
-  return slots_for(dag, batch) * dag->slot_doubles * (int64_t)sizeof(double);
+  const int64_t slots = slots_for(dag, batch) * dag->slot_doubles * (int64_t)sizeof(double);
+  if (dag->tc_nodes.empty() || batch == 0) return slots;
+  return tc_layout(dag, batch, slots).total;
 }
 
 static int crown_lower_impl(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
@@ -265,7 +407,45 @@ static int crown_lower_impl(const gear_dag* dag, const double* x_L, const double
   wk.slot_doubles = dag->slot_doubles;
   wk.B = batch;
   wk.status = nullptr;
-  return launch_crown(dag, wk, slots_for(dag, batch), (cudaStream_t)stream);
+  wk.fold_ext = nullptr;
+  wk.fold_fail = nullptr;
+  int pre = 0;
+  if (!dag->tc_nodes.empty()) {
+    const int64_t slots_bytes = slots_for(dag, batch) * dag->slot_doubles * (int64_t)sizeof(double);
+    const TcLayout L = tc_layout(dag, batch, slots_bytes);
+    pre = tc_launch(dag, x_L, x_U, batch, (char*)workspace, L, (cudaStream_t)stream);
+    if (pre < 0) return pre;
+    wk.fold_ext = (const double*)((char*)workspace + L.fold);
+    wk.fold_fail = (const int*)((char*)workspace + L.flag);
+  }
+  const int st = launch_crown(dag, wk, slots_for(dag, batch), (cudaStream_t)stream);
+  g_launches += pre;
+  return st;
+}
+
+extern "C" int gear_crown_fold_vectors(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
+                                       double* fold_out, int* fail_out, void* workspace, int64_t workspace_bytes,
+                                       void* stream) {
+  g_launches = 0;
+  if (!dag || batch < 0) return fail(GEAR_E_INVALID, "gear_crown_fold_vectors: %s", "bad arguments");
+  if (dag->tc_nodes.empty()) return fail(GEAR_E_INVALID, "gear_crown_fold_vectors: %s", "program without the tensor-core fold");
+  if (batch == 0) return GEAR_OK;
+  if (!x_L || !x_U || !fold_out) return fail(GEAR_E_INVALID, "gear_crown_fold_vectors: %s", "bad arguments");
+  const TcLayout L = tc_layout(dag, batch, 0);
+  if (!workspace || workspace_bytes < L.total) return fail(GEAR_E_WORKSPACE, "gear_crown_fold_vectors: %s", "workspace too small");
+  const int pre = tc_launch(dag, x_L, x_U, batch, (char*)workspace, L, (cudaStream_t)stream);
+  if (pre < 0) return pre;
+  g_launches = pre;
+  cudaError_t e = cudaMemcpyAsync(fold_out, (char*)workspace + L.fold, batch * dag->hdr[gear::H_FOLDW] * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, (cudaStream_t)stream);
+  if (e == cudaSuccess && fail_out)
+    e = cudaMemcpyAsync(fail_out, (char*)workspace + L.flag, sizeof(int), cudaMemcpyDeviceToDevice, (cudaStream_t)stream);
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_crown_fold_vectors copy");
+}
+
+extern "C" int64_t gear_crown_fold_workspace_bytes(const gear_dag* dag, int64_t batch) {
+  if (!dag || batch < 0 || dag->tc_nodes.empty()) return -1;
+  return tc_layout(dag, batch, 0).total;
 }
 
 // ------------------------------------------------------------------ no-allocation entry point
@@ -339,6 +519,8 @@ extern "C" int gear_crown_lower_static(const gear_dag* dag, const double* x_L, c
   wk.slot_doubles = dag->slot_doubles;
   wk.B = batch;
   wk.status = nullptr;
+  wk.fold_ext = nullptr;
+  wk.fold_fail = nullptr;
   return launch_crown(dag, wk, slots, (cudaStream_t)stream);
 }
 
@@ -390,6 +572,8 @@ extern "C" int gear_crown_lower_plain(const gear_dag* dag, const double* x_L, co
   wk.slot_doubles = dag->slot_doubles;   // one slot per box
   wk.B = batch;
   wk.status = nullptr;
+  wk.fold_ext = nullptr;
+  wk.fold_fail = nullptr;
   cudaStream_t st = (cudaStream_t)stream;
   int bps = 0;
   cudaError_t e = cudaErrorInvalidValue;
@@ -584,6 +768,8 @@ extern "C" int gear_crown_lower_multi(const gear_lower_args* items, int32_t coun
     it.wk.slot_doubles = pl.slot_doubles;
     it.wk.B = a.batch;
     it.wk.status = nullptr;
+    it.wk.fold_ext = nullptr;
+    it.wk.fold_fail = nullptr;
     hstart[k + 1] = hstart[k] + (a.batch + a.dag->boxes_per_slot - 1) / a.dag->boxes_per_slot;
     ++k;
   }

@@ -47,9 +47,11 @@ constexpr int RED_SLOTS = 32;
 enum HeaderField {
   H_NNODES = 0, H_NSTEPS, H_NPASSES, H_NOPS, H_N, H_S, H_T, H_ARENA, H_PLANES, H_FOLDW,
   H_SMEM, H_MAXS, H_SINOFF, H_MAXW, H_RETA, H_MAXOPS, H_SIMT_BUF, H_SIMT_ROWS, H_X_IN_LA, H_MODE,
-  H_CTA_THREADS, H_PASS_GLOBAL, H_TIES, H_R23, HEADER_LEN = 24
+  H_CTA_THREADS, H_PASS_GLOBAL, H_TIES, H_FOLD_TC, HEADER_LEN = 24
 };
 // H_TIES: McCormick tie rule, 0 = the reference's float comparison, 1 = exact-arithmetic ties.
+// H_FOLD_TC: 1 = the fold vectors of the dense nodes on the input come from the tensor-core
+// fold (fold_tc.cuh) launched before the CROWN kernel (box-per-CTA programs only).
 // H_PASS_GLOBAL: 0, or the doubles of a box-per-CTA program's pass working set when it is too
 // large for shared memory and lives at the end of the CTA's scratch slot instead (H_SMEM then
 // counts only the staged node table and op records).

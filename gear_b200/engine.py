@@ -40,9 +40,9 @@ def smem_class(prog) -> int:
 class _Dag:
     """One compiled program uploaded to the device (a gear_dag handle)."""
 
-    def __init__(self, graph, spec_rows, dense_c, mode, cta_threads, tie_rule="reference"):
+    def __init__(self, graph, spec_rows, dense_c, mode, cta_threads, tie_rule="reference", fold_tc=False):
         self._upload(Program(graph, spec_rows=spec_rows, dense_c=dense_c, mode=mode, cta_threads=cta_threads,
-                             tie_rule=tie_rule))
+                             tie_rule=tie_rule, fold_tc=fold_tc))
 
     def _upload(self, prog):
         self.prog = p = prog
@@ -87,10 +87,11 @@ class CrownEngine:
     mode "cta" runs one box per CTA (cta_threads threads), "simt" one box per thread; both
     give the same bounds. mode "auto" times the kernel variants on the first call for each
     batch size class (powers of two) on the caller's own boxes and keeps the fastest.
-    tie_rule: the McCormick tie rule of the compiled programs (``Program``)."""
+    tie_rule: the McCormick tie rule of the compiled programs (``Program``); fold_tc: the fold
+    products of dense nodes on the input on the tensor cores (box-per-CTA variants)."""
 
     def __init__(self, graph: Graph, spec_rows: Optional[int] = None, dense_c: bool = False, mode: str = "auto",
-                 cta_threads: int = 128, tie_rule: str = "reference"):
+                 cta_threads: int = 128, tie_rule: str = "reference", fold_tc: bool = False):
         if not torch.cuda.is_available():
             raise _lib.GearError("gear_b200 needs a CUDA device (no CPU fallback)")
         if mode not in ("auto", "cta", "simt"):
@@ -100,6 +101,7 @@ class CrownEngine:
         self.dense_c = dense_c
         self._args = (graph, spec_rows, dense_c)
         self.tie_rule = tie_rule
+        self.fold_tc = fold_tc
         self._dags = {}
         first = ("cta", cta_threads) if mode == "auto" else (mode, cta_threads)
         d = self._dag(*first)
@@ -114,7 +116,7 @@ class CrownEngine:
     def _dag(self, mode, threads):
         key = (mode, threads if mode == "cta" else 0)
         if key not in self._dags:
-            self._dags[key] = _Dag(*self._args, mode, threads, self.tie_rule)
+            self._dags[key] = _Dag(*self._args, mode, threads, self.tie_rule, self.fold_tc)
         return self._dags[key]
 
     def _candidates(self):

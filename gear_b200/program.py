@@ -127,7 +127,7 @@ class Program:
 
     def __init__(self, graph: Graph, spec_rows: Optional[int] = None, dense_c: bool = False,
                  return_a: bool = True, smem_limit: int = 232448, mode: str = "cta",
-                 cta_threads: int = 128, tie_rule: str = "reference"):
+                 cta_threads: int = 128, tie_rule: str = "reference", fold_tc: bool = False):
         """mode: "cta" runs one box per CTA with the pass working set in shared memory, and the
         final pass accumulates the input's A directly in the lA output; "simt" runs one box per
         thread with every per-box array box-interleaved in global scratch, and writes lA from the
@@ -137,10 +137,14 @@ class Program:
         whose box minima are equal in exact arithmetic (x entirely negative and y entirely
         positive, or the reverse): "reference" compares the two rounded minima as the reference
         does (bivariate.py:250; the outcome then follows the last bits of the intermediate
-        bounds), "exact" picks plane 1, the exact-arithmetic outcome."""
+        bounds), "exact" picks plane 1, the exact-arithmetic outcome.
+        fold_tc: compute the fold vectors of the dense nodes on the input (W x0, |W| eps) for the
+        whole batch on the tensor cores before the CROWN kernel (int8 digit slicing with a rigorous
+        error term; box-per-CTA programs with such nodes only, otherwise ignored)."""
         if tie_rule not in TIE_RULES:
             raise ProgramError(f"unknown tie rule {tie_rule!r}")
         self.tie_rule = tie_rule
+        self.fold_tc = bool(fold_tc) and mode == "cta"
         if mode not in MODES:
             raise ProgramError(f"unknown execution mode {mode!r}")
         if cta_threads not in (64, 128, 256):
@@ -509,7 +513,7 @@ class Program:
                                 self.smem_total, self.max_S, self.sin_off, self.maxw,
                                 1 if self.return_a else 0, max_ops, self.simt_buf, self.simt_rows,
                                 1 if self.x_in_la else 0, MODES[self.mode], self.cta_threads, self.pass_global,
-                                TIE_RULES[self.tie_rule], 0],
+                                TIE_RULES[self.tie_rule], 1 if (self.fold_tc and self.fold_w > 0) else 0],
                                dtype=np.int32)
 
     def _emit_pass(self, pid, pi: PassInfo):
@@ -781,7 +785,7 @@ class Program:
 
 
 # ===================================================================== compile pools
-_KEEP = ("S", "n", "t", "mode", "cta_threads", "tie_rule", "x_in_la", "return_a", "dense_c", "arena_w", "plane_w", "fold_w", "maxw",
+_KEEP = ("S", "n", "t", "mode", "cta_threads", "tie_rule", "fold_tc", "x_in_la", "return_a", "dense_c", "arena_w", "plane_w", "fold_w", "maxw",
          "max_S", "max_smem", "smem_total", "pass_global", "simt_buf", "simt_rows", "sin_off", "work", "header",
          "node_arr", "step_arr", "pass_arr", "op_arr", "int_pool", "dbl_pool")
 

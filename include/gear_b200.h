@@ -204,12 +204,35 @@ int gear_crown_lower_ibp(const gear_dag* dag, const double* x_L, const double* x
  * (cudaGetSymbolAddress); make that first call before any stream capture. All calls share the
  * one array, so calls that overlap on the GPU (different streams, different host threads on
  * the same device) race: serialise them. The gear_dag handle itself is still created (and
- * allocated) once by gear_dag_create. */
+ * allocated) once by gear_dag_create. A program compiled with the tensor-core fold computes its
+ * fold products on the CUDA cores here (the digit planes need workspace), so its bounds differ
+ * from gear_crown_lower's within the fold's stated error term (~1e-8 relative). */
 int gear_crown_lower_static(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
                             const double* C, double* lb, double* lA, double* lbias, void* stream);
 
 /* Size in bytes of gear_crown_lower_static's built-in scratch array. */
 int64_t gear_crown_static_scratch_bytes(void);
+
+/* ---------------------------------------------------------------- tensor-core fold
+ * A program compiled with the tensor-core fold (header field H_FOLD_TC) gets, for each dense
+ * Linear/MatMul node on the input, the products W x0, |W| eps and |W| max(|x_L|, |x_U|) over the
+ * whole batch from int8 digit-sliced GEMMs on the tcgen05 tensor cores (exact int32 level sums in
+ * TMEM, combined in float64) before the CROWN kernel runs; the radius carries the rigorous bound
+ * of the slicing error, so every CROWN bound stays sound. This is the dense work of
+ * BoundLinear.bound_backward / interval_propagate on the input (auto_LiRPA/operators/linear.py:268,
+ * interval_bound.py:156-254). gear_crown_lower and gear_crown_lower_ibp launch it themselves
+ * (their workspace then includes the digit planes: gear_crown_workspace_bytes).
+ *
+ * gear_crown_fold_vectors runs only that step and copies the fold vectors (batch, fold width of
+ * the program: per dense node, w centres, w radii (error included), w magnitudes) to fold_out;
+ * fail_out (one int, may be NULL) receives 1 when a bounded device wait expired (the vectors are
+ * then invalid; gear_crown_lower falls back to the CUDA-core fold by itself). */
+int gear_crown_fold_vectors(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
+                            double* fold_out, int* fail_out, void* workspace, int64_t workspace_bytes,
+                            void* stream);
+
+/* Workspace bytes of gear_crown_fold_vectors (-1 for a program without the tensor-core fold). */
+int64_t gear_crown_fold_workspace_bytes(const gear_dag* dag, int64_t batch);
 
 /* ---------------------------------------------------------------- the plain (unfused) form
  * The same CROWN bounds as gear_crown_lower, computed the unfused way: one kernel launch per

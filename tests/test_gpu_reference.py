@@ -26,7 +26,8 @@ from gear_b200.engine import CrownEngine
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-5
-VARIANTS = [("cta", 64), ("cta", 128), ("cta", 256), ("simt", 128)]
+# (execution mode, threads per CTA, tensor-core fold of dense nodes on the input)
+VARIANTS = [("cta", 64, False), ("cta", 128, False), ("cta", 256, False), ("simt", 128, False), ("cta", 128, True)]
 
 
 def _rel(a, b):
@@ -35,18 +36,18 @@ def _rel(a, b):
     return np.where(same_inf, 0.0, np.abs(a - b) / np.maximum(1.0, np.abs(b)))
 
 
-def _run(g, d, mode, threads, tie_rule):
-    eng = CrownEngine(g, mode=mode, cta_threads=threads, tie_rule=tie_rule)
+def _run(g, d, mode, threads, tc, tie_rule):
+    eng = CrownEngine(g, mode=mode, cta_threads=threads, tie_rule=tie_rule, fold_tc=tc)
     lb, lA, lbias = eng.lower(torch.tensor(d["x_L"], device="cuda"), torch.tensor(d["x_U"], device="cuda"))
     torch.cuda.synchronize()
     return lb.cpu().numpy(), lA.cpu().numpy(), lbias.cpu().numpy()
 
 
 @pytest.mark.parametrize("case", cases())
-@pytest.mark.parametrize("mode,threads", VARIANTS)
-def test_exact_ties_match_reference_every_row(case, mode, threads):
+@pytest.mark.parametrize("mode,threads,tc", VARIANTS)
+def test_exact_ties_match_reference_every_row(case, mode, threads, tc):
     m, g, d, _ = load(case)
-    lb, lA, lbias = _run(g, d, mode, threads, "exact")
+    lb, lA, lbias = _run(g, d, mode, threads, tc, "exact")
     assert _rel(lb, d["lb_exact"]).max() < TOL
     assert _rel(lbias, d["lbias_exact"]).max() < TOL
     scale = max(1.0, float(np.abs(d["lA_exact"]).max()))
@@ -54,10 +55,10 @@ def test_exact_ties_match_reference_every_row(case, mode, threads):
 
 
 @pytest.mark.parametrize("case", cases())
-@pytest.mark.parametrize("mode,threads", VARIANTS)
-def test_default_matches_reference_on_determined_rows(case, mode, threads):
+@pytest.mark.parametrize("mode,threads,tc", VARIANTS)
+def test_default_matches_reference_on_determined_rows(case, mode, threads, tc):
     m, g, d, _ = load(case)
-    lb, lA, lbias = _run(g, d, mode, threads, "reference")
+    lb, lA, lbias = _run(g, d, mode, threads, tc, "reference")
     stable = d["lb_ulp_dev"] <= TOL
     err = _rel(lb, d["lb"])
     assert err[stable].max(initial=0.0) < TOL, f"{int((err[stable] >= TOL).sum())} determined rows differ"
