@@ -216,7 +216,7 @@ def mixed_setup(instances=512, workers=None):
     me = MultiEngine(graphs, programs=compile_many(graphs, kw=dict(mode="cta", cta_threads=256,
                                                                    smem_limit=PACK_SMEM_LIMIT),
                                                    simt_items_max=SIMT_PACK_ITEMS, workers=workers))
-    return insts, graphs, me, time.perf_counter() - t0
+    return insts, graphs, me, time.perf_counter() - t0, {}
 
 
 def mixed_batch(dev, setup, boxes=256, steps=2, warmup=1, baselines=True):
@@ -230,7 +230,7 @@ def mixed_batch(dev, setup, boxes=256, steps=2, warmup=1, baselines=True):
     from gear_b200 import _lib, problems
     from gear_b200.engine import _Dag
     from gear_b200.program import compile_many
-    insts, graphs, me, compile_s = setup
+    insts, graphs, me, compile_s = setup[:4]
     instances = len(insts)
     bx = [tuple(t.to(dev) for t in problems.mixed_boxes(m, boxes, k)) for k, m in enumerate(insts)]
     total = instances * boxes
@@ -279,7 +279,7 @@ def mixed_batch(dev, setup, boxes=256, steps=2, warmup=1, baselines=True):
                 "packed_vs_alone": alone_ms / packed_ms, "bitwise_equal_alone": same})
     if baselines:
         t1 = time.perf_counter()
-        pprogs = compile_many(graphs, kw=dict(mode="cta", cta_threads=128, smem_limit=0))
+        pprogs = plain_programs(setup)
         pdags = [_Dag.from_program(p) for p in pprogs]
         compile_s += time.perf_counter() - t1
         pws_bytes = max(int(L.gear_crown_plain_workspace_bytes(d.handle, boxes)) for d in pdags)
@@ -295,24 +295,62 @@ def mixed_batch(dev, setup, boxes=256, steps=2, warmup=1, baselines=True):
                                                     lb.data_ptr(), lA.data_ptr(), lbias.data_ptr(), pws.data_ptr(),
                                                     pws_bytes, stream), "gear_crown_lower_plain")
                 launches[0] += int(L.gear_last_launch_count())
-        plain_ms = timed(plain_step, 1, 0)
+        plain_ms = timed(plain_step, 1, 1)
         res.update({"plain_ms": plain_ms, "plain_subdomains_per_s": total / (plain_ms / 1000.0),
                     "plain_launches_per_call": launches[0], "packed_vs_plain": plain_ms / packed_ms,
-                    "bitwise_equal_plain": all(torch.equal(a[0], b[0]) for a, b in zip(outs, pl))})
+                    "plain_difference": lb_difference(outs, pl)})
         del pws
     res.update({"compile_s": compile_s, "timing": f"CUDA events; packed and alone {steps} calls after {warmup} "
-                "warm-up, plain 1 call (its kernels already loaded)"})
+                "warm-up, plain 1 call after 1 warm-up call"})
     return res
 
 
-def mixed_bab(dev, setup, batch=256, rel_gap=1e-4, time_limit=60.0):
-    """Branch and bound on the uneven batch, every instance at once (MultiBaB: one packed CROWN
-    launch per kernel variant per iteration): wall time to the relative gap per instance (host
-    loop included) over the instances that reach it within the time limit, and subdomains
-    bounded per second over the run."""
+def plain_programs(setup):
+    """The plain form's programs of the uneven batch (pass working set in global memory,
+    128 threads per CTA), compiled once per setup."""
+    from gear_b200.program import compile_many
+    cache = setup[4]
+    if "plain" not in cache:
+        cache["plain"] = compile_many(setup[1], kw=dict(mode="cta", cta_threads=128, smem_limit=0))
+    return cache["plain"]
+
+
+def lb_difference(a_outs, b_outs):
+    """How the lower bounds of two runs of the same boxes differ: the largest relative difference
+    (to max(1, |lb|)) and the share of rows that differ by more than 1e-9. Kernel variants sum in
+    different orders, and where two McCormick planes tie (equal box minima) the reference's float
+    comparison, used by default, follows those last bits: such rows can differ by much more than
+    the rounding (both bounds are sound)."""
+    import torch
+    num, rows, worst = 0, 0, 0.0
+    for (la, _, _), (lb_, _, _) in zip(a_outs, b_outs):
+        if la.numel() == 0:
+            continue
+        same_inf = torch.isinf(la) & torch.isinf(lb_) & (torch.sign(la) == torch.sign(lb_))
+        err = torch.where(same_inf, torch.zeros_like(la), (la - lb_).abs() / torch.clamp(lb_.abs(), min=1.0))
+        err = torch.nan_to_num(err, nan=float("inf"))
+        worst = max(worst, float(err.max()))
+        num += int((err > 1e-9).sum())
+        rows += err.numel()
+    return {"max_rel": worst, "rows_over_1e-9": num, "rows": rows,
+            "note": "default McCormick tie rule (the reference's float comparison): tie-decided rows follow the "
+                    "summation order of the kernel variant; both arms' bounds are sound"}
+
+
+def mixed_bab(dev, setup, batch=256, rel_gap=1e-4, time_limit=60.0, plain=False):
+    """Branch and bound on the uneven batch to relative gap 1e-4, every instance at once
+    (MultiBaB): certified subdomains per second (subdomains bounded, each with a sound lower bound,
+    per second of wall time, host loop included), wall time to the gap per instance over the
+    instances that reach it within the time limit. plain=False bounds every iteration's batches in
+    one packed CROWN launch per kernel variant (MultiEngine); plain=True is the plain GPU form:
+    each instance's batch bounded alone, one launch per schedule step and per op
+    (PlainMultiEngine), the same loop otherwise."""
     import torch
     from gear_b200.bab import MultiBaB
-    insts, graphs, me, _ = setup
+    insts, graphs, me = setup[:3]
+    if plain:
+        from gear_b200.engine import PlainMultiEngine
+        me = PlainMultiEngine(graphs, programs=plain_programs(setup))
     instances = len(insts)
     roots = [(torch.full((1, m.n), -2.0, dtype=torch.float64), torch.full((1, m.n), 2.0, dtype=torch.float64))
              for m in insts]
@@ -327,6 +365,8 @@ def mixed_bab(dev, setup, batch=256, rel_gap=1e-4, time_limit=60.0):
     q = (lambda p: ttg[min(len(ttg) - 1, int(round(p * (len(ttg) - 1))))]) if ttg else (lambda p: None)
     closed_n = [insts[i].n for i, r in enumerate(res) if r["time_to_gap"] is not None]
     return {"workload": "mixed family (n log-uniform [5, 500], depth 3-12, m = n // 4)", "instances": instances,
+            "form": "plain GPU form (one instance, one launch per step and per op)" if plain else
+                    "packed (one launch per kernel variant per iteration)",
             "batch_per_instance": batch, "rel_gap": rel_gap, "time_limit_s": time_limit, "wall_s": wall,
             "iterations": mb.iterations, "closed": len(ttg), "closed_max_n": max(closed_n) if closed_n else None,
             "time_to_gap_s": {"p50": q(0.5), "p99": q(0.99), "max": ttg[-1] if ttg else None},
@@ -422,6 +462,70 @@ def plain_gpu(dev, workload, lo, hi, fused_value, steps=3, warmup=1):
                     "box state in global memory between launches"}, out
 
 
+def dense_nodes(dev, batch=8192, steps=3, warmup=1):
+    """The dense-node configuration (dense_a_n2048: y = A x with A 1024 x 2048, objective
+    sum alpha_j y_j^2 + beta_j y_j y_{j+1}), `batch` boxes: CROWN with the fold products of the
+    dense node on the tensor cores (int8 digit slicing on tcgen05, fold_tc.cuh) against the same
+    kernel with the fold on FP64 CUDA cores; the tensor-core fold kernel alone; the error of the
+    tensor-core path against the FP64 one (both with exact-arithmetic McCormick ties, so the
+    difference is the fold's own; with the default tie rule tie-decided rows can differ more)."""
+    import torch
+    from gear_b200 import _lib, graph, problems
+    from gear_b200.engine import CrownEngine
+    wl = "dense_a_n2048"
+    m = problems.make_instance(wl, 0)
+    lo, hi = problems.make_boxes(wl, batch, 0)
+    g = graph.trace(m, lo[:2])
+    xL, xU = lo.to(dev), hi.to(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / steps
+
+    res = {"workload": wl, "batch": batch, "n": 2048, "dense_node": "1024 x 2048"}
+    lbs = {}
+    for name, tc, tie in (("tensor_core_fold", True, "reference"), ("cuda_core_fold", False, "reference"),
+                          ("tensor_core_fold_exact_ties", True, "exact"), ("cuda_core_fold_exact_ties", False, "exact")):
+        eng = CrownEngine(g, mode="cta", cta_threads=256, fold_tc=tc, tie_rule=tie)
+        out = eng.lower(xL, xU)
+        if tie == "reference":
+            ms = timed(lambda: eng.lower(xL, xU, out=out))
+            res[name] = {"ms_per_call": ms, "subdomains_per_s": batch / (ms / 1000.0)}
+        torch.cuda.synchronize(dev)
+        lbs[name] = out[0].clone()
+        if name == "tensor_core_fold":
+            L = _lib.lib()
+            ws = torch.empty(int(L.gear_crown_fold_workspace_bytes(eng.handle, batch)), dtype=torch.uint8, device=dev)
+            fold = torch.empty(batch, eng.prog.fold_w, dtype=torch.float64, device=dev)
+            st = torch.cuda.current_stream(dev).cuda_stream
+            fms = timed(lambda: _lib.check(L.gear_crown_fold_vectors(eng.handle, xL.data_ptr(), xU.data_ptr(), batch,
+                                                                     fold.data_ptr(), None, ws.data_ptr(), ws.numel(),
+                                                                     st), "gear_crown_fold_vectors"))
+            k_pad, w, K = (2048 + 63) // 64 * 64, 1024, 2048
+            macs = 2 * 15 * batch * w * k_pad            # two products, 15 digit pairs (levels 2..6)
+            res["fold_kernels_ms"] = fms
+            res["fold_int8_tops"] = 2 * macs / (fms / 1000.0) / 1e12
+            res["fold_fp64_equivalent_tflops"] = 2 * 2 * batch * w * K / (fms / 1000.0) / 1e12
+            res["fold_kernels"] = "box_digits_kernel + fold_tc_kernel (tcgen05.mma.kind::i8, TMEM accumulators)"
+            del ws, fold
+        del eng, out
+    a, b = lbs["tensor_core_fold_exact_ties"], lbs["cuda_core_fold_exact_ties"]
+    res["error_vs_fp64"] = {"max_rel_lb": float(((a - b).abs() / torch.clamp(b.abs(), min=1.0)).max()),
+                            "tie_rule": "exact (both)", "tolerance_north_star": 1e-5}
+    a, b = lbs["tensor_core_fold"], lbs["cuda_core_fold"]
+    res["default_rule_difference"] = {"max_rel_lb": float(((a - b).abs() / torch.clamp(b.abs(), min=1.0)).max())}
+    res["speedup_tensor_core_fold"] = res["cuda_core_fold"]["ms_per_call"] / res["tensor_core_fold"]["ms_per_call"]
+    return res
+
+
 # ---------------------------------------------------------------- GPU leg
 def main():
     ap = argparse.ArgumentParser()
@@ -442,10 +546,13 @@ def main():
     ap.add_argument("--e2e-chunk", type=int, default=16384, help="boxes per chunk of the pipelined end-to-end call")
     ap.add_argument("--no-mixed-baselines", dest="mixed_baselines", action="store_false",
                     help="time only the packed launch of the uneven batch (no per-instance or plain-form runs)")
-    ap.add_argument("--mixed-bab-seconds", type=float, default=60.0,
-                    help="time limit of branch and bound on the uneven batch (all instances at once); 0 skips it")
-    ap.add_argument("--serve-seconds", type=float, default=10.0,
+    ap.add_argument("--mixed-bab-seconds", type=float, default=45.0,
+                    help="time limit of branch and bound on the uneven batch (all instances at once), for the "
+                         "packed arm and again for the plain-form arm; 0 skips it")
+    ap.add_argument("--serve-seconds", type=float, default=120.0,
                     help="run the serving loop under Poisson arrivals (50 per second) for this long; 0 skips it")
+    ap.add_argument("--dense-batch", type=int, default=8192,
+                    help="boxes of the dense-node configuration (dense_a_n2048, tensor-core fold); 0 skips it")
     ap.add_argument("--no-plain", dest="plain", action="store_false",
                     help="skip the plain GPU form (one launch per step and per op) on the workload")
     ap.add_argument("--workload", default=WORKLOAD, help="benchmark workload (profiling of other shapes)")
@@ -597,6 +704,14 @@ def main():
             res["mixed"] = mixed_batch(dev, setup, args.mixed_boxes, baselines=args.mixed_baselines)
             if args.mixed_bab_seconds > 0:
                 res["mixed_bab"] = mixed_bab(dev, setup, time_limit=args.mixed_bab_seconds)
+                if args.mixed_baselines:
+                    pb = mixed_bab(dev, setup, time_limit=args.mixed_bab_seconds, plain=True)
+                    res["mixed_bab_plain"] = pb
+                    res["mixed_bab_vs_plain"] = {
+                        "certified_subdomains_per_s_ratio": res["mixed_bab"]["subdomains_per_s"] / pb["subdomains_per_s"],
+                        "closed": [res["mixed_bab"]["closed"], pb["closed"]], "target": 10.0}
+        if args.dense_batch > 0:
+            res["dense_nodes"] = dense_nodes(dev, batch=args.dense_batch)
         if args.serve_seconds > 0:
             res["serve"] = serve(dev, seconds=args.serve_seconds)
         if world == 1 and not args.no_cpu_baseline:

@@ -90,6 +90,8 @@ def lib():
         L.gear_crown_plain_workspace_bytes.restype = i64
         L.gear_crown_lower_plain.argtypes = [vp, vp, vp, i64, vp, vp, vp, vp, vp, i64, vp]
         L.gear_crown_lower_plain.restype = i32
+        L.gear_crown_lower_plain_ibp.argtypes = [vp, vp, vp, i64, vp, vp, vp, vp, vp, vp, i64, vp]
+        L.gear_crown_lower_plain_ibp.restype = i32
         L.gear_crown_multi_workspace_bytes.argtypes = [ctypes.POINTER(LowerArgs), i32]
         L.gear_crown_multi_workspace_bytes.restype = i64
         L.gear_crown_lower_multi.argtypes = [ctypes.POINTER(LowerArgs), i32, vp, i64, vp]
@@ -122,4 +124,5 @@ EXPORTED = ("gear_dag_create", "gear_dag_destroy", "gear_crown_workspace_bytes",
             "gear_constrained_lower", "gear_clip_domains", "gear_bab_child_keys", "gear_bab_compact",
             "gear_dual_lower_bound", "gear_crown_lower_ibp", "gear_crown_multi_workspace_bytes",
             "gear_crown_lower_multi", "gear_crown_plain_workspace_bytes", "gear_crown_lower_plain",
-            "gear_queue_merge", "gear_crown_fold_vectors", "gear_crown_fold_workspace_bytes")
+            "gear_queue_merge", "gear_crown_fold_vectors", "gear_crown_fold_workspace_bytes",
+            "gear_crown_lower_plain_ibp")

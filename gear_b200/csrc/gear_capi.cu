@@ -548,9 +548,26 @@ extern "C" int64_t gear_crown_plain_workspace_bytes(const gear_dag* dag, int64_t
   return batch * dag->slot_doubles * (int64_t)sizeof(double);
 }
 
+static int plain_impl(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch, const double* C,
+                      double* lb, double* lA, double* lbias, double* lb_ibp, void* workspace, int64_t workspace_bytes,
+                      void* stream);
+
 extern "C" int gear_crown_lower_plain(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
                                       const double* C, double* lb, double* lA, double* lbias, void* workspace,
                                       int64_t workspace_bytes, void* stream) {
+  return plain_impl(dag, x_L, x_U, batch, C, lb, lA, lbias, nullptr, workspace, workspace_bytes, stream);
+}
+
+extern "C" int gear_crown_lower_plain_ibp(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
+                                          const double* C, double* lb, double* lA, double* lbias, double* lb_ibp,
+                                          void* workspace, int64_t workspace_bytes, void* stream) {
+  if (!lb_ibp) return fail(GEAR_E_INVALID, "gear_crown_lower_plain_ibp: %s", "lb_ibp is required");
+  return plain_impl(dag, x_L, x_U, batch, C, lb, lA, lbias, lb_ibp, workspace, workspace_bytes, stream);
+}
+
+static int plain_impl(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch, const double* C,
+                      double* lb, double* lA, double* lbias, double* lb_ibp, void* workspace, int64_t workspace_bytes,
+                      void* stream) {
   g_launches = 0;
   if (!dag || batch < 0) return fail(GEAR_E_INVALID, "gear_crown_lower_plain: %s", "bad arguments");
   if (!plain_ok(dag))
@@ -567,7 +584,7 @@ extern "C" int gear_crown_lower_plain(const gear_dag* dag, const double* x_L, co
   wk.lb = lb;
   wk.lA = lA;
   wk.lbias = lbias;
-  wk.lb_ibp = nullptr;
+  wk.lb_ibp = lb_ibp;
   wk.scratch = (double*)workspace;
   wk.slot_doubles = dag->slot_doubles;   // one slot per box
   wk.B = batch;

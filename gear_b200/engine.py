@@ -423,7 +423,8 @@ class PlainEngine:
         self._ws = None
         self.launches = 0
 
-    def lower(self, x_L: torch.Tensor, x_U: torch.Tensor, out=None):
+    def lower(self, x_L: torch.Tensor, x_U: torch.Tensor, out=None, lb_ibp: Optional[torch.Tensor] = None):
+        """lb, lA, lbias as CrownEngine.lower; lb_ibp (B, S) as there (the bounding glue's IBP pass)."""
         B = x_L.shape[0]
         dev = x_L.device
         if dev.type != "cuda":
@@ -443,8 +444,57 @@ class PlainEngine:
             self._ws = None
             self._ws = torch.empty(max(nbytes, 8), dtype=torch.uint8, device=dev)
         stream = torch.cuda.current_stream(dev).cuda_stream
-        _lib.check(L.gear_crown_lower_plain(self.dag.handle, x_L.data_ptr(), x_U.data_ptr(), B, None, lb.data_ptr(),
-                                            lA.data_ptr(), lbias.data_ptr(), self._ws.data_ptr(), self._ws.numel(),
-                                            stream), "gear_crown_lower_plain")
+        if lb_ibp is None:
+            _lib.check(L.gear_crown_lower_plain(self.dag.handle, x_L.data_ptr(), x_U.data_ptr(), B, None,
+                                                lb.data_ptr(), lA.data_ptr(), lbias.data_ptr(), self._ws.data_ptr(),
+                                                self._ws.numel(), stream), "gear_crown_lower_plain")
+        else:
+            _lib.check(L.gear_crown_lower_plain_ibp(self.dag.handle, x_L.data_ptr(), x_U.data_ptr(), B, None,
+                                                    lb.data_ptr(), lA.data_ptr(), lbias.data_ptr(), lb_ibp.data_ptr(),
+                                                    self._ws.data_ptr(), self._ws.numel(), stream),
+                       "gear_crown_lower_plain_ibp")
         self.launches = int(L.gear_last_launch_count())
         return out
+
+
+class PlainMultiEngine:
+    """The plain GPU form of many instances (the denominator of the uneven batch): each instance
+    bounded alone by its own PlainEngine, one instance after another, one kernel launch per
+    schedule step and per op. Same lower(boxes, out, lb_ibp) interface as MultiEngine.
+    programs: optional precompiled plain programs (Program(graph, mode="cta", smem_limit=0))."""
+
+    def __init__(self, graphs, programs=None, cta_threads: int = 128):
+        if not torch.cuda.is_available():
+            raise _lib.GearError("gear_b200 needs a CUDA device (no CPU fallback)")
+        self.engines = []
+        for i, g in enumerate(graphs):
+            pe = PlainEngine.__new__(PlainEngine)
+            prog = programs[i] if programs is not None else Program(g, mode="cta", cta_threads=cta_threads,
+                                                                    smem_limit=0)
+            pe.dag = _Dag.from_program(prog)
+            pe.prog = prog
+            pe.n, pe.S = prog.n, prog.S
+            pe._ws = None
+            pe.launches = 0
+            self.engines.append(pe)
+        self.n = [e.n for e in self.engines]
+        self.S = [e.S for e in self.engines]
+        self.launch_count = 0
+
+    def lower(self, boxes, out=None, lb_ibp=None):
+        outs = []
+        self.launch_count = 0
+        for i, (x_L, x_U) in enumerate(boxes):
+            e = self.engines[i]
+            B = x_L.shape[0]
+            o = out[i] if out is not None else None
+            ibp = lb_ibp[i] if lb_ibp is not None else None
+            if B == 0:
+                dev = x_L.device
+                outs.append((torch.empty(0, e.S, dtype=torch.float64, device=dev),
+                             torch.empty(0, e.S, e.n, dtype=torch.float64, device=dev),
+                             torch.empty(0, e.S, dtype=torch.float64, device=dev)))
+                continue
+            outs.append(e.lower(x_L, x_U, out=o, lb_ibp=ibp))
+            self.launch_count += e.launches
+        return outs

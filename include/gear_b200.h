@@ -247,6 +247,13 @@ int gear_crown_lower_plain(const gear_dag* dag, const double* x_L, const double*
                            const double* C, double* lb, double* lA, double* lbias, void* workspace,
                            int64_t workspace_bytes, void* stream);
 
+/* gear_crown_lower_plain with the IBP pass of the bounding glue, as gear_crown_lower_ibp
+ * (complete_verifier/input_split/bounding.py:789-948): lb_ibp (batch, S) receives the rows' bounds
+ * over the output's plain interval and lb the larger of that and CROWN's. */
+int gear_crown_lower_plain_ibp(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
+                               const double* C, double* lb, double* lA, double* lbias, double* lb_ibp,
+                               void* workspace, int64_t workspace_bytes, void* stream);
+
 /* ---------------------------------------------------------------- many instances, one launch
  * One instance of a multi-instance CROWN call: the arguments gear_crown_lower takes for one
  * DAG (same shapes and meaning; batch may be 0). The reference bounds each instance with its own
