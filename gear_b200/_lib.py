@@ -53,6 +53,30 @@ def lib():
         L.gear_crown_lower_static.restype = i32
         L.gear_crown_static_scratch_bytes.argtypes = []
         L.gear_crown_static_scratch_bytes.restype = i64
+        L.gear_queue_create.argtypes = [i32, i32, i64, i64, vp, vp, ctypes.POINTER(ctypes.c_void_p)]
+        L.gear_queue_create.restype = i32
+        L.gear_queue_destroy.argtypes = [vp]
+        L.gear_queue_destroy.restype = i32
+        L.gear_queue_push.argtypes = [vp, vp, vp, vp, i64, vp]
+        L.gear_queue_push.restype = i32
+        L.gear_queue_pop.argtypes = [vp, vp, vp, vp]
+        L.gear_queue_pop.restype = i32
+        L.gear_queue_size.argtypes = [vp, ctypes.POINTER(ctypes.c_int64), vp]
+        L.gear_queue_size.restype = i32
+        L.gear_queue_counters.argtypes = [vp, vp, vp, vp]
+        L.gear_queue_counters.restype = i32
+        L.gear_bab_step_workspace_bytes.argtypes = [vp, i64]
+        L.gear_bab_step_workspace_bytes.restype = i64
+        L.gear_bab_step.argtypes = [vp, vp, vp, vp, vp, vp, dbl, dbl, i32, vp, i64, vp]
+        L.gear_bab_step.restype = i32
+        L.gear_bab_step_bounded.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, dbl, dbl, vp]
+        L.gear_bab_step_bounded.restype = i32
+        L.gear_crown_multi_prepare.argtypes = [ctypes.POINTER(LowerArgs), i32, vp, i64, ctypes.POINTER(ctypes.c_void_p)]
+        L.gear_crown_multi_prepare.restype = i32
+        L.gear_crown_multi_launch.argtypes = [vp, vp]
+        L.gear_crown_multi_launch.restype = i32
+        L.gear_crown_multi_plan_destroy.argtypes = [vp]
+        L.gear_crown_multi_plan_destroy.restype = i32
         L.gear_crown_fold_vectors.argtypes = [vp, vp, vp, i64, vp, vp, vp, i64, vp]
         L.gear_crown_fold_vectors.restype = i32
         L.gear_crown_fold_workspace_bytes.argtypes = [vp, i64]
@@ -125,4 +149,7 @@ EXPORTED = ("gear_dag_create", "gear_dag_destroy", "gear_crown_workspace_bytes",
             "gear_dual_lower_bound", "gear_crown_lower_ibp", "gear_crown_multi_workspace_bytes",
             "gear_crown_lower_multi", "gear_crown_plain_workspace_bytes", "gear_crown_lower_plain",
             "gear_queue_merge", "gear_crown_fold_vectors", "gear_crown_fold_workspace_bytes",
-            "gear_crown_lower_plain_ibp")
+            "gear_crown_lower_plain_ibp", "gear_queue_create", "gear_queue_destroy", "gear_queue_push",
+            "gear_queue_pop", "gear_queue_size", "gear_queue_counters", "gear_bab_step_workspace_bytes",
+            "gear_bab_step", "gear_bab_step_bounded", "gear_crown_multi_prepare", "gear_crown_multi_launch",
+            "gear_crown_multi_plan_destroy")

@@ -21,6 +21,7 @@ discarded by the objective row (``batch_branch_and_bound.py:628-636``).
 """
 from __future__ import annotations
 
+import ctypes
 import math
 import time
 from dataclasses import dataclass, field
@@ -569,3 +570,330 @@ class MultiBaB:
             active = nxt
         return [{"P": b.incumbent, "gap": last[i], "time_to_gap": reached[i], "iterations": rounds[i],
                  "bounded": b.stats.bounded} for i, b in enumerate(self.babs)]
+
+
+class GraphBaB:
+    """Branch and bound to a relative gap on one instance with its queue on the device.
+
+    The open domains live in a gear_queue (slot arrays, the ordered active list, free list and
+    counters in device memory); an iteration is gear_queue_pop, the incumbent proposal from the
+    popped boxes' midpoints (the model in float64, on the device), and gear_bab_step (CROWN, prune,
+    SB branch, split, child keys, sort and merge of the children). Every size is read on the
+    device, so `chunk` iterations are captured once into a CUDA graph and replayed; the host reads
+    the counters, the dual bound and the incumbent once per replay to test the gap. The search is
+    the one BaB runs: same queue order, same kernels."""
+
+    N_COUNTERS = 8
+    (C_ACTIVE, C_FREE, C_NEXT_ID, C_BOUNDED, C_POPPED, C_KEPT_TOTAL, C_ITER, C_OVERFLOW) = range(8)
+
+    def __init__(self, graph: Graph, lo: torch.Tensor, hi: torch.Tensor, rhs: Optional[torch.Tensor] = None,
+                 device="cuda", batch: int = 2048, model: Optional[torch.nn.Module] = None,
+                 capacity: Optional[int] = None, sb_coeff_thresh: float = 1e-3, sb_min_width_ratio: float = 1e-3,
+                 ibp_enhancement: bool = True, chunk: int = 8, use_graph: bool = True,
+                 engine: Optional[CrownEngine] = None, engine_mode: str = "auto", cta_threads: int = 128):
+        """capacity: queue slots (default 256 x batch); each iteration grows the open list by at
+        most `batch`, and a replay of `chunk` iterations starts only with that much room."""
+        self.device = torch.device(device)
+        self.graph = graph
+        self.batch = int(batch)
+        self.chunk = max(1, int(chunk))
+        self.use_graph = use_graph
+        self.model = model
+        self.coeff_thresh = sb_coeff_thresh
+        self.min_width_ratio = sb_min_width_ratio
+        self.ibp_enhancement = ibp_enhancement
+        self.engine = engine if engine is not None else CrownEngine(graph, mode=engine_mode, cta_threads=cta_threads)
+        if self.engine.mode == "auto":
+            gen = torch.Generator(device="cpu").manual_seed(0)
+            r0, r1 = lo.reshape(1, -1).cpu().double(), hi.reshape(1, -1).cpu().double()
+            c = r0 + (r1 - r0) * torch.rand(batch, r0.shape[1], generator=gen, dtype=torch.float64)
+            w = (r1 - r0) * torch.rand(batch, r0.shape[1], generator=gen, dtype=torch.float64) * 0.25
+            self.engine.freeze(torch.maximum(r0, c - w).to(self.device), torch.minimum(r1, c + w).to(self.device))
+        self.n, self.S = self.engine.n, self.engine.S
+        dev = self.device
+        root_lo = lo.reshape(-1).to(torch.float64).cpu().contiguous()
+        root_hi = hi.reshape(-1).to(torch.float64).cpu().contiguous()
+        self.capacity = int(capacity or 256 * self.batch)
+        L = _lib.lib()
+        h = ctypes.c_void_p()
+        _lib.check(L.gear_queue_create(self.n, self.S, self.capacity, self.batch, root_lo.data_ptr(),
+                                       root_hi.data_ptr(), ctypes.byref(h)), "gear_queue_create")
+        self.q = h
+        self.plo = torch.empty(self.batch, self.n, dtype=torch.float64, device=dev)
+        self.phi = torch.empty_like(self.plo)
+        self.inc = torch.full((1,), math.inf, dtype=torch.float64, device=dev)
+        self.x_best = ((root_lo + root_hi) / 2).to(dev)
+        rhs = torch.zeros(self.S - 1, dtype=torch.float64) if rhs is None else rhs.to(torch.float64).reshape(-1)
+        self.rhs = torch.cat([rhs.to(dev), torch.zeros(1, dtype=torch.float64, device=dev)])   # never empty
+        self.ws = torch.empty(int(L.gear_bab_step_workspace_bytes(self.engine.handle, self.batch)), dtype=torch.uint8,
+                              device=dev)
+        self.counters = torch.zeros(self.N_COUNTERS, dtype=torch.int64, device=dev)
+        self.dual = torch.full((1,), -math.inf, dtype=torch.float64, device=dev)
+        self.graph_obj = None
+        self.incumbent = math.inf
+        self.replays = 0
+        self.status = {}
+
+    def __del__(self):
+        q = getattr(self, "q", None)
+        if q is not None and q.value:
+            try:
+                self.graph_obj = None
+                _lib.lib().gear_queue_destroy(q)
+            except Exception:
+                pass
+            self.q = None
+
+    def _propose(self):
+        """Best feasible model value among the popped boxes' midpoints into the device incumbent."""
+        if self.model is None:
+            return
+        with torch.no_grad():
+            x = (self.plo + self.phi) / 2
+            y = self.model(x)
+            if y.shape[1] > 1:
+                feas = (y[:, 1:] <= self.rhs[:self.S - 1]).all(1)
+            else:
+                feas = torch.ones(y.shape[0], dtype=torch.bool, device=self.device)
+            obj = torch.where(feas, y[:, 0], torch.full_like(y[:, 0], math.inf))
+            best = obj.min(0)
+            val = best.values.reshape(1)
+            pt = x.index_select(0, best.indices.reshape(1)).reshape(-1)
+            self.x_best.copy_(torch.where(val < self.inc, pt, self.x_best))
+            self.inc.copy_(torch.minimum(self.inc, val))
+
+    def _iteration(self):
+        L = _lib.lib()
+        st = torch.cuda.current_stream(self.device).cuda_stream
+        _lib.check(L.gear_queue_pop(self.q, self.plo.data_ptr(), self.phi.data_ptr(), st), "gear_queue_pop")
+        self._propose()
+        _lib.check(L.gear_bab_step(self.q, self.engine.handle, self.plo.data_ptr(), self.phi.data_ptr(),
+                                   self.inc.data_ptr(), self.rhs.data_ptr(), self.coeff_thresh, self.min_width_ratio,
+                                   1 if self.ibp_enhancement else 0, self.ws.data_ptr(), self.ws.numel(), st),
+                   "gear_bab_step")
+
+    def _chunk(self):
+        for _ in range(self.chunk):
+            self._iteration()
+        L = _lib.lib()
+        _lib.check(L.gear_queue_counters(self.q, self.counters.data_ptr(), self.dual.data_ptr(),
+                                         torch.cuda.current_stream(self.device).cuda_stream), "gear_queue_counters")
+
+    def _read(self):
+        vals = torch.cat([self.counters.to(torch.float64), self.dual, self.inc]).tolist()
+        c = [int(v) for v in vals[:self.N_COUNTERS]]
+        self.status = dict(open=c[self.C_ACTIVE], bounded=c[self.C_BOUNDED], iterations=c[self.C_ITER],
+                           kept=c[self.C_KEPT_TOTAL], overflow=c[self.C_OVERFLOW], dual=vals[-2], incumbent=vals[-1])
+        self.incumbent = vals[-1]
+        return self.status
+
+    def run(self, rel_gap: float = 1e-4, time_limit: float = 60.0, max_iterations: int = 100000):
+        """Iterate until the relative gap, an empty queue or a limit; returns (P, D, gap)."""
+        t0 = time.perf_counter()
+        st = self._read()
+        while True:
+            if st["open"] == 0 or st["iterations"] >= max_iterations or time.perf_counter() - t0 > time_limit:
+                break
+            if st["open"] + self.chunk * self.batch > self.capacity:
+                raise RuntimeError(f"gear_queue capacity {self.capacity} too small for {st['open']} open domains "
+                                   f"plus a replay of {self.chunk} iterations of {self.batch}")
+            if self.use_graph:
+                if self.graph_obj is None:
+                    self._chunk()                       # eager first chunk: loads, workspaces, warm caches
+                    torch.cuda.synchronize(self.device)
+                    g = torch.cuda.CUDAGraph()
+                    with torch.cuda.graph(g):
+                        self._chunk()
+                    self.graph_obj = g
+                    st = self._read()                   # the captured chunk did not run yet
+                    gap = self._gap(st["incumbent"], st["dual"])
+                    if gap <= rel_gap:
+                        break
+                    continue
+                self.graph_obj.replay()
+            else:
+                self._chunk()
+            self.replays += 1
+            st = self._read()
+            if st["overflow"]:
+                raise RuntimeError("gear_queue overflow: children were not pushed")
+            if self._gap(st["incumbent"], st["dual"]) <= rel_gap:
+                break
+        return st["incumbent"], st["dual"], self._gap(st["incumbent"], st["dual"])
+
+    @staticmethod
+    def _gap(P, D):
+        return BaB._gap(P, D)
+
+
+class MultiGraphBaB:
+    """Branch and bound on many instances at once (the uneven batch), every instance's queue on
+    the device (gear_queue), and a whole round captured into one CUDA graph: for every instance
+    gear_queue_pop and its incumbent proposal (its model at the popped boxes' midpoints), one
+    prepared many-instance CROWN launch per kernel group for all the batches
+    (MultiEngine.prepare / launch_prepared), then gear_bab_step_bounded for every instance. The
+    host reads all counters, dual bounds and incumbents once per replay (`chunk` rounds); an
+    instance retires when it reaches the gap, empties its queue or fills its queue capacity, and
+    the round is captured again (for the instances still running) once the running set has shrunk
+    below `recapture` of the captured one. Each instance's search is the one GraphBaB runs for it
+    alone (same kernels, same order)."""
+
+    def __init__(self, graphs, roots, models=None, rhs=None, batch: int = 256, engine=None, programs=None,
+                 device="cuda", ibp_enhancement: bool = True, sb_coeff_thresh: float = 1e-3,
+                 sb_min_width_ratio: float = 1e-3, chunk: int = 2, queue_bytes: int = 64 << 20,
+                 recapture: float = 0.8):
+        """queue_bytes: device memory of one instance's queue (its capacity in slots follows from
+        its width); roots: [(lo (1, n_i), hi (1, n_i))]."""
+        from .engine import MultiEngine
+        self.device = dev = torch.device(device)
+        self.engine = engine if engine is not None else MultiEngine(graphs, programs=programs)
+        N = len(graphs)
+        self.N, self.batch, self.chunk = N, int(batch), max(1, int(chunk))
+        self.recapture = recapture
+        self.coeff_thresh, self.min_width_ratio = sb_coeff_thresh, sb_min_width_ratio
+        self.models = list(models) if models is not None else [None] * N
+        self.n, self.S = list(self.engine.n), list(self.engine.S)
+        L = _lib.lib()
+        self.inc = torch.full((N,), math.inf, dtype=torch.float64, device=dev)
+        self.counters = torch.zeros(N, GraphBaB.N_COUNTERS, dtype=torch.int64, device=dev)
+        self.dual = torch.full((N,), -math.inf, dtype=torch.float64, device=dev)
+        self.boxes, self.x_best, self.rhs, self.queues, self.caps = [], [], [], [], []
+        for i in range(N):
+            n, S = self.n[i], self.S[i]
+            lo = roots[i][0].reshape(-1).to(torch.float64).cpu().contiguous()
+            hi = roots[i][1].reshape(-1).to(torch.float64).cpu().contiguous()
+            slot_bytes = 8 * (2 * n + S + 2) + 12
+            cap = max((self.chunk + 3) * self.batch, min(256 * self.batch, queue_bytes // slot_bytes))
+            h = ctypes.c_void_p()
+            _lib.check(L.gear_queue_create(n, S, cap, self.batch, lo.data_ptr(), hi.data_ptr(), ctypes.byref(h)),
+                       "gear_queue_create")
+            self.queues.append(h)
+            self.caps.append(cap)
+            self.boxes.append((torch.empty(self.batch, n, dtype=torch.float64, device=dev),
+                               torch.empty(self.batch, n, dtype=torch.float64, device=dev)))
+            self.x_best.append(((lo + hi) / 2).to(dev))
+            r = rhs[i] if rhs is not None and rhs[i] is not None else torch.zeros(S - 1, dtype=torch.float64)
+            self.rhs.append(torch.cat([r.to(torch.float64).reshape(-1).to(dev),
+                                       torch.zeros(1, dtype=torch.float64, device=dev)]))
+        self.outs = self.engine.outputs([self.batch] * N, dev)
+        self.ibp = ([torch.empty(self.batch, self.S[i], dtype=torch.float64, device=dev) for i in range(N)]
+                    if ibp_enhancement else None)
+        self.graph_obj = None
+        self.captured = ()
+        self.replays = 0
+        self.captures = 0
+
+    def __del__(self):
+        try:
+            self.graph_obj = None
+            self.engine.release_prepared()
+            L = _lib.lib()
+            for h in getattr(self, "queues", []):
+                if h is not None and h.value:
+                    L.gear_queue_destroy(h)
+            self.queues = []
+        except Exception:
+            pass
+
+    def _propose(self, i):
+        m = self.models[i]
+        if m is None:
+            return
+        plo, phi = self.boxes[i]
+        S = self.S[i]
+        with torch.no_grad():
+            x = (plo + phi) / 2
+            y = m(x)
+            feas = (y[:, 1:] <= self.rhs[i][:S - 1]).all(1) if y.shape[1] > 1 else \
+                torch.ones(y.shape[0], dtype=torch.bool, device=self.device)
+            obj = torch.where(feas, y[:, 0], torch.full_like(y[:, 0], math.inf))
+            best = obj.min(0)
+            val = best.values.reshape(1)
+            pt = x.index_select(0, best.indices.reshape(1)).reshape(-1)
+            inc = self.inc[i:i + 1]
+            self.x_best[i].copy_(torch.where(val < inc, pt, self.x_best[i]))
+            inc.copy_(torch.minimum(inc, val))
+
+    def _round(self, run):
+        L = _lib.lib()
+        st = torch.cuda.current_stream(self.device).cuda_stream
+        for i in run:
+            plo, phi = self.boxes[i]
+            _lib.check(L.gear_queue_pop(self.queues[i], plo.data_ptr(), phi.data_ptr(), st), "gear_queue_pop")
+            self._propose(i)
+        self.engine.launch_prepared()
+        for i in run:
+            plo, phi = self.boxes[i]
+            lb, lA, lbias = self.outs[i]
+            _lib.check(L.gear_bab_step_bounded(self.queues[i], plo.data_ptr(), phi.data_ptr(), lb.data_ptr(),
+                                               lA.data_ptr(), lbias.data_ptr(), self.inc[i:i + 1].data_ptr(),
+                                               self.rhs[i].data_ptr(), self.coeff_thresh, self.min_width_ratio, st),
+                       "gear_bab_step_bounded")
+
+    def _chunk(self, run):
+        for _ in range(self.chunk):
+            self._round(run)
+        L = _lib.lib()
+        st = torch.cuda.current_stream(self.device).cuda_stream
+        for i in run:
+            _lib.check(L.gear_queue_counters(self.queues[i], self.counters[i].data_ptr(), self.dual[i:i + 1].data_ptr(),
+                                             st), "gear_queue_counters")
+
+    def _capture(self, run):
+        """Prepare the packed launch for `run`, one eager chunk, then capture a chunk."""
+        e = torch.empty(0, dtype=torch.float64, device=self.device)
+        boxes = [self.boxes[i] if i in run else (e.view(0, self.n[i]), e.view(0, self.n[i])) for i in range(self.N)]
+        ibp = [self.ibp[i] if i in run else None for i in range(self.N)] if self.ibp is not None else None
+        self.graph_obj = None
+        self.engine.prepare(boxes, self.outs, ibp)
+        self._chunk(run)
+        torch.cuda.synchronize(self.device)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self._chunk(run)
+        self.graph_obj = g
+        self.captured = tuple(run)
+        self.captures += 1
+
+    def _read(self):
+        v = torch.cat([self.counters.reshape(-1).to(torch.float64), self.dual, self.inc]).cpu()
+        N = self.N
+        c = v[:N * GraphBaB.N_COUNTERS].reshape(N, GraphBaB.N_COUNTERS).to(torch.int64).tolist()
+        return c, v[N * GraphBaB.N_COUNTERS:N * (GraphBaB.N_COUNTERS + 1)].tolist(), v[-N:].tolist()
+
+    def run(self, rel_gap: float = 1e-4, time_limit: float = 60.0, max_rounds: int = 100000):
+        """Until every instance reaches the gap, empties its queue or fills its capacity, or a limit.
+        Returns per instance: incumbent, dual bound, gap, wall time to the gap (None if not
+        reached), status, domains bounded (counted up to the instance's retirement)."""
+        t0 = time.perf_counter()
+        N = self.N
+        res = [dict(P=math.inf, D=-math.inf, gap=math.inf, time_to_gap=None, status="running", bounded=0)
+               for _ in range(N)]
+        running = list(range(N))
+        rounds = 0
+        while running and rounds < max_rounds and time.perf_counter() - t0 < time_limit:
+            if self.graph_obj is None or len(running) < self.recapture * len(self.captured):
+                self._capture(running)
+                rounds += self.chunk
+            else:
+                self.graph_obj.replay()
+                self.replays += 1
+                rounds += self.chunk
+            c, D, P = self._read()
+            now = time.perf_counter() - t0
+            nxt = []
+            for i in running:
+                g = BaB._gap(P[i], D[i])
+                r = res[i]
+                r.update(P=P[i], D=D[i], gap=g, bounded=c[i][GraphBaB.C_BOUNDED])
+                if g <= rel_gap:
+                    r.update(time_to_gap=now, status="closed")
+                elif c[i][GraphBaB.C_ACTIVE] == 0:
+                    r.update(status="emptied")
+                elif c[i][GraphBaB.C_ACTIVE] + self.chunk * self.batch > self.caps[i] or c[i][GraphBaB.C_OVERFLOW]:
+                    r.update(status="capacity")
+                else:
+                    nxt.append(i)
+            running = nxt
+        self.rounds = rounds
+        return res

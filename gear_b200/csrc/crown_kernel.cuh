@@ -1434,8 +1434,9 @@ __device__ __forceinline__ void cta_load(Box& bx, const int32_t* hdr, const Work
 }
 
 // Schedule step si of the bound program for the current box (a CROWN pass: ops [op_lo, op_hi)
-// and the phases of run_pass).
-template <int NT, bool WHOLE = true, bool IDX = false>
+// and the phases of run_pass). FX: the fold step may read the batch's tensor-core fold vectors
+// (Work::fold_ext); a separate instance, so the kernels without it keep their register budget.
+template <int NT, bool WHOLE = true, bool IDX = false, bool FX = false>
 __device__ __forceinline__ void cta_step(const DevProgram& P, Box& bx, double* tmp_lo, double* tmp_hi, int32_t* sops,
                                          const Work& wk, double* work, int si, int op_lo = 0, int op_hi = 1 << 30,
                                          int phase = 3) {
@@ -1445,7 +1446,7 @@ __device__ __forceinline__ void cta_step(const DevProgram& P, Box& bx, double* t
   const int type = st[0], a = st[1];
   switch (type) {
     case ST_FOLD:
-      if (wk.fold_ext && !bx.open && *wk.fold_fail == 0) {
+      if (FX && wk.fold_ext && !bx.open && *wk.fold_fail == 0) {
         // tensor-core fold vectors of this box (a box with a non-finite centre or radius folds
         // here, as the reference's dense product does)
         const int32_t* nd = node_rec(&P, a);
@@ -1497,7 +1498,7 @@ __device__ __forceinline__ void cta_step(const DevProgram& P, Box& bx, double* t
 }
 
 // The whole schedule for box b of wk on the bound program.
-template <int NT, bool IDX = false>
+template <int NT, bool IDX = false, bool FX = false>
 __device__ __forceinline__ void cta_box(const DevProgram& P, Box& bx, double* tmp_lo, double* tmp_hi, int32_t* sops,
                                         const Work& wk, int64_t b, double* work) {
   const int nsteps = P.hdr[H_NSTEPS];
@@ -1506,7 +1507,7 @@ __device__ __forceinline__ void cta_box(const DevProgram& P, Box& bx, double* tm
 #ifdef GEAR_STEP_PROFILE
     long long t_step = clock64();
 #endif
-    cta_step<NT, true, IDX>(P, bx, tmp_lo, tmp_hi, sops, wk, work, si);
+    cta_step<NT, true, IDX, FX>(P, bx, tmp_lo, tmp_hi, sops, wk, work, si);
     __syncthreads();
 #ifdef GEAR_STEP_PROFILE
     if (threadIdx.x == 0 && si < 8192) atomicAdd(&g_step_cycles[si], (unsigned long long)(clock64() - t_step));
@@ -1515,8 +1516,9 @@ __device__ __forceinline__ void cta_box(const DevProgram& P, Box& bx, double* tm
 }
 
 // GWS: the program keeps its pass working set in global memory (H_PASS_GLOBAL > 0). A separate
-// instance per address space keeps the shared-memory one on shared loads and stores.
-template <int NT, bool GWS>
+// instance per address space keeps the shared-memory one on shared loads and stores. FX: the
+// program's fold vectors come from the tensor-core fold (H_FOLD_TC, shared-memory programs only).
+template <int NT, bool GWS, bool FX = false>
 __global__ void __launch_bounds__(NT, GEAR_CTA_MINB / NT) crown_megakernel(DevProgram Pg, Work wk) {
   extern __shared__ double sm[];
   DevProgram P;
@@ -1524,7 +1526,7 @@ __global__ void __launch_bounds__(NT, GEAR_CTA_MINB / NT) crown_megakernel(DevPr
   double *tmp_lo, *tmp_hi, *work;
   int32_t* sops = cta_bind<NT>(P, bx, tmp_lo, tmp_hi, work, Pg, sm, wk.scratch + (size_t)blockIdx.x * wk.slot_doubles);
   for (int64_t b = blockIdx.x; b < wk.B; b += gridDim.x)
-    cta_box<NT, GWS>(P, bx, tmp_lo, tmp_hi, sops, wk, b, GWS ? work : sm);
+    cta_box<NT, GWS, FX>(P, bx, tmp_lo, tmp_hi, sops, wk, b, GWS ? work : sm);
 }
 
 // ------------------------------------------------------------------ the plain (unfused) form

@@ -5,6 +5,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <map>
 #include <mutex>
 #include <new>
 #include <string>
@@ -17,6 +18,7 @@
 #include "concretize_kernels.cuh"
 #include "dual_kernels.cuh"
 #include "fold_tc.cuh"
+#include "bab_queue.cuh"
 
 namespace {
 thread_local std::string g_err;
@@ -176,43 +178,68 @@ int tc_launch(const gear_dag* d, const double* x_L, const double* x_U, int64_t b
 }
 }  // namespace
 
+// The dynamic shared-memory limit of a kernel (a cap on what a launch may request), raised when
+// a launch needs more than the value set so far on this device and never lowered: launches that
+// fit make no attribute call, so the iterations of a branch-and-bound run can be captured into a
+// CUDA graph after their first eager run.
+static std::mutex g_smem_attr_mu;
+static std::map<std::pair<const void*, int>, int> g_smem_attr;
+static cudaError_t set_smem_limit(const void* func, int bytes) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(g_smem_attr_mu);
+  auto key = std::make_pair(func, dev);
+  auto it = g_smem_attr.find(key);
+  if (it != g_smem_attr.end() && it->second >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) g_smem_attr[key] = bytes;
+  return e;
+}
+
 // box-per-CTA kernel instances: dynamic shared-memory limit and resident CTAs per SM
-// (GWS: the program keeps its pass working set in global memory, a kernel instance of its own)
-template <int NT, bool GWS>
+// (GWS: the program keeps its pass working set in global memory, a kernel instance of its own;
+// FX: its fold vectors come from the tensor-core fold, shared-memory programs only)
+template <int NT, bool GWS, bool FX>
 cudaError_t cta_occupancy_t(int smem_bytes, int* bps) {
-  cudaError_t e = cudaFuncSetAttribute(gear::crown_megakernel<NT, GWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       smem_bytes);
+  cudaError_t e = set_smem_limit((const void*)gear::crown_megakernel<NT, GWS, FX>, smem_bytes);
   if (e != cudaSuccess) return e;
 #ifdef GEAR_CTA_CARVEOUT
   // shared-memory share of the unified L1 (percent) for builds that fix it
-  e = cudaFuncSetAttribute(gear::crown_megakernel<NT, GWS>, cudaFuncAttributePreferredSharedMemoryCarveout,
+  e = cudaFuncSetAttribute(gear::crown_megakernel<NT, GWS, FX>, cudaFuncAttributePreferredSharedMemoryCarveout,
                            GEAR_CTA_CARVEOUT);
   if (e != cudaSuccess) return e;
 #endif
 
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, gear::crown_megakernel<NT, GWS>, NT, smem_bytes);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, gear::crown_megakernel<NT, GWS, FX>, NT, smem_bytes);
 }
-static cudaError_t cta_occupancy(int threads, bool gws, int smem_bytes, int* bps) {
+template <int NT>
+cudaError_t cta_occupancy_nt(bool gws, bool fx, int smem_bytes, int* bps) {
+  if (gws) return cta_occupancy_t<NT, true, false>(smem_bytes, bps);
+  return fx ? cta_occupancy_t<NT, false, true>(smem_bytes, bps) : cta_occupancy_t<NT, false, false>(smem_bytes, bps);
+}
+static cudaError_t cta_occupancy(int threads, bool gws, bool fx, int smem_bytes, int* bps) {
   switch (threads) {
-    case 64: return gws ? cta_occupancy_t<64, true>(smem_bytes, bps) : cta_occupancy_t<64, false>(smem_bytes, bps);
-    case 128: return gws ? cta_occupancy_t<128, true>(smem_bytes, bps) : cta_occupancy_t<128, false>(smem_bytes, bps);
-    case 256: return gws ? cta_occupancy_t<256, true>(smem_bytes, bps) : cta_occupancy_t<256, false>(smem_bytes, bps);
+    case 64: return cta_occupancy_nt<64>(gws, fx, smem_bytes, bps);
+    case 128: return cta_occupancy_nt<128>(gws, fx, smem_bytes, bps);
+    case 256: return cta_occupancy_nt<256>(gws, fx, smem_bytes, bps);
     default: return cudaErrorInvalidValue;
   }
 }
-template <int NT, bool GWS>
+template <int NT, bool GWS, bool FX>
 cudaError_t cta_launch_t(const gear::DevProgram& P, const gear::Work& wk, int64_t slots, int smem_bytes, cudaStream_t st) {
   // the kernel's dynamic shared-memory limit is per function: set it for this program
-  cudaError_t e = cudaFuncSetAttribute(gear::crown_megakernel<NT, GWS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       smem_bytes);
+  cudaError_t e = set_smem_limit((const void*)gear::crown_megakernel<NT, GWS, FX>, smem_bytes);
   if (e != cudaSuccess) return e;
-  gear::crown_megakernel<NT, GWS><<<(unsigned)slots, NT, smem_bytes, st>>>(P, wk);
+  gear::crown_megakernel<NT, GWS, FX><<<(unsigned)slots, NT, smem_bytes, st>>>(P, wk);
   return cudaGetLastError();
 }
 template <int NT>
 cudaError_t cta_launch_any(const gear::DevProgram& P, const gear::Work& wk, int64_t slots, int smem_bytes, bool gws,
                            cudaStream_t st) {
-  return gws ? cta_launch_t<NT, true>(P, wk, slots, smem_bytes, st) : cta_launch_t<NT, false>(P, wk, slots, smem_bytes, st);
+  if (gws) return cta_launch_t<NT, true, false>(P, wk, slots, smem_bytes, st);
+  return wk.fold_ext ? cta_launch_t<NT, false, true>(P, wk, slots, smem_bytes, st)
+                     : cta_launch_t<NT, false, false>(P, wk, slots, smem_bytes, st);
 }
 
 extern "C" const char* gear_last_error(void) { return g_err.c_str(); }
@@ -292,7 +319,12 @@ extern "C" int gear_dag_create(const int32_t* header, int64_t header_len, const 
       delete d;
       return fail(GEAR_E_INVALID, "gear_dag_create: %s", "pass working set exceeds shared memory");
     }
-    e = cta_occupancy(d->threads, header[H_PASS_GLOBAL] > 0, d->smem_bytes, &bps);
+    if (header[H_PASS_GLOBAL] > 0 && header[H_FOLD_TC] != 0) {
+      cudaFree(d->dev);
+      delete d;
+      return fail(GEAR_E_INVALID, "gear_dag_create: %s", "the tensor-core fold needs the pass working set in shared memory");
+    }
+    e = cta_occupancy(d->threads, header[H_PASS_GLOBAL] > 0, header[H_FOLD_TC] != 0, d->smem_bytes, &bps);
     if (e == cudaErrorInvalidValue) {
       cudaFree(d->dev);
       delete d;
@@ -633,8 +665,7 @@ static int plain_impl(const gear_dag* dag, const double* x_L, const double* x_U,
 namespace {
 template <int NT, bool GWS>
 cudaError_t multi_cta_occupancy_t(int smem_bytes, int* bps) {
-  cudaError_t e = cudaFuncSetAttribute(gear::crown_multi_megakernel<NT, GWS>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+  cudaError_t e = set_smem_limit((const void*)gear::crown_multi_megakernel<NT, GWS>, smem_bytes);
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(bps, gear::crown_multi_megakernel<NT, GWS>, NT, smem_bytes);
 }
@@ -726,6 +757,69 @@ struct Staging {
 thread_local Staging g_staging[kMaxDevices];
 }  // namespace
 
+namespace {
+// The instance table and the work-item prefix of a launch, written to host memory at `host`
+// (laid out as the workspace from items_off on).
+void multi_table(const gear_lower_args* items, int32_t count, const MultiPlan& pl, char* host) {
+  gear::MultiItem* hitems = (gear::MultiItem*)host;
+  int64_t* hstart = (int64_t*)(host + (pl.start_off - pl.items_off));
+  int k = 0;
+  hstart[0] = 0;
+  for (int32_t i = 0; i < count; ++i) {
+    const gear_lower_args& a = items[i];
+    if (a.batch == 0) continue;
+    gear::MultiItem& it = hitems[k];
+    it.P = a.dag->P;
+    it.wk.xL = a.x_L;
+    it.wk.xU = a.x_U;
+    it.wk.C = a.C;
+    it.wk.lb = a.lb;
+    it.wk.lA = a.lA;
+    it.wk.lbias = a.lbias;
+    it.wk.lb_ibp = a.lb_ibp;
+    it.wk.scratch = nullptr;
+    it.wk.slot_doubles = pl.slot_doubles;
+    it.wk.B = a.batch;
+    it.wk.status = nullptr;
+    it.wk.fold_ext = nullptr;
+    it.wk.fold_fail = nullptr;
+    hstart[k + 1] = hstart[k] + (a.batch + a.dag->boxes_per_slot - 1) / a.dag->boxes_per_slot;
+    ++k;
+  }
+}
+
+// The launch of a planned many-instance call whose table is already in the workspace.
+int multi_launch(const MultiPlan& pl, char* ws, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(ws, 0, sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return cuda_fail(e, "crown multi-instance launch");
+  const gear::MultiItem* ditems = (const gear::MultiItem*)(ws + pl.items_off);
+  const int64_t* dstart = (const int64_t*)(ws + pl.start_off);
+  unsigned long long* next = (unsigned long long*)ws;
+  double* scratch = (double*)(ws + pl.scratch_off);
+  const unsigned grid = (unsigned)pl.slots;
+  if (pl.mode == gear::MODE_SIMT) {
+    gear::crown_multi_simt_kernel<<<grid, gear::SIMT_T, 0, st>>>(ditems, pl.count, dstart, next, scratch,
+                                                                  pl.slot_doubles);
+  } else {
+    switch (pl.threads) {
+      case 64: multi_cta_launch<64>(pl.gws, grid, pl.smem, st, ditems, pl.count, dstart, next, scratch, pl.slot_doubles); break;
+      case 128: multi_cta_launch<128>(pl.gws, grid, pl.smem, st, ditems, pl.count, dstart, next, scratch, pl.slot_doubles); break;
+      default: multi_cta_launch<256>(pl.gws, grid, pl.smem, st, ditems, pl.count, dstart, next, scratch, pl.slot_doubles); break;
+    }
+  }
+  e = cudaGetLastError();
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "crown multi-instance launch");
+}
+}  // namespace
+
+// A many-instance launch prepared once: its plan, and its instance table already in the caller's
+// workspace, so that every later launch (gear_crown_multi_launch) is a counter reset and one
+// kernel with fixed arguments, which a CUDA graph can capture.
+struct gear_multi_plan {
+  MultiPlan pl;
+  char* ws = nullptr;
+};
+
 extern "C" int64_t gear_crown_multi_workspace_bytes(const gear_lower_args* items, int32_t count) {
   MultiPlan pl;
   if (multi_plan(items, count, pl) != GEAR_OK) return -1;
@@ -765,53 +859,51 @@ extern "C" int gear_crown_lower_multi(const gear_lower_args* items, int32_t coun
     e = cudaEventCreateWithFlags(&sg.done, cudaEventDisableTiming);
     if (e != cudaSuccess) return cuda_fail(e, "gear_crown_lower_multi staging");
   }
-  gear::MultiItem* hitems = (gear::MultiItem*)sg.host;
-  int64_t* hstart = (int64_t*)((char*)sg.host + (pl.start_off - pl.items_off));
-  int k = 0;
-  hstart[0] = 0;
-  for (int32_t i = 0; i < count; ++i) {
-    const gear_lower_args& a = items[i];
-    if (a.batch == 0) continue;
-    gear::MultiItem& it = hitems[k];
-    it.P = a.dag->P;
-    it.wk.xL = a.x_L;
-    it.wk.xU = a.x_U;
-    it.wk.C = a.C;
-    it.wk.lb = a.lb;
-    it.wk.lA = a.lA;
-    it.wk.lbias = a.lbias;
-    it.wk.lb_ibp = a.lb_ibp;
-    it.wk.scratch = nullptr;
-    it.wk.slot_doubles = pl.slot_doubles;
-    it.wk.B = a.batch;
-    it.wk.status = nullptr;
-    it.wk.fold_ext = nullptr;
-    it.wk.fold_fail = nullptr;
-    hstart[k + 1] = hstart[k] + (a.batch + a.dag->boxes_per_slot - 1) / a.dag->boxes_per_slot;
-    ++k;
-  }
-  e = cudaMemsetAsync(ws, 0, sizeof(unsigned long long), st);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(ws + pl.items_off, sg.host, table_bytes, cudaMemcpyHostToDevice, st);
+  multi_table(items, count, pl, (char*)sg.host);
+  e = cudaMemcpyAsync(ws + pl.items_off, sg.host, table_bytes, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaEventRecord(sg.done, st);
   if (e != cudaSuccess) return cuda_fail(e, "gear_crown_lower_multi table upload");
-  const gear::MultiItem* ditems = (const gear::MultiItem*)(ws + pl.items_off);
-  const int64_t* dstart = (const int64_t*)(ws + pl.start_off);
-  unsigned long long* next = (unsigned long long*)ws;
-  double* scratch = (double*)(ws + pl.scratch_off);
-  const unsigned grid = (unsigned)pl.slots;
-  if (pl.mode == gear::MODE_SIMT) {
-    gear::crown_multi_simt_kernel<<<grid, gear::SIMT_T, 0, st>>>(ditems, pl.count, dstart, next, scratch,
-                                                                  pl.slot_doubles);
-  } else {
-    switch (pl.threads) {
-      case 64: multi_cta_launch<64>(pl.gws, grid, pl.smem, st, ditems, pl.count, dstart, next, scratch, pl.slot_doubles); break;
-      case 128: multi_cta_launch<128>(pl.gws, grid, pl.smem, st, ditems, pl.count, dstart, next, scratch, pl.slot_doubles); break;
-      default: multi_cta_launch<256>(pl.gws, grid, pl.smem, st, ditems, pl.count, dstart, next, scratch, pl.slot_doubles); break;
-    }
+  rc = multi_launch(pl, ws, st);
+  if (rc == GEAR_OK) g_launches = 1;
+  return rc;
+}
+
+extern "C" int gear_crown_multi_prepare(const gear_lower_args* items, int32_t count, void* workspace,
+                                        int64_t workspace_bytes, gear_multi_plan** out) {
+  g_launches = 0;
+  if (!out) return fail(GEAR_E_INVALID, "gear_crown_multi_prepare: %s", "bad arguments");
+  MultiPlan pl;
+  int rc = multi_plan(items, count, pl);
+  if (rc != GEAR_OK) return rc;
+  if (pl.count > 0 && (!workspace || workspace_bytes < pl.bytes))
+    return fail(GEAR_E_WORKSPACE, "gear_crown_multi_prepare: %s", "workspace too small");
+  gear_multi_plan* p = new (std::nothrow) gear_multi_plan();
+  if (!p) return fail(GEAR_E_NOMEM, "gear_crown_multi_prepare: %s", "host allocation");
+  p->pl = pl;
+  p->ws = (char*)workspace;
+  if (pl.count > 0) {
+    const size_t table_bytes = (size_t)(pl.start_off - pl.items_off) + (size_t)(pl.count + 1) * sizeof(int64_t);
+    std::vector<char> host(table_bytes);
+    multi_table(items, count, pl, host.data());
+    cudaError_t e = cudaMemcpy(p->ws + pl.items_off, host.data(), table_bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { delete p; return cuda_fail(e, "gear_crown_multi_prepare table upload"); }
   }
-  g_launches = 1;
-  e = cudaGetLastError();
-  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "crown multi-instance launch");
+  *out = p;
+  return GEAR_OK;
+}
+
+extern "C" int gear_crown_multi_launch(const gear_multi_plan* plan, void* stream) {
+  g_launches = 0;
+  if (!plan) return fail(GEAR_E_INVALID, "gear_crown_multi_launch: %s", "bad arguments");
+  if (plan->pl.count == 0) return GEAR_OK;
+  const int rc = multi_launch(plan->pl, plan->ws, (cudaStream_t)stream);
+  if (rc == GEAR_OK) g_launches = 1;
+  return rc;
+}
+
+extern "C" int gear_crown_multi_plan_destroy(gear_multi_plan* plan) {
+  delete plan;
+  return GEAR_OK;
 }
 
 // ------------------------------------------------------------------ branch and bound
@@ -907,7 +999,7 @@ extern "C" int gear_queue_order(const double* key, const int64_t* id, const int3
   if (n2 <= SORT_SMEM_MAX) {
     // the whole network in one CTA (one launch instead of log2(n2)(log2(n2)+1)/2)
     const size_t smem = (size_t)n2 * (sizeof(double) + sizeof(int64_t) + sizeof(int32_t));
-    cudaError_t ea = cudaFuncSetAttribute(bitonic_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t ea = set_smem_limit((const void*)bitonic_smem, (int)smem);
     if (ea != cudaSuccess) return cuda_fail(ea, "cudaFuncSetAttribute");
     bitonic_smem<<<1, SORT_THREADS, smem, st>>>(order, key, id, (int)n2);
     launches = 1;
@@ -1010,6 +1102,297 @@ extern "C" int gear_bab_compact(const uint8_t* keep, int64_t batch, int32_t* kep
   g_launches = 3;
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_bab_compact");
+}
+
+// ------------------------------------------------------------------ device-resident BaB queue
+// The queue handle of gear_queue_* / gear_bab_step (bab_queue.cuh): slot arrays, ordered active
+// list, free list and counters in one device block owned by the handle, plus the buffers of one
+// iteration at the handle's batch size (popped rows' thresholds, CROWN outputs, keep mask, kept
+// list, split indices, children, sort buffer).
+struct gear_queue {
+  gear::bq::QueueDev q;
+  void* dev = nullptr;
+  int device = 0;
+  int64_t batch = 0, N2 = 1;
+  int32_t* pslot = nullptr;
+  double *thr = nullptr, *lb = nullptr, *lA = nullptr, *lbias = nullptr, *lb_ibp = nullptr, *root_width = nullptr;
+  uint8_t* keep = nullptr;
+  int32_t *kept = nullptr, *nk = nullptr, *nchild = nullptr, *split_idx = nullptr, *newslot = nullptr;
+  int32_t* block_counts = nullptr;
+  int* nonfinite = nullptr;
+  double *clo = nullptr, *chi = nullptr, *ckey = nullptr;
+};
+
+namespace {
+// Carve the handle's arrays out of one allocation (pass dev = nullptr to size it).
+int64_t queue_layout(gear_queue* h, char* dev) {
+  using namespace gear::bq;
+  const int n = h->q.n, S = h->q.S;
+  const int64_t cap = h->q.cap, B = h->batch;
+  int64_t o = 0;
+  auto take = [&](int64_t bytes) -> char* {
+    char* p = dev ? dev + o : nullptr;
+    o = align_up(o + bytes, kAlign);
+    return p;
+  };
+  h->q.lo = (double*)take(cap * n * 8);
+  h->q.hi = (double*)take(cap * n * 8);
+  h->q.key = (double*)take(cap * S * 8);
+  h->q.key0 = (double*)take(cap * 8);
+  h->q.ids = (int64_t*)take(cap * 8);
+  h->q.active = (int32_t*)take(cap * 4);
+  h->q.merged = (int32_t*)take(cap * 4);
+  h->q.free_list = (int32_t*)take(cap * 4);
+  h->q.counters = (int64_t*)take(C_COUNT * 8);
+  h->q.disc_min = (unsigned long long*)take(8);
+  h->q.root_lo = (double*)take(n * 8);
+  h->q.root_hi = (double*)take(n * 8);
+  h->root_width = (double*)take(n * 8);
+  h->pslot = (int32_t*)take(B * 4);
+  h->thr = (double*)take(B * S * 8);
+  h->lb = (double*)take(B * S * 8);
+  h->lA = (double*)take(B * S * n * 8);
+  h->lbias = (double*)take(B * S * 8);
+  h->lb_ibp = (double*)take(B * S * 8);
+  h->keep = (uint8_t*)take(B);
+  h->kept = (int32_t*)take(B * 4);
+  h->nk = (int32_t*)take(4);
+  h->nchild = (int32_t*)take(4);
+  h->split_idx = (int32_t*)take(B * 4);
+  h->newslot = (int32_t*)take(h->N2 * 4);
+  h->block_counts = (int32_t*)take(((B + gear::bab::BT - 1) / gear::bab::BT + 64) * 4);
+  h->nonfinite = (int*)take(4);
+  h->clo = (double*)take(2 * B * n * 8);
+  h->chi = (double*)take(2 * B * n * 8);
+  h->ckey = (double*)take(2 * B * S * 8);
+  return o;
+}
+
+__global__ void queue_init_kernel(gear::bq::QueueDev q, const double* root_lo, const double* root_hi,
+                                  double* root_width) {
+  using namespace gear::bq;
+  const int64_t t = (int64_t)blockIdx.x * gear::bab::BT + threadIdx.x;
+  // the root domain in slot 0 (key -inf, id 0); slots 1..cap-1 free
+  if (t < q.n) {
+    q.lo[t] = root_lo[t];
+    q.hi[t] = root_hi[t];
+    q.root_lo[t] = root_lo[t];
+    q.root_hi[t] = root_hi[t];
+    root_width[t] = root_hi[t] - root_lo[t];
+  }
+  if (t < q.S) q.key[t] = -INFINITY;
+  if (t < q.cap - 1) q.free_list[t] = (int32_t)(q.cap - 1 - t);
+  if (t == 0) {
+    q.key0[0] = -INFINITY;
+    q.ids[0] = 0;
+    q.active[0] = 0;
+    for (int c = 0; c < C_COUNT; ++c) q.counters[c] = 0;
+    q.counters[C_ACTIVE] = 1;
+    q.counters[C_FREE] = q.cap - 1;
+    q.counters[C_NEXT_ID] = 1;
+    *q.disc_min = gear::bab::ordered_bits(INFINITY);
+  }
+}
+
+// sort the N2 new slot entries (children first, -1 padding last) by (key desc, id asc)
+int queue_sort_new(gear_queue* h, cudaStream_t st) {
+  using namespace gear::bab;
+  if (h->N2 <= SORT_SMEM_MAX) {
+    const size_t smem = (size_t)h->N2 * (sizeof(double) + sizeof(int64_t) + sizeof(int32_t));
+    cudaError_t e = set_smem_limit((const void*)bitonic_smem, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+    bitonic_smem<<<1, SORT_THREADS, smem, st>>>(h->newslot, h->q.key0, h->q.ids, (int)h->N2);
+    return 1;
+  }
+  int launches = 0;
+  for (int64_t k = 2; k <= h->N2; k <<= 1)
+    for (int64_t j = k >> 1; j > 0; j >>= 1) {
+      bitonic_step<<<grid_for(h->N2), BT, 0, st>>>(h->newslot, h->q.key0, h->q.ids, h->N2, h->N2, (int)j, (int)k);
+      ++launches;
+    }
+  return launches;
+}
+
+// the domains in h->clo / chi / ckey (mult x *h->nk of them) into the active list
+int queue_push_rows(gear_queue* h, int mult, cudaStream_t st) {
+  using namespace gear::bq;
+  push_plan_kernel<<<1, 1, 0, st>>>(h->q, h->nk, mult, h->nchild);
+  const int w = h->q.n > h->q.S ? h->q.n : h->q.S;
+  push_scatter_kernel<<<grid_for(h->N2 * w), BT, 0, st>>>(h->q, h->nchild, h->clo, h->chi, h->ckey, h->N2, h->newslot);
+  int launches = 2;
+  const int s = queue_sort_new(h, st);
+  if (s < 0) return s;
+  launches += s;
+  merge_dev_kernel<<<grid_for(h->q.cap), BT, 0, st>>>(h->q, h->nchild, h->newslot);
+  merge_copy_kernel<<<grid_for(h->q.cap), BT, 0, st>>>(h->q, h->nchild);
+  push_commit_kernel<<<1, 1, 0, st>>>(h->q, h->nchild);
+  return launches + 3;
+}
+}  // namespace
+
+extern "C" int gear_queue_create(int n, int S, int64_t capacity, int64_t batch, const double* root_lo,
+                                 const double* root_hi, gear_queue** out) {
+  if (!out || n < 1 || S < 1 || batch < 1 || capacity < 2 * batch + 1 || capacity > ((int64_t)1 << 31) - 1 ||
+      !root_lo || !root_hi)
+    return fail(GEAR_E_INVALID, "gear_queue_create: %s", "bad arguments (capacity must exceed 2 x batch)");
+  gear_queue* h = new (std::nothrow) gear_queue();
+  if (!h) return fail(GEAR_E_NOMEM, "gear_queue_create: %s", "host allocation");
+  h->q.n = n;
+  h->q.S = S;
+  h->q.cap = capacity;
+  h->batch = batch;
+  while (h->N2 < 2 * batch) h->N2 <<= 1;
+  const int64_t bytes = queue_layout(h, nullptr);
+  cudaError_t e = cudaGetDevice(&h->device);
+  if (e == cudaSuccess) e = cudaMalloc(&h->dev, bytes);
+  if (e != cudaSuccess) { delete h; return cuda_fail(e, "cudaMalloc(queue)"); }
+  queue_layout(h, (char*)h->dev);
+  double* root = nullptr;
+  e = cudaMalloc(&root, 2 * n * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpy(root, root_lo, n * sizeof(double), cudaMemcpyDefault);
+  if (e == cudaSuccess) e = cudaMemcpy(root + n, root_hi, n * sizeof(double), cudaMemcpyDefault);
+  if (e == cudaSuccess) {
+    const int64_t m = capacity > n ? capacity : n;
+    queue_init_kernel<<<grid_for(m > S ? m : S), gear::bab::BT>>>(h->q, root, root + n, h->root_width);
+    e = cudaDeviceSynchronize();
+  }
+  if (root) cudaFree(root);
+  if (e != cudaSuccess) { cudaFree(h->dev); delete h; return cuda_fail(e, "gear_queue_create"); }
+  *out = h;
+  return GEAR_OK;
+}
+
+extern "C" int gear_queue_destroy(gear_queue* q) {
+  if (!q) return GEAR_OK;
+  if (q->dev) cudaFree(q->dev);
+  delete q;
+  return GEAR_OK;
+}
+
+extern "C" int gear_queue_counters(const gear_queue* q, int64_t* counters, double* dual, void* stream) {
+  if (!q || !counters) return fail(GEAR_E_INVALID, "gear_queue_counters: %s", "bad arguments");
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(counters, q->q.counters, gear::bq::C_COUNT * sizeof(int64_t), cudaMemcpyDefault, st);
+  if (e == cudaSuccess && dual) {
+    gear::bq::dual_bound_kernel<<<1, 1, 0, st>>>(q->q, dual);
+    e = cudaGetLastError();
+  }
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_queue_counters");
+}
+
+extern "C" int gear_queue_size(const gear_queue* q, int64_t* open, void* stream) {
+  if (!q || !open) return fail(GEAR_E_INVALID, "gear_queue_size: %s", "bad arguments");
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(open, q->q.counters + gear::bq::C_ACTIVE, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_queue_size");
+}
+
+extern "C" int gear_queue_push(gear_queue* q, const double* lo, const double* hi, const double* key, int64_t count,
+                               void* stream) {
+  g_launches = 0;
+  if (!q || count < 0 || count > 2 * q->batch || (count > 0 && (!lo || !hi || !key)))
+    return fail(GEAR_E_INVALID, "gear_queue_push: %s", "bad arguments (at most 2 x batch domains per push)");
+  if (count == 0) return GEAR_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int n = q->q.n, S = q->q.S;
+  cudaError_t e = cudaMemcpyAsync(q->clo, lo, count * n * sizeof(double), cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(q->chi, hi, count * n * sizeof(double), cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(q->ckey, key, count * S * sizeof(double), cudaMemcpyDeviceToDevice, st);
+  if (e != cudaSuccess) return cuda_fail(e, "gear_queue_push copy");
+  gear::bq::set_count_kernel<<<1, 1, 0, st>>>(q->nk, (int32_t)count);
+  const int l = queue_push_rows(q, 1, st);
+  if (l < 0) return l;
+  g_launches = l + 1;
+  e = cudaGetLastError();
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_queue_push");
+}
+
+extern "C" int gear_queue_pop(gear_queue* q, double* lo_out, double* hi_out, void* stream) {
+  if (!q || !lo_out || !hi_out) return fail(GEAR_E_INVALID, "gear_queue_pop: %s", "bad arguments");
+  cudaStream_t st = (cudaStream_t)stream;
+  gear::bq::pop_gather_kernel<<<grid_for(q->batch * q->q.n), gear::bab::BT, 0, st>>>(q->q, q->batch, lo_out, hi_out,
+                                                                                     q->pslot);
+  gear::bq::pop_commit_kernel<<<1, gear::bab::BT, 0, st>>>(q->q, q->batch, q->pslot);
+  g_launches = 2;
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_queue_pop");
+}
+
+extern "C" int64_t gear_bab_step_workspace_bytes(const gear_dag* dag, int64_t batch) {
+  if (!dag || batch < 1) return -1;
+  return align_up(gear_crown_workspace_bytes(dag, batch), kAlign) + kAlign;
+}
+
+static int bab_step_after_bound(gear_queue* q, const double* lo, const double* hi, const double* lb, const double* lA,
+                                const double* lbias, const double* incumbent, const double* rhs, double sb_coeff_thresh,
+                                double sb_min_width_ratio, cudaStream_t st) {
+  using namespace gear;
+  const int64_t B = q->batch;
+  const int n = q->q.n, S = q->q.S;
+  // prune against the thresholds (incumbent read on the device), drop the padding rows, compact
+  bq::thresholds_kernel<<<grid_for(B * S), bab::BT, 0, st>>>(incumbent, rhs, B, S, q->thr);
+  const int64_t nblocks = (B + bab::BT - 1) / bab::BT;
+  bab::prune_kernel<<<(unsigned)nblocks, bab::BT, 0, st>>>(lb, q->thr, B, S, q->keep, q->q.disc_min);
+  bq::mask_padding_kernel<<<(unsigned)nblocks, bab::BT, 0, st>>>(q->q.counters, B, q->keep);
+  bab::count_kernel<<<(unsigned)nblocks, bab::BT, 0, st>>>(q->keep, B, q->block_counts);
+  bab::scan_counts_kernel<<<1, bab::BT, 0, st>>>(q->block_counts, (int)nblocks, q->nk);
+  bab::compact_kernel<<<(unsigned)nblocks, bab::BT, 0, st>>>(q->keep, B, q->block_counts, q->kept);
+  // branch: SB score, top-1, width guard
+  cudaError_t e = cudaMemsetAsync(q->nonfinite, 0, sizeof(int), st);
+  if (e != cudaSuccess) return cuda_fail(e, "gear_bab_step");
+  const int64_t nA = B * (int64_t)S * n, nS = B * (int64_t)S;
+  bab::nonfinite_kernel<<<grid_for(nA < ((int64_t)1 << 26) ? nA : ((int64_t)1 << 26)), bab::BT, 0, st>>>(
+      lA, nA, lb, q->thr, nS, q->nonfinite);
+  bab::branch_kernel<<<grid_for(B * 32), bab::BT, 0, st>>>(lA, lo, hi, B, S, n, q->root_width, sb_coeff_thresh,
+                                                           sb_min_width_ratio, q->nonfinite, q->split_idx);
+  // split the kept parents, key the children, push them
+  bq::split_dev_kernel<<<grid_for(2 * B * n), bab::BT, 0, st>>>(lo, hi, q->kept, q->nk, n, q->split_idx, q->clo,
+                                                                  q->chi);
+  bq::child_keys_dev_kernel<<<grid_for(2 * B * 32), bab::BT, 0, st>>>(lb, lA, lbias, q->clo, q->chi, q->kept, q->nk, S,
+                                                                      n, q->ckey);
+  const int l = queue_push_rows(q, 2, st);
+  if (l < 0) return l;
+  e = cudaGetLastError();
+  return e == cudaSuccess ? 11 + l : cuda_fail(e, "gear_bab_step");
+}
+
+extern "C" int gear_bab_step(gear_queue* q, const gear_dag* dag, const double* lo, const double* hi,
+                             const double* incumbent, const double* rhs, double sb_coeff_thresh,
+                             double sb_min_width_ratio, int ibp_enhancement, void* workspace, int64_t ws_bytes,
+                             void* stream) {
+  using namespace gear;
+  g_launches = 0;
+  if (!q || !dag || !lo || !hi || !incumbent || (q->q.S > 1 && !rhs))
+    return fail(GEAR_E_INVALID, "gear_bab_step: %s", "bad arguments");
+  if (dag->hdr[H_N] != q->q.n || dag->hdr[H_S] != q->q.S || dag->hdr[H_RETA] == 0)
+    return fail(GEAR_E_INVALID, "gear_bab_step: %s", "program and queue differ in width or rows, or the program has no A");
+  const int64_t B = q->batch;
+  if (!workspace || ws_bytes < gear_bab_step_workspace_bytes(dag, B))
+    return fail(GEAR_E_WORKSPACE, "gear_bab_step: %s", "workspace too small");
+  // bound: CROWN over the popped batch (padding rows included), with the IBP pass when asked
+  int rc = crown_lower_impl(dag, lo, hi, B, nullptr, q->lb, q->lA, q->lbias, ibp_enhancement ? q->lb_ibp : nullptr,
+                            workspace, ws_bytes, stream);
+  if (rc != GEAR_OK) return rc;
+  const int crown = g_launches;
+  const int l = bab_step_after_bound(q, lo, hi, q->lb, q->lA, q->lbias, incumbent, rhs, sb_coeff_thresh,
+                                     sb_min_width_ratio, (cudaStream_t)stream);
+  if (l < 0) return l;
+  g_launches = crown + l;
+  return GEAR_OK;
+}
+
+extern "C" int gear_bab_step_bounded(gear_queue* q, const double* lo, const double* hi, const double* lb,
+                                     const double* lA, const double* lbias, const double* incumbent, const double* rhs,
+                                     double sb_coeff_thresh, double sb_min_width_ratio, void* stream) {
+  g_launches = 0;
+  if (!q || !lo || !hi || !lb || !lA || !lbias || !incumbent || (q->q.S > 1 && !rhs))
+    return fail(GEAR_E_INVALID, "gear_bab_step_bounded: %s", "bad arguments");
+  const int l = bab_step_after_bound(q, lo, hi, lb, lA, lbias, incumbent, rhs, sb_coeff_thresh, sb_min_width_ratio,
+                                     (cudaStream_t)stream);
+  if (l < 0) return l;
+  g_launches = l;
+  return GEAR_OK;
 }
 
 // ------------------------------------------------------------------ rigorous LP dual bound

@@ -394,6 +394,48 @@ class MultiEngine:
                 cur.wait_event(done)
         return outs
 
+    def prepare(self, boxes, out, lb_ibp=None):
+        """Plan every group's launch for these box buffers and outputs once (instance tables
+        uploaded into per-group workspaces); launch_prepared() then runs the call with fixed
+        arguments, capturable in a CUDA graph. The buffers must stay allocated and in place;
+        a box set of 0 rows leaves its instance out."""
+        self.release_prepared()
+        L = _lib.lib()
+        plans = []
+        for key, idx in self.groups.items():
+            args = self._args(idx, boxes, out, lb_ibp)
+            nbytes = int(L.gear_crown_multi_workspace_bytes(args, len(args)))
+            if nbytes < 0:
+                _lib.check(-1, "gear_crown_multi_workspace_bytes")
+            if nbytes == 0:
+                continue
+            dev = next(b[0].device for b in boxes)
+            ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+            h = ctypes.c_void_p()
+            _lib.check(L.gear_crown_multi_prepare(args, len(args), ws.data_ptr(), ws.numel(), ctypes.byref(h)),
+                       "gear_crown_multi_prepare")
+            plans.append((h, ws, args))
+        self._plans = plans
+
+    def launch_prepared(self):
+        """The prepared call (prepare()): one launch per kernel group on the current stream."""
+        L = _lib.lib()
+        for h, ws, _ in self._plans:
+            _lib.check(L.gear_crown_multi_launch(h, torch.cuda.current_stream(ws.device).cuda_stream),
+                       "gear_crown_multi_launch")
+
+    def release_prepared(self):
+        L = _lib.lib()
+        for h, _, _ in getattr(self, "_plans", []):
+            L.gear_crown_multi_plan_destroy(h)
+        self._plans = []
+
+    def __del__(self):
+        try:
+            self.release_prepared()
+        except Exception:
+            pass
+
     def group_ms(self):
         """Device time of each group's launch in the last lower() (after record_groups())."""
         torch.cuda.synchronize()

@@ -513,7 +513,8 @@ class Program:
                                 self.smem_total, self.max_S, self.sin_off, self.maxw,
                                 1 if self.return_a else 0, max_ops, self.simt_buf, self.simt_rows,
                                 1 if self.x_in_la else 0, MODES[self.mode], self.cta_threads, self.pass_global,
-                                TIE_RULES[self.tie_rule], 1 if (self.fold_tc and self.fold_w > 0) else 0],
+                                TIE_RULES[self.tie_rule],
+                                1 if (self.fold_tc and self.fold_w > 0 and self.pass_global == 0) else 0],
                                dtype=np.int32)
 
     def _emit_pass(self, pid, pi: PassInfo):

@@ -130,6 +130,51 @@ int gear_gather_rows(const double* src, const int32_t* rows, int64_t count, int6
 int gear_scatter_rows(const double* src, const int32_t* rows, int64_t count, int64_t width, double* dst,
                       void* stream);
 
+/* ---------------------------------------------------------------- device-resident queue, one BaB step
+ * A gear_queue holds the open domains of one branch-and-bound run on the device: slot arrays (box,
+ * keys, insertion ids), the active slot list kept in the reference's pop order (objective key
+ * descending, insertion id ascending; branching_domains.py:831-962, 1171, with a stable sort), a
+ * free list and the counters, all in device memory. gear_queue_pop and gear_bab_step read every
+ * size from those counters: an iteration is a fixed sequence of launches with fixed arguments,
+ * needs no host read, and can be captured once into a CUDA graph and replayed. They replace the
+ * reference's domain list and its per-iteration loop body (UnsortedInputDomainList,
+ * batch_branch_and_bound.py:275-652).
+ *
+ * gear_queue_create: n variables, S rows, `capacity` slots (> 2 x batch), iterations of `batch`
+ * domains; the root box (n doubles each, host or device memory) is the first open domain.
+ * gear_queue_pop: the next batch into lo_out / hi_out (batch, n): the tail of the active list, rows
+ * beyond the open count repeat the first popped box (the root box when nothing is open).
+ * gear_bab_step: bounds that batch with dag (gear_crown_lower, with the IBP pass when
+ * ibp_enhancement), prunes against thresholds [*incumbent, rhs[0..S-2]] read on the device
+ * (get_remaining_index, branching_domains.py:412-558), picks split variables (SB with sb_sum,
+ * branching_heuristics.py:25-202), bisects the kept boxes (split.py:26-122), keys the children
+ * (batch_branch_and_bound.py:189-225) and merges them into the active list. Workspace:
+ * gear_bab_step_workspace_bytes. Children that would not fit the free slots are not pushed and
+ * counted in counter 7: keep capacity >= open + 2 x batch per iteration run.
+ * gear_queue_counters: copies the 8 counters (open, free, next id, domains bounded, last batch,
+ * kept, iterations, overflows) to `counters` (host or device, asynchronous) and, when dual is
+ * non-NULL, the dual bound min(open keys, smallest discarded threshold) to *dual (device).
+ * gear_queue_size: the open count, synchronously. gear_queue_push: `count` <= 2 x batch domains
+ * (device arrays lo, hi (count, n), key (count, S)) into the queue. */
+typedef struct gear_queue gear_queue;
+int gear_queue_create(int n, int S, int64_t capacity, int64_t batch, const double* root_lo, const double* root_hi,
+                      gear_queue** out);
+int gear_queue_destroy(gear_queue* q);
+int gear_queue_push(gear_queue* q, const double* lo, const double* hi, const double* key, int64_t count, void* stream);
+int gear_queue_pop(gear_queue* q, double* lo_out, double* hi_out, void* stream);
+int gear_queue_size(const gear_queue* q, int64_t* open, void* stream);
+int gear_queue_counters(const gear_queue* q, int64_t* counters, double* dual, void* stream);
+int64_t gear_bab_step_workspace_bytes(const gear_dag* dag, int64_t batch);
+int gear_bab_step(gear_queue* q, const gear_dag* dag, const double* lo, const double* hi, const double* incumbent,
+                  const double* rhs, double sb_coeff_thresh, double sb_min_width_ratio, int ibp_enhancement,
+                  void* workspace, int64_t ws_bytes, void* stream);
+/* gear_bab_step after its CROWN call: the batch's bounds lb (batch, S), lA (batch, S, n), lbias
+ * (batch, S) come from the caller (a many-instance launch, gear_crown_lower_multi, bounds the
+ * batches of many queues at once). Same prune, branch, split, keys and push. */
+int gear_bab_step_bounded(gear_queue* q, const double* lo, const double* hi, const double* lb, const double* lA,
+                          const double* lbias, const double* incumbent, const double* rhs, double sb_coeff_thresh,
+                          double sb_min_width_ratio, void* stream);
+
 /* Domain clipping, in place: shrink every box [x_L, x_U] (batch, n) along each coordinate to the
  * part where each plane lA_s x + lbias_s (s < S) can still be <= thr_s, rounding every candidate
  * outward; a box some plane already proves done becomes empty (x_L[0] = next double above x_U[0]).
@@ -284,6 +329,18 @@ int64_t gear_crown_multi_workspace_bytes(const gear_lower_args* items, int32_t c
  * Asynchronous on `stream`. */
 int gear_crown_lower_multi(const gear_lower_args* items, int32_t count, void* workspace, int64_t workspace_bytes,
                            void* stream);
+
+/* The same launch prepared once: gear_crown_multi_prepare plans it and uploads its instance table
+ * into `workspace` (gear_crown_multi_workspace_bytes; the workspace and every instance's buffers
+ * must stay in place), after which each gear_crown_multi_launch is a work-counter reset and one
+ * kernel with fixed arguments -- a launch a CUDA graph can capture and replay (the instances'
+ * inputs change in place between replays). Synchronous prepare; the plan is host memory, freed by
+ * gear_crown_multi_plan_destroy. No counterpart in the reference (its batching is per instance). */
+typedef struct gear_multi_plan gear_multi_plan;
+int gear_crown_multi_prepare(const gear_lower_args* items, int32_t count, void* workspace, int64_t workspace_bytes,
+                             gear_multi_plan** out);
+int gear_crown_multi_launch(const gear_multi_plan* plan, void* stream);
+int gear_crown_multi_plan_destroy(gear_multi_plan* plan);
 
 /* Number of kernel launches the last gear_crown_lower on this thread issued. */
 int gear_last_launch_count(void);
