@@ -169,13 +169,14 @@ def max_over_ranks(value, world, device):
 
 
 # ---------------------------------------------------------------- branch and bound to the gap
-def bab_to_gap(instances, dev, rel_gap=1e-4, batch=2048):
+def bab_to_gap(instances, dev, rel_gap=1e-4, batch=2048, graph_capture=True):
     """Branch and bound (select, CROWN, prune, SB branch, split on the device) to a relative gap
-    on quad_exp_n10 instances 0..instances-1: wall time to the gap per instance (host loop
-    included), p50 / p99, and subdomains bounded per second over all runs."""
+    on quad_exp_n10 instances 0..instances-1: wall time to the gap per instance (host included),
+    p50 / p99, and subdomains bounded per second over all runs. graph_capture=True: the queue on the
+    device and 8 iterations per CUDA-graph replay (GraphBaB); False: the host-driven loop (BaB)."""
     import torch
     from gear_b200 import graph, problems
-    from gear_b200.bab import BaB
+    from gear_b200.bab import BaB, GraphBaB
     times, bounded, iters, gaps = [], 0, [], []
     for inst in range(-1, instances):
         m = problems.make_instance("quad_exp_n10", max(inst, 0))
@@ -184,22 +185,28 @@ def bab_to_gap(instances, dev, rel_gap=1e-4, batch=2048):
         m = m.to(dev)
         torch.cuda.synchronize(dev)
         t = time.perf_counter()
-        bb = BaB(g, lo, hi, batch=batch, model=m, device=str(dev))
+        if graph_capture:
+            bb = GraphBaB(g, lo, hi, batch=batch, model=m, device=str(dev))
+        else:
+            bb = BaB(g, lo, hi, batch=batch, model=m, device=str(dev))
         P, D, gap = bb.run(rel_gap=rel_gap, max_iterations=5000, time_limit=60)
         torch.cuda.synchronize(dev)
         dt = time.perf_counter() - t
         if inst < 0:
             continue                                        # warm-up run (module load)
         times.append(dt)
-        bounded += bb.stats.bounded
-        iters.append(bb.stats.iterations)
+        bounded += bb.status["bounded"] if graph_capture else bb.stats.bounded
+        iters.append(bb.status["iterations"] if graph_capture else bb.stats.iterations)
         gaps.append(gap)
     q = sorted(times)
     p99 = q[min(len(q) - 1, int(round(0.99 * (len(q) - 1))))]
     return {"workload": "quad_exp_n10 (config-1 family)", "instances": instances, "rel_gap": rel_gap,
             "batch": batch, "time_to_gap_s": {"p50": statistics.median(times), "p99": p99, "max": max(times)},
             "closed": sum(1 for gp in gaps if gp <= rel_gap), "iterations_median": statistics.median(iters),
-            "subdomains_per_s": bounded / sum(times), "timing": "wall clock, host loop included"}
+            "subdomains_per_s": bounded / sum(times),
+            "form": "device queue, 8 iterations per CUDA-graph replay (GraphBaB)" if graph_capture else
+                    "host-driven loop (BaB)",
+            "timing": "wall clock per instance from construction (engine pick, capture) to the gap"}
 
 
 def mixed_setup(instances=512, workers=None):
@@ -337,16 +344,17 @@ def lb_difference(a_outs, b_outs):
                     "summation order of the kernel variant; both arms' bounds are sound"}
 
 
-def mixed_bab(dev, setup, batch=256, rel_gap=1e-4, time_limit=60.0, plain=False):
+def mixed_bab(dev, setup, batch=256, rel_gap=1e-4, time_limit=60.0, plain=False, graph_capture=True):
     """Branch and bound on the uneven batch to relative gap 1e-4, every instance at once
     (MultiBaB): certified subdomains per second (subdomains bounded, each with a sound lower bound,
     per second of wall time, host loop included), wall time to the gap per instance over the
     instances that reach it within the time limit. plain=False bounds every iteration's batches in
     one packed CROWN launch per kernel variant (MultiEngine); plain=True is the plain GPU form:
     each instance's batch bounded alone, one launch per schedule step and per op
-    (PlainMultiEngine), the same loop otherwise."""
+    (PlainMultiEngine), the same loop otherwise. graph_capture (packed only): every instance's
+    queue on the device and whole rounds replayed from a CUDA graph (MultiGraphBaB)."""
     import torch
-    from gear_b200.bab import MultiBaB
+    from gear_b200.bab import MultiBaB, MultiGraphBaB
     insts, graphs, me = setup[:3]
     if plain:
         from gear_b200.engine import PlainMultiEngine
@@ -355,18 +363,32 @@ def mixed_bab(dev, setup, batch=256, rel_gap=1e-4, time_limit=60.0, plain=False)
     roots = [(torch.full((1, m.n), -2.0, dtype=torch.float64), torch.full((1, m.n), 2.0, dtype=torch.float64))
              for m in insts]
     models = [m.to(dev) for m in insts]
-    mb = MultiBaB(graphs, roots, models, batch=batch, engine=me, device=str(dev))
+    graphed = graph_capture and not plain
+    if graphed:
+        mb = MultiGraphBaB(graphs, roots, models, batch=batch, engine=me, device=str(dev))
+    else:
+        mb = MultiBaB(graphs, roots, models, batch=batch, engine=me, device=str(dev))
     torch.cuda.synchronize(dev)
     t = time.perf_counter()
     res = mb.run(rel_gap=rel_gap, time_limit=time_limit)
     torch.cuda.synchronize(dev)
     wall = time.perf_counter() - t
+    if graphed:
+        # domains bounded per instance up to its retirement (the captured round may run on)
+        mb.bounded = sum(r["bounded"] for r in res)
+        mb.iterations = mb.rounds
+        statuses = {}
+        for r in res:
+            statuses[r["status"]] = statuses.get(r["status"], 0) + 1
     ttg = sorted(r["time_to_gap"] for r in res if r["time_to_gap"] is not None)
     q = (lambda p: ttg[min(len(ttg) - 1, int(round(p * (len(ttg) - 1))))]) if ttg else (lambda p: None)
     closed_n = [insts[i].n for i, r in enumerate(res) if r["time_to_gap"] is not None]
     return {"workload": "mixed family (n log-uniform [5, 500], depth 3-12, m = n // 4)", "instances": instances,
-            "form": "plain GPU form (one instance, one launch per step and per op)" if plain else
-                    "packed (one launch per kernel variant per iteration)",
+            "form": "plain GPU form (one instance, one launch per step and per op, host-driven loop)" if plain else
+                    ("packed launch per kernel variant, device queues, rounds replayed from a CUDA graph "
+                     "(MultiGraphBaB)" if graphed else "packed launch per kernel variant, host-driven loop (MultiBaB)"),
+            "statuses": statuses if graphed else None,
+            "graph_captures": getattr(mb, "captures", None), "graph_replays": getattr(mb, "replays", None),
             "batch_per_instance": batch, "rel_gap": rel_gap, "time_limit_s": time_limit, "wall_s": wall,
             "iterations": mb.iterations, "closed": len(ttg), "closed_max_n": max(closed_n) if closed_n else None,
             "time_to_gap_s": {"p50": q(0.5), "p99": q(0.99), "max": ttg[-1] if ttg else None},

@@ -629,6 +629,8 @@ class GraphBaB:
                               device=dev)
         self.counters = torch.zeros(self.N_COUNTERS, dtype=torch.int64, device=dev)
         self.dual = torch.full((1,), -math.inf, dtype=torch.float64, device=dev)
+        _lib.check(L.gear_queue_counters(self.q, self.counters.data_ptr(), self.dual.data_ptr(),
+                                         torch.cuda.current_stream(dev).cuda_stream), "gear_queue_counters")
         self.graph_obj = None
         self.incumbent = math.inf
         self.replays = 0
