@@ -397,15 +397,18 @@ def mixed_bab(dev, setup, batch=256, rel_gap=1e-4, time_limit=60.0, plain=False,
 
 
 def serve(dev, seconds=10.0, rate=50.0, budget=30.0, batch=2048, rel_gap=1e-4, seed=0, round_bytes=16 << 20,
-          max_live=128, admission="small_first", incumbent_every=4, round_cap=16):
+          max_live=128, admission="small_first", incumbent_every=4, round_cap=16, device_queues=False,
+          compile_workers=8):
     """The serving loop under Poisson arrivals (rate per second for `seconds`): instances of the
     quad-exp family with n log-uniform in [5, 2000] (two bilinear constraints), each to the
-    relative gap or its time budget (from arrival). Continuous batching (Server): requests are
-    admitted as memory allows and join the running rounds. Time to gap = finish - arrival."""
+    relative gap or its time budget (from arrival). Continuous batching: requests are admitted as
+    memory allows and join the running rounds (Server: host-driven rounds; device_queues:
+    DeviceServer, every request's queue on the device and its round in CUDA graphs). Time to gap
+    = finish - arrival."""
     import math as _m
     import torch
     from gear_b200 import problems
-    from gear_b200.serve import Server
+    from gear_b200.serve import DeviceServer, Server
     g = torch.Generator().manual_seed(5000 + seed)
     t, arrivals = 0.0, []
     while True:
@@ -415,7 +418,7 @@ def serve(dev, seconds=10.0, rate=50.0, budget=30.0, batch=2048, rel_gap=1e-4, s
         arrivals.append(t)
     ns = [int(round(_m.exp(_m.log(5) + (_m.log(2000) - _m.log(5)) * float(torch.rand(1, generator=g)))))
           for _ in arrivals]
-    srv = Server(device=str(dev), batch=batch, rel_gap=rel_gap, time_budget=budget, round_bytes=round_bytes,
+    srv = (DeviceServer if device_queues else Server)(device=str(dev), compile_workers=compile_workers, batch=batch, rel_gap=rel_gap, time_budget=budget, round_bytes=round_bytes,
                  max_live=max_live, admission=admission, incumbent_every=incumbent_every, round_cap=round_cap)
     t0 = time.perf_counter()
     clock = lambda: time.perf_counter() - t0
@@ -433,6 +436,7 @@ def serve(dev, seconds=10.0, rate=50.0, budget=30.0, batch=2048, rel_gap=1e-4, s
             continue
         srv.step()
     torch.cuda.synchronize(dev)
+    srv.close()
     wall = clock()
     done = list(srv.done.values())
     ttg = sorted(r.finished - r.arrival for r in done if r.status == "closed")
@@ -448,8 +452,11 @@ def serve(dev, seconds=10.0, rate=50.0, budget=30.0, batch=2048, rel_gap=1e-4, s
             "rel_gap": rel_gap, "budget_s": budget, "batch_per_instance_max": batch, "round_bytes": round_bytes,
             "max_live": max_live, "waited_out": sum(1 for r in done if r.admitted is None),
             "admission": admission, "incumbent_every": incumbent_every, "round_cap": round_cap,
+            "compile_workers": compile_workers,
             "closed_n_max": max((r.lo.shape[1] for r in done if r.status == "closed"), default=None),
             "host_s": {"rounds": srv.t_round, "crown_launch_calls": srv.t_bound}, "wall_s": wall,
+            "form": "device queues, per-request CUDA graphs (DeviceServer)" if device_queues else
+                    "host-driven rounds (Server)",
             "timing": "wall clock; time to gap from each request's arrival to the round that closed it"}
 
 
@@ -579,9 +586,10 @@ def main():
                     help="skip the plain GPU form (one launch per step and per op) on the workload")
     ap.add_argument("--workload", default=WORKLOAD, help="benchmark workload (profiling of other shapes)")
     ap.add_argument("--cta-threads", type=int, default=128, help="threads per CTA of --mode cta")
-    ap.add_argument("--mode", default="auto", choices=["auto", "cta", "simt"],
-                    help="CROWN kernel: one box per CTA, one box per thread, or the faster one timed on the "
-                         "first (warm-up) call")
+    ap.add_argument("--mode", default="tune", choices=["tune", "auto", "cta", "simt"],
+                    help="CROWN kernel: the autotuner's pick (execution shape, working-set placement, GEMV "
+                         "tile, tensor-core fold, searched on the first call), the faster of four variants, one "
+                         "box per CTA, or one box per thread")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -620,6 +628,10 @@ def main():
         step()
     torch.cuda.synchronize()
     variant = eng.variant(B)
+    if hasattr(eng, "kernel_name"):
+        kname = eng.kernel_name(B)
+    else:
+        kname = "crown_simt_kernel" if variant == "simt" else f"crown_megakernel<{variant[3:]}, 0, 0>"
 
     def barrier():
         if world > 1:
@@ -688,8 +700,7 @@ def main():
             try:
                 with open(tfile) as f:
                     tj = json.load(f)
-                kname = "crown_simt_kernel" if variant == "simt" else f"crown_megakernel<{variant[3:]}>"
-                traffic = tj.get(args.workload, {}).get(kname, {}).get("bytes_per_box")
+                traffic = tj.get(args.workload, {}).get(kname.split(",")[0] + (">" if "," in kname else ""), {}).get("bytes_per_box")
                 traffic = traffic * B if traffic is not None else None
             except Exception:
                 traffic = None
@@ -703,7 +714,7 @@ def main():
                "gpu_launches": launches,
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                             "frac": achieved / peak, "traffic": traffic,
-                            "kernel": "crown_simt_kernel" if variant == "simt" else f"crown_megakernel<{variant[3:]}>",
+                            "kernel": kname,
                             "peak_source": peak_kind,
                             "alg_bytes_per_box": prog.alg_bytes_per_box(), "work_per_box": prog.work,
                             "fp64_gemm_gflops": prog.work["gemm_flops"] * B / (ms_launch / 1000.0) / 1e9},

@@ -65,6 +65,10 @@ def lib():
         L.gear_queue_size.restype = i32
         L.gear_queue_counters.argtypes = [vp, vp, vp, vp]
         L.gear_queue_counters.restype = i32
+        L.gear_queue_reserve.argtypes = [vp, i64, vp]
+        L.gear_queue_reserve.restype = i32
+        L.gear_queue_capacity.argtypes = [vp]
+        L.gear_queue_capacity.restype = i64
         L.gear_bab_step_workspace_bytes.argtypes = [vp, i64]
         L.gear_bab_step_workspace_bytes.restype = i64
         L.gear_bab_step.argtypes = [vp, vp, vp, vp, vp, vp, dbl, dbl, i32, vp, i64, vp]
@@ -152,4 +156,4 @@ EXPORTED = ("gear_dag_create", "gear_dag_destroy", "gear_crown_workspace_bytes",
             "gear_crown_lower_plain_ibp", "gear_queue_create", "gear_queue_destroy", "gear_queue_push",
             "gear_queue_pop", "gear_queue_size", "gear_queue_counters", "gear_bab_step_workspace_bytes",
             "gear_bab_step", "gear_bab_step_bounded", "gear_crown_multi_prepare", "gear_crown_multi_launch",
-            "gear_crown_multi_plan_destroy")
+            "gear_crown_multi_plan_destroy", "gear_queue_reserve", "gear_queue_capacity")

@@ -591,8 +591,9 @@ class GraphBaB:
                  capacity: Optional[int] = None, sb_coeff_thresh: float = 1e-3, sb_min_width_ratio: float = 1e-3,
                  ibp_enhancement: bool = True, chunk: int = 8, use_graph: bool = True,
                  engine: Optional[CrownEngine] = None, engine_mode: str = "auto", cta_threads: int = 128):
-        """capacity: queue slots (default 256 x batch); each iteration grows the open list by at
-        most `batch`, and a replay of `chunk` iterations starts only with that much room."""
+        """capacity: the queue's first capacity in slots (default 64 x batch); each iteration grows
+        the open list by at most `batch`, a replay of `chunk` iterations starts only with that much
+        room, and the queue doubles (gear_queue_reserve) when it has less."""
         self.device = torch.device(device)
         self.graph = graph
         self.batch = int(batch)
@@ -613,7 +614,7 @@ class GraphBaB:
         dev = self.device
         root_lo = lo.reshape(-1).to(torch.float64).cpu().contiguous()
         root_hi = hi.reshape(-1).to(torch.float64).cpu().contiguous()
-        self.capacity = int(capacity or 256 * self.batch)
+        self.capacity = int(capacity or 64 * self.batch)
         L = _lib.lib()
         h = ctypes.c_void_p()
         _lib.check(L.gear_queue_create(self.n, self.S, self.capacity, self.batch, root_lo.data_ptr(),
@@ -634,6 +635,7 @@ class GraphBaB:
         self.graph_obj = None
         self.incumbent = math.inf
         self.replays = 0
+        self.regrown = 0
         self.status = {}
 
     def __del__(self):
@@ -697,8 +699,14 @@ class GraphBaB:
             if st["open"] == 0 or st["iterations"] >= max_iterations or time.perf_counter() - t0 > time_limit:
                 break
             if st["open"] + self.chunk * self.batch > self.capacity:
-                raise RuntimeError(f"gear_queue capacity {self.capacity} too small for {st['open']} open domains "
-                                   f"plus a replay of {self.chunk} iterations of {self.batch}")
+                # grow the queue (its device pointers change: capture the iterations again)
+                L = _lib.lib()
+                new = max(2 * self.capacity, st["open"] + 2 * self.chunk * self.batch)
+                _lib.check(L.gear_queue_reserve(self.q, new, torch.cuda.current_stream(self.device).cuda_stream),
+                           "gear_queue_reserve")
+                self.capacity = int(L.gear_queue_capacity(self.q))
+                self.graph_obj = None
+                self.regrown += 1
             if self.use_graph:
                 if self.graph_obj is None:
                     self._chunk()                       # eager first chunk: loads, workspaces, warm caches
@@ -730,64 +738,70 @@ class GraphBaB:
 
 class MultiGraphBaB:
     """Branch and bound on many instances at once (the uneven batch), every instance's queue on
-    the device (gear_queue), and a whole round captured into one CUDA graph: for every instance
-    gear_queue_pop and its incumbent proposal (its model at the popped boxes' midpoints), one
-    prepared many-instance CROWN launch per kernel group for all the batches
-    (MultiEngine.prepare / launch_prepared), then gear_bab_step_bounded for every instance. The
-    host reads all counters, dual bounds and incumbents once per replay (`chunk` rounds); an
-    instance retires when it reaches the gap, empties its queue or fills its queue capacity, and
-    the round is captured again (for the instances still running) once the running set has shrunk
-    below `recapture` of the captured one. Each instance's search is the one GraphBaB runs for it
-    alone (same kernels, same order)."""
+    the device (gear_queue) and its round captured once into CUDA graphs: one for its pop and
+    incumbent proposal (its model at the popped boxes' midpoints), one for its
+    gear_bab_step_bounded and a copy of its counters, dual bound and incumbent into a status row.
+    A round replays every running instance's first graph, makes one prepared many-instance CROWN
+    launch per kernel group for all the batches (MultiEngine.prepare / launch_prepared, re-planned
+    only when the running set changes), replays the second graphs and reads all status rows in one
+    copy. An instance retires when it reaches the gap or empties its queue; a queue about to fill
+    grows (gear_queue_reserve, up to max_queue_bytes) and that instance's graphs are captured
+    again. Each instance's search is the one GraphBaB runs for it alone (same kernels, same order;
+    tested)."""
 
     def __init__(self, graphs, roots, models=None, rhs=None, batch: int = 256, engine=None, programs=None,
                  device="cuda", ibp_enhancement: bool = True, sb_coeff_thresh: float = 1e-3,
-                 sb_min_width_ratio: float = 1e-3, chunk: int = 2, queue_bytes: int = 64 << 20,
-                 recapture: float = 0.8):
-        """queue_bytes: device memory of one instance's queue (its capacity in slots follows from
-        its width); roots: [(lo (1, n_i), hi (1, n_i))]."""
+                 sb_min_width_ratio: float = 1e-3, queue_slots: Optional[int] = None,
+                 max_queue_bytes: int = 1 << 30):
+        """roots: [(lo (1, n_i), hi (1, n_i))]; queue_slots: the first capacity of every queue
+        (default 16 x batch); a queue doubles when fewer than 2 x batch slots stay free, while its
+        memory stays within max_queue_bytes."""
         from .engine import MultiEngine
         self.device = dev = torch.device(device)
         self.engine = engine if engine is not None else MultiEngine(graphs, programs=programs)
         N = len(graphs)
-        self.N, self.batch, self.chunk = N, int(batch), max(1, int(chunk))
-        self.recapture = recapture
+        self.N, self.batch = N, int(batch)
         self.coeff_thresh, self.min_width_ratio = sb_coeff_thresh, sb_min_width_ratio
         self.models = list(models) if models is not None else [None] * N
         self.n, self.S = list(self.engine.n), list(self.engine.S)
+        self.max_queue_bytes = max_queue_bytes
         L = _lib.lib()
-        self.inc = torch.full((N,), math.inf, dtype=torch.float64, device=dev)
-        self.counters = torch.zeros(N, GraphBaB.N_COUNTERS, dtype=torch.int64, device=dev)
-        self.dual = torch.full((N,), -math.inf, dtype=torch.float64, device=dev)
-        self.boxes, self.x_best, self.rhs, self.queues, self.caps = [], [], [], [], []
+        st = torch.cuda.current_stream(dev).cuda_stream
+        self.status = torch.zeros(N, GraphBaB.N_COUNTERS + 2, dtype=torch.float64, device=dev)
+        self.inc, self.counters, self.dual = [], [], []
+        self.boxes, self.x_best, self.rhs, self.queues = [], [], [], []
+        first = int(queue_slots or 16 * self.batch)
         for i in range(N):
             n, S = self.n[i], self.S[i]
             lo = roots[i][0].reshape(-1).to(torch.float64).cpu().contiguous()
             hi = roots[i][1].reshape(-1).to(torch.float64).cpu().contiguous()
-            slot_bytes = 8 * (2 * n + S + 2) + 12
-            cap = max((self.chunk + 3) * self.batch, min(256 * self.batch, queue_bytes // slot_bytes))
             h = ctypes.c_void_p()
-            _lib.check(L.gear_queue_create(n, S, cap, self.batch, lo.data_ptr(), hi.data_ptr(), ctypes.byref(h)),
-                       "gear_queue_create")
+            _lib.check(L.gear_queue_create(n, S, max(first, 2 * self.batch + 1), self.batch, lo.data_ptr(),
+                                           hi.data_ptr(), ctypes.byref(h)), "gear_queue_create")
             self.queues.append(h)
-            self.caps.append(cap)
             self.boxes.append((torch.empty(self.batch, n, dtype=torch.float64, device=dev),
                                torch.empty(self.batch, n, dtype=torch.float64, device=dev)))
             self.x_best.append(((lo + hi) / 2).to(dev))
             r = rhs[i] if rhs is not None and rhs[i] is not None else torch.zeros(S - 1, dtype=torch.float64)
             self.rhs.append(torch.cat([r.to(torch.float64).reshape(-1).to(dev),
                                        torch.zeros(1, dtype=torch.float64, device=dev)]))
+            self.inc.append(torch.full((1,), math.inf, dtype=torch.float64, device=dev))
+            self.counters.append(torch.zeros(GraphBaB.N_COUNTERS, dtype=torch.int64, device=dev))
+            self.dual.append(torch.full((1,), -math.inf, dtype=torch.float64, device=dev))
+            _lib.check(L.gear_queue_counters(h, self.counters[i].data_ptr(), self.dual[i].data_ptr(), st),
+                       "gear_queue_counters")
         self.outs = self.engine.outputs([self.batch] * N, dev)
         self.ibp = ([torch.empty(self.batch, self.S[i], dtype=torch.float64, device=dev) for i in range(N)]
                     if ibp_enhancement else None)
-        self.graph_obj = None
-        self.captured = ()
-        self.replays = 0
-        self.captures = 0
+        self.graphs = [None] * N
+        for i in range(N):
+            self._capture(i)
+        self._planned = None
+        self.rounds = self.captures_regrown = self.prepares = 0
 
     def __del__(self):
         try:
-            self.graph_obj = None
+            self.graphs = []
             self.engine.release_prepared()
             L = _lib.lib()
             for h in getattr(self, "queues", []):
@@ -797,105 +811,108 @@ class MultiGraphBaB:
         except Exception:
             pass
 
-    def _propose(self, i):
+    def _pre(self, i):
+        L = _lib.lib()
+        dev = self.device
+        plo, phi = self.boxes[i]
+        _lib.check(L.gear_queue_pop(self.queues[i], plo.data_ptr(), phi.data_ptr(),
+                                    torch.cuda.current_stream(dev).cuda_stream), "gear_queue_pop")
         m = self.models[i]
         if m is None:
             return
-        plo, phi = self.boxes[i]
         S = self.S[i]
         with torch.no_grad():
             x = (plo + phi) / 2
             y = m(x)
             feas = (y[:, 1:] <= self.rhs[i][:S - 1]).all(1) if y.shape[1] > 1 else \
-                torch.ones(y.shape[0], dtype=torch.bool, device=self.device)
+                torch.ones(y.shape[0], dtype=torch.bool, device=dev)
             obj = torch.where(feas, y[:, 0], torch.full_like(y[:, 0], math.inf))
             best = obj.min(0)
             val = best.values.reshape(1)
             pt = x.index_select(0, best.indices.reshape(1)).reshape(-1)
-            inc = self.inc[i:i + 1]
+            inc = self.inc[i]
             self.x_best[i].copy_(torch.where(val < inc, pt, self.x_best[i]))
             inc.copy_(torch.minimum(inc, val))
 
-    def _round(self, run):
+    def _post(self, i):
         L = _lib.lib()
         st = torch.cuda.current_stream(self.device).cuda_stream
-        for i in run:
-            plo, phi = self.boxes[i]
-            _lib.check(L.gear_queue_pop(self.queues[i], plo.data_ptr(), phi.data_ptr(), st), "gear_queue_pop")
-            self._propose(i)
-        self.engine.launch_prepared()
-        for i in run:
-            plo, phi = self.boxes[i]
-            lb, lA, lbias = self.outs[i]
-            _lib.check(L.gear_bab_step_bounded(self.queues[i], plo.data_ptr(), phi.data_ptr(), lb.data_ptr(),
-                                               lA.data_ptr(), lbias.data_ptr(), self.inc[i:i + 1].data_ptr(),
-                                               self.rhs[i].data_ptr(), self.coeff_thresh, self.min_width_ratio, st),
-                       "gear_bab_step_bounded")
+        plo, phi = self.boxes[i]
+        lb, lA, lbias = self.outs[i]
+        _lib.check(L.gear_bab_step_bounded(self.queues[i], plo.data_ptr(), phi.data_ptr(), lb.data_ptr(), lA.data_ptr(),
+                                           lbias.data_ptr(), self.inc[i].data_ptr(), self.rhs[i].data_ptr(),
+                                           self.coeff_thresh, self.min_width_ratio, st), "gear_bab_step_bounded")
+        _lib.check(L.gear_queue_counters(self.queues[i], self.counters[i].data_ptr(), self.dual[i].data_ptr(), st),
+                   "gear_queue_counters")
+        self.status[i].copy_(torch.cat([self.counters[i].to(torch.float64), self.dual[i], self.inc[i]]))
 
-    def _chunk(self, run):
-        for _ in range(self.chunk):
-            self._round(run)
-        L = _lib.lib()
-        st = torch.cuda.current_stream(self.device).cuda_stream
-        for i in run:
-            _lib.check(L.gear_queue_counters(self.queues[i], self.counters[i].data_ptr(), self.dual[i:i + 1].data_ptr(),
-                                             st), "gear_queue_counters")
+    def _capture(self, i):
+        self.graphs[i] = None
+        gs = {}
+        for name, fn in (("pre", self._pre), ("post", self._post)):
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                fn(i)
+            gs[name] = g
+        self.graphs[i] = gs
 
-    def _capture(self, run):
-        """Prepare the packed launch for `run`, one eager chunk, then capture a chunk."""
+    def _prepare(self, run):
         e = torch.empty(0, dtype=torch.float64, device=self.device)
-        boxes = [self.boxes[i] if i in run else (e.view(0, self.n[i]), e.view(0, self.n[i])) for i in range(self.N)]
-        ibp = [self.ibp[i] if i in run else None for i in range(self.N)] if self.ibp is not None else None
-        self.graph_obj = None
+        rs = set(run)
+        boxes = [self.boxes[i] if i in rs else (e.view(0, self.n[i]), e.view(0, self.n[i])) for i in range(self.N)]
+        ibp = [self.ibp[i] if i in rs else None for i in range(self.N)] if self.ibp is not None else None
         self.engine.prepare(boxes, self.outs, ibp)
-        self._chunk(run)
-        torch.cuda.synchronize(self.device)
-        g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g):
-            self._chunk(run)
-        self.graph_obj = g
-        self.captured = tuple(run)
-        self.captures += 1
-
-    def _read(self):
-        v = torch.cat([self.counters.reshape(-1).to(torch.float64), self.dual, self.inc]).cpu()
-        N = self.N
-        c = v[:N * GraphBaB.N_COUNTERS].reshape(N, GraphBaB.N_COUNTERS).to(torch.int64).tolist()
-        return c, v[N * GraphBaB.N_COUNTERS:N * (GraphBaB.N_COUNTERS + 1)].tolist(), v[-N:].tolist()
+        self._planned = tuple(run)
+        self.prepares += 1
 
     def run(self, rel_gap: float = 1e-4, time_limit: float = 60.0, max_rounds: int = 100000):
-        """Until every instance reaches the gap, empties its queue or fills its capacity, or a limit.
-        Returns per instance: incumbent, dual bound, gap, wall time to the gap (None if not
-        reached), status, domains bounded (counted up to the instance's retirement)."""
+        """Until every instance reaches the gap or empties its queue, or a limit. Returns per
+        instance: incumbent, dual bound, gap, wall time to the gap (None if not reached), status,
+        domains bounded (counted up to its retirement), rounds."""
         t0 = time.perf_counter()
         N = self.N
-        res = [dict(P=math.inf, D=-math.inf, gap=math.inf, time_to_gap=None, status="running", bounded=0)
+        res = [dict(P=math.inf, D=-math.inf, gap=math.inf, time_to_gap=None, status="running", bounded=0, rounds=0)
                for _ in range(N)]
         running = list(range(N))
-        rounds = 0
-        while running and rounds < max_rounds and time.perf_counter() - t0 < time_limit:
-            if self.graph_obj is None or len(running) < self.recapture * len(self.captured):
-                self._capture(running)
-                rounds += self.chunk
-            else:
-                self.graph_obj.replay()
-                self.replays += 1
-                rounds += self.chunk
-            c, D, P = self._read()
+        L = _lib.lib()
+        C = GraphBaB
+        while running and self.rounds < max_rounds and time.perf_counter() - t0 < time_limit:
+            if self._planned != tuple(running):
+                self._prepare(running)
+            for i in running:
+                self.graphs[i]["pre"].replay()
+            self.engine.launch_prepared()
+            for i in running:
+                self.graphs[i]["post"].replay()
+            idx = torch.tensor(running, dtype=torch.int64, device=self.device)
+            rows = self.status.index_select(0, idx).cpu().tolist()
+            self.rounds += 1
             now = time.perf_counter() - t0
             nxt = []
-            for i in running:
-                g = BaB._gap(P[i], D[i])
+            for i, row in zip(running, rows):
+                D, P = row[C.N_COUNTERS], row[C.N_COUNTERS + 1]
+                g = BaB._gap(P, D)
                 r = res[i]
-                r.update(P=P[i], D=D[i], gap=g, bounded=c[i][GraphBaB.C_BOUNDED])
+                r.update(P=P, D=D, gap=g, bounded=int(row[C.C_BOUNDED]), rounds=r["rounds"] + 1)
+                open_ = int(row[C.C_ACTIVE])
                 if g <= rel_gap:
                     r.update(time_to_gap=now, status="closed")
-                elif c[i][GraphBaB.C_ACTIVE] == 0:
+                    continue
+                if open_ == 0:
                     r.update(status="emptied")
-                elif c[i][GraphBaB.C_ACTIVE] + self.chunk * self.batch > self.caps[i] or c[i][GraphBaB.C_OVERFLOW]:
-                    r.update(status="capacity")
-                else:
-                    nxt.append(i)
+                    continue
+                cap = int(L.gear_queue_capacity(self.queues[i]))
+                if open_ + 2 * self.batch > cap or int(row[C.C_OVERFLOW]):
+                    slot = 8 * (2 * self.n[i] + self.S[i] + 2) + 12
+                    new = min(2 * cap, self.max_queue_bytes // slot)
+                    if int(row[C.C_OVERFLOW]) or new < open_ + 2 * self.batch:
+                        r.update(status="capacity")
+                        continue
+                    _lib.check(L.gear_queue_reserve(self.queues[i], new,
+                                                    torch.cuda.current_stream(self.device).cuda_stream),
+                               "gear_queue_reserve")
+                    self._capture(i)
+                    self.captures_regrown += 1
+                nxt.append(i)
             running = nxt
-        self.rounds = rounds
         return res

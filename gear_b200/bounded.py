@@ -93,6 +93,12 @@ class BoundedModule:
         eng = self._engines.get(key)
         if eng is None:
             with torch.cuda.device(self.device):
+                if self.bound_opts.get("gear_mode", "auto") == "tune":
+                    from .autotune import TunedEngine
+                    eng = TunedEngine(self.graph, spec_rows=spec_rows, dense_c=dense_c,
+                                      tie_rule=self.bound_opts.get("gear_tie_rule", "reference"))
+                    self._engines[key] = eng
+                    return eng
                 eng = CrownEngine(self.graph, spec_rows=spec_rows, dense_c=dense_c,
                                   mode=self.bound_opts.get("gear_mode", "auto"),
                                   cta_threads=int(self.bound_opts.get("gear_cta_threads", 128)),

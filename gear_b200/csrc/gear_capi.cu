@@ -1269,6 +1269,54 @@ extern "C" int gear_queue_destroy(gear_queue* q) {
   return GEAR_OK;
 }
 
+namespace {
+__global__ void append_free_kernel(int32_t* free_list, int64_t nf, int64_t first, int64_t count) {
+  const int64_t i = (int64_t)blockIdx.x * gear::bab::BT + threadIdx.x;
+  if (i < count) free_list[nf + i] = (int32_t)(first + i);
+}
+}  // namespace
+
+extern "C" int gear_queue_reserve(gear_queue* q, int64_t capacity, void* stream) {
+  using namespace gear::bq;
+  if (!q || capacity > ((int64_t)1 << 31) - 1) return fail(GEAR_E_INVALID, "gear_queue_reserve: %s", "bad arguments");
+  if (capacity <= q->q.cap) return GEAR_OK;
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  int64_t cnt[C_COUNT];
+  if (e == cudaSuccess) e = cudaMemcpy(cnt, q->q.counters, sizeof(cnt), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "gear_queue_reserve");
+  gear_queue nh = *q;
+  const int64_t old = q->q.cap;
+  const int n = q->q.n, S = q->q.S;
+  nh.q.cap = capacity;
+  const int64_t bytes = queue_layout(&nh, nullptr);
+  e = cudaMalloc(&nh.dev, bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(queue)");
+  queue_layout(&nh, (char*)nh.dev);
+  struct Copy { void* dst; const void* src; size_t bytes; };
+  const Copy copies[] = {
+      {nh.q.lo, q->q.lo, (size_t)old * n * 8}, {nh.q.hi, q->q.hi, (size_t)old * n * 8},
+      {nh.q.key, q->q.key, (size_t)old * S * 8}, {nh.q.key0, q->q.key0, (size_t)old * 8},
+      {nh.q.ids, q->q.ids, (size_t)old * 8}, {nh.q.active, q->q.active, (size_t)old * 4},
+      {nh.q.free_list, q->q.free_list, (size_t)old * 4}, {nh.q.counters, q->q.counters, (size_t)C_COUNT * 8},
+      {nh.q.disc_min, q->q.disc_min, 8}, {nh.q.root_lo, q->q.root_lo, (size_t)n * 8},
+      {nh.q.root_hi, q->q.root_hi, (size_t)n * 8}, {nh.root_width, q->root_width, (size_t)n * 8}};
+  for (const Copy& c : copies) {
+    e = cudaMemcpy(c.dst, c.src, c.bytes, cudaMemcpyDeviceToDevice);
+    if (e != cudaSuccess) { cudaFree(nh.dev); return cuda_fail(e, "gear_queue_reserve copy"); }
+  }
+  const int64_t nf = cnt[C_FREE], add = capacity - old;
+  append_free_kernel<<<grid_for(add), gear::bab::BT>>>(nh.q.free_list, nf, old, add);
+  cnt[C_FREE] = nf + add;
+  e = cudaMemcpy(nh.q.counters, cnt, sizeof(cnt), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) { cudaFree(nh.dev); return cuda_fail(e, "gear_queue_reserve"); }
+  cudaFree(q->dev);
+  *q = nh;
+  return GEAR_OK;
+}
+
+extern "C" int64_t gear_queue_capacity(const gear_queue* q) { return q ? q->q.cap : -1; }
+
 extern "C" int gear_queue_counters(const gear_queue* q, int64_t* counters, double* dual, void* stream) {
   if (!q || !counters) return fail(GEAR_E_INVALID, "gear_queue_counters: %s", "bad arguments");
   cudaStream_t st = (cudaStream_t)stream;

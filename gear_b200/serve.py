@@ -28,6 +28,27 @@ from .engine import PACK_SMEM_LIMIT, SIMT_PACK_ITEMS, _Dag, smem_class
 from .program import Program, simt_items
 
 
+def _compile_program(graph, cta_threads, simt_items_max):
+    """A request's program: one box per thread when its per-box state is small, else one box per
+    CTA (the choice of Server._admit)."""
+    prog = Program(graph, mode="simt")
+    if simt_items(prog) > simt_items_max:
+        prog = Program(graph, mode="cta", cta_threads=cta_threads, smem_limit=PACK_SMEM_LIMIT)
+    return prog
+
+
+def _compile_request(args):
+    """Pool job: trace a request's model and compile its program (stripped for the trip back)."""
+    from .program import stripped
+    model, lo, cta_threads, simt_items_max = args
+    g = _graph.trace(model, lo.repeat(2, 1))
+    return g, stripped(_compile_program(g, cta_threads, simt_items_max))
+
+
+def _warm(_):
+    return 0
+
+
 @dataclass
 class Request:
     key: object
@@ -45,6 +66,8 @@ class Request:
     bounded: int = 0
     status: str = "waiting"            # waiting, running, closed, emptied, budget
     group: tuple = ()                  # kernel group: (mode, threads, global working set, smem class)
+    compiled: object = None            # future of (graph, program) from the compile pool, or None
+    program: object = None             # the compiled program once known
 
 
 @dataclass
@@ -68,7 +91,9 @@ class Server:
     round_bytes / (its algorithmic bytes per box) domains per round, clamped to
     [min_batch, batch]: small instances take large batches (fewer rounds to their gap) and
     large ones do not stretch every round. max_live: at most this many instances run at once
-    (a round's host work grows with the number of live instances); the others wait. admission:
+    (a round's host work grows with the number of live instances); the others wait. compile_workers:
+    trace and compile arriving requests in a pool of that many processes (spawned) instead of in
+    the loop (a program of n = 2000 takes tens of milliseconds to compile). admission:
     "fifo" admits waiting requests in arrival order, "small_first" the narrowest boxes first
     (the quickest to close). incumbent_every: each instance evaluates its model at the popped
     midpoints on every k-th of its rounds only (BaB(incumbent_every=k)). round_cap: a round
@@ -79,7 +104,7 @@ class Server:
                  hbm_budget: Optional[int] = None, cta_threads: int = 256, simt_items_max: int = SIMT_PACK_ITEMS,
                  ibp_enhancement: bool = True, clock=time.perf_counter, round_bytes: Optional[int] = None,
                  min_batch: int = 16, max_live: Optional[int] = None, admission: str = "fifo",
-                 incumbent_every: int = 1, round_cap: Optional[int] = None):
+                 incumbent_every: int = 1, round_cap: Optional[int] = None, compile_workers: int = 0):
         if not torch.cuda.is_available():
             raise _lib.GearError("gear_b200 needs a CUDA device (no CPU fallback)")
         self.device = torch.device(device)
@@ -107,17 +132,35 @@ class Server:
         self.bounded = 0
         self.max_live = 0
         self._ws: Dict[tuple, torch.Tensor] = {}
+        self.pool = None
+        if compile_workers:
+            import multiprocessing as mp
+            from concurrent.futures import ProcessPoolExecutor
+            self.pool = ProcessPoolExecutor(max_workers=compile_workers, mp_context=mp.get_context("spawn"))
+            list(self.pool.map(_warm, range(compile_workers)))   # workers import torch before arrivals
 
     # ------------------------------------------------------------------ requests
     def submit(self, key, model: torch.nn.Module, lo: torch.Tensor, hi: torch.Tensor,
                rhs: Optional[torch.Tensor] = None, arrival: Optional[float] = None):
-        """Queue a request: minimise model(x)[0] s.t. model(x)[1:] <= rhs over lo <= x <= hi."""
+        """Queue a request: minimise model(x)[0] s.t. model(x)[1:] <= rhs over lo <= x <= hi.
+        With compile_workers, the request's trace and program compile run in the pool and it
+        becomes admissible when they are done."""
         lo = lo.reshape(1, -1).to(torch.float64).cpu()
         hi = hi.reshape(1, -1).to(torch.float64).cpu()
         r = Request(key, model, lo, hi, rhs, self.clock() if arrival is None else arrival)
-        r.graph = _graph.trace(model.to(torch.float64).cpu(), lo.repeat(2, 1))
+        if self.pool is not None:
+            r.compiled = self.pool.submit(_compile_request, (model.to(torch.float64).cpu(), lo, self.cta_threads,
+                                                             self.simt_items_max))
+        else:
+            r.graph = _graph.trace(model.to(torch.float64).cpu(), lo.repeat(2, 1))
         self.waiting.append(r)
         return r
+
+    def close(self):
+        """Stop the compile pool (if any)."""
+        if self.pool is not None:
+            self.pool.shutdown(wait=False, cancel_futures=True)
+            self.pool = None
 
     def _estimate(self, n, S, prog):
         """Device bytes an instance holds: its program, a queue of 8 batches and one round's
@@ -143,29 +186,40 @@ class Server:
             if r.arrival > now or (self.live_cap is not None and len(self.live) >= self.live_cap):
                 still.append(r)
                 continue
-            g = r.graph
-            prog = Program(g, mode="simt")
-            group = ("simt", 0, False, 0)
-            if simt_items(prog) > self.simt_items_max:
-                prog = Program(g, mode="cta", cta_threads=self.cta_threads, smem_limit=PACK_SMEM_LIMIT)
-                group = ("cta", self.cta_threads, prog.pass_global > 0, smem_class(prog))
+            if r.compiled is not None:
+                if not r.compiled.done():
+                    still.append(r)                  # its program is still being compiled
+                    continue
+                r.graph, prog = r.compiled.result()
+                r.compiled = None
+                r.program = prog
+            elif r.program is not None:
+                prog = r.program
+            else:
+                prog = _compile_program(r.graph, self.cta_threads, self.simt_items_max)
+            group = ("simt", 0, False, 0) if prog.mode == "simt" else \
+                ("cta", self.cta_threads, prog.pass_global > 0, smem_class(prog))
             est = self._estimate(prog.n, prog.S, prog)
             if torch.cuda.memory_allocated(self.device) + est > self.hbm_budget:
                 still.append(r)                      # no room yet: admitted when memory frees up
                 continue
             dag = _Dag.from_program(prog)
-            model = r.model.to(self.device)
             batch = self.batch
             if self.round_bytes:
                 batch = int(min(self.batch, max(self.min_batch, self.round_bytes // max(prog.alg_bytes_per_box(), 1))))
-            bab = BaB(g, r.lo, r.hi, rhs=r.rhs, device=str(self.device), batch=batch,
-                      engine=_Shape(prog.n, prog.S), model=model, ibp_enhancement=self.ibp_enhancement,
-                      incumbent_every=self.incumbent_every)
             r.admitted = now
             r.status = "running"
             r.group = group
-            self.live[r.key] = _Live(r, dag, bab, group, prog.alg_bytes_per_box(), est)
+            self.live[r.key] = self._make_live(r, prog, dag, group, batch, est)
         self.waiting = sorted(still, key=lambda r: r.arrival)
+
+    def _make_live(self, r, prog, dag, group, batch, est):
+        """The running state of an admitted request (a host-driven BaB over its device queue)."""
+        model = r.model.to(self.device)
+        bab = BaB(r.graph, r.lo, r.hi, rhs=r.rhs, device=str(self.device), batch=batch,
+                  engine=_Shape(prog.n, prog.S), model=model, ibp_enhancement=self.ibp_enhancement,
+                  incumbent_every=self.incumbent_every)
+        return _Live(r, dag, bab, group, prog.alg_bytes_per_box(), est)
 
     # ------------------------------------------------------------------ one round
     def _bound(self, popped, ibp):
@@ -251,3 +305,218 @@ class Server:
 
     def idle(self) -> bool:
         return not self.live and not self.waiting
+
+
+@dataclass
+class _LiveDQ:
+    req: Request
+    dag: _Dag
+    q: object                  # gear_queue handle (ctypes.c_void_p)
+    batch: int
+    group: tuple
+    cost: int
+    est_bytes: int
+    cap: int
+    boxes: tuple               # (lo, hi) (batch, n): the popped batch
+    outs: tuple                # (lb, lA, lbias) of the batch
+    ibp: Optional[torch.Tensor]
+    status: torch.Tensor       # (10,) float64: 8 counters, dual bound, incumbent (written on the device)
+    graphs: dict               # "pop", "pop_propose", "step": CUDA graphs of the instance's round
+    keep: tuple                # tensors the graphs read or write (kept alive with them)
+
+    def release(self):
+        self.graphs = {}
+        if self.q is not None and self.q.value:
+            _lib.lib().gear_queue_destroy(self.q)
+            self.q = None
+
+
+class DeviceServer(Server):
+    """The serving loop with every admitted request's queue on the device and its round captured
+    into CUDA graphs once, at admission.
+
+    Each request gets a gear_queue (capacity from queue_bytes) and three graphs: its pop, its pop
+    followed by the incumbent proposal (the model at the popped midpoints), and its
+    gear_bab_step_bounded followed by a copy of its counters, dual bound and incumbent into a
+    status row. A round replays the pop graph of every running request, makes one prepared
+    many-instance CROWN launch per kernel group for all their batches (re-planned only when the
+    set of running requests changes), replays their step graphs and reads every status row in one
+    copy: the host cost of a request per round is two graph launches instead of dozens of launches
+    and a synchronisation. Same admission, time budget and retirement rules as Server, and each
+    request's search is the one BaB runs for it alone (tested)."""
+
+    def __init__(self, *args, queue_bytes: int = 256 << 20, **kwargs):
+        super().__init__(*args, **kwargs)
+        self.queue_bytes = queue_bytes
+        self._plan_keys = None
+        self._plans = []
+
+    def _estimate(self, n, S, prog):
+        batch = self.batch
+        if self.round_bytes:
+            batch = int(min(self.batch, max(self.min_batch, self.round_bytes // max(prog.alg_bytes_per_box(), 1))))
+        per_box = 8 * (2 * n + 4 * S + S * n)
+        prog_b = 4 * prog.int_pool.size + 8 * prog.dbl_pool.size + 4 * (prog.node_arr.size + prog.op_arr.size)
+        return prog_b + self._cap(n, S, batch) * (8 * (2 * n + S + 2) + 12) + 4 * batch * per_box
+
+    def _cap(self, n, S, batch):
+        return int(max(4 * batch + 1, min(256 * batch, self.queue_bytes // (8 * (2 * n + S + 2) + 12))))
+
+    def _make_live(self, r, prog, dag, group, batch, est):
+        import ctypes
+        L = _lib.lib()
+        dev = self.device
+        n, S = prog.n, prog.S
+        cap = self._cap(n, S, batch)
+        lo = r.lo.reshape(-1).contiguous()
+        hi = r.hi.reshape(-1).contiguous()
+        h = ctypes.c_void_p()
+        _lib.check(L.gear_queue_create(n, S, cap, batch, lo.data_ptr(), hi.data_ptr(), ctypes.byref(h)),
+                   "gear_queue_create")
+        plo = torch.empty(batch, n, dtype=torch.float64, device=dev)
+        phi = torch.empty_like(plo)
+        lb = torch.empty(batch, S, dtype=torch.float64, device=dev)
+        lA = torch.empty(batch, S, n, dtype=torch.float64, device=dev)
+        lbias = torch.empty_like(lb)
+        ibp = torch.empty_like(lb) if self.ibp_enhancement else None
+        inc = torch.full((1,), math.inf, dtype=torch.float64, device=dev)
+        x_best = ((r.lo + r.hi) / 2).reshape(-1).to(dev)
+        rr = r.rhs if r.rhs is not None else torch.zeros(S - 1, dtype=torch.float64)
+        rhs = torch.cat([rr.to(torch.float64).reshape(-1).to(dev), torch.zeros(1, dtype=torch.float64, device=dev)])
+        counters = torch.zeros(8, dtype=torch.int64, device=dev)
+        dual = torch.full((1,), -math.inf, dtype=torch.float64, device=dev)
+        status = torch.zeros(10, dtype=torch.float64, device=dev)
+        model = r.model.to(dev)
+
+        def pop():
+            st = torch.cuda.current_stream(dev).cuda_stream
+            _lib.check(L.gear_queue_pop(h, plo.data_ptr(), phi.data_ptr(), st), "gear_queue_pop")
+
+        def propose():
+            with torch.no_grad():
+                x = (plo + phi) / 2
+                y = model(x)
+                feas = (y[:, 1:] <= rhs[:S - 1]).all(1) if y.shape[1] > 1 else \
+                    torch.ones(y.shape[0], dtype=torch.bool, device=dev)
+                obj = torch.where(feas, y[:, 0], torch.full_like(y[:, 0], math.inf))
+                best = obj.min(0)
+                val = best.values.reshape(1)
+                pt = x.index_select(0, best.indices.reshape(1)).reshape(-1)
+                x_best.copy_(torch.where(val < inc, pt, x_best))
+                inc.copy_(torch.minimum(inc, val))
+
+        def step():
+            st = torch.cuda.current_stream(dev).cuda_stream
+            _lib.check(L.gear_bab_step_bounded(h, plo.data_ptr(), phi.data_ptr(), lb.data_ptr(), lA.data_ptr(),
+                                               lbias.data_ptr(), inc.data_ptr(), rhs.data_ptr(), 1e-3, 1e-3, st),
+                       "gear_bab_step_bounded")
+            _lib.check(L.gear_queue_counters(h, counters.data_ptr(), dual.data_ptr(), st), "gear_queue_counters")
+            status.copy_(torch.cat([counters.to(torch.float64), dual, inc]))
+
+        graphs = {}
+        for name, fns in (("pop", (pop,)), ("pop_propose", (pop, propose)), ("step", (step,))):
+            gr = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(gr):
+                for f in fns:
+                    f()
+            graphs[name] = gr
+        keep = (plo, phi, lb, lA, lbias, ibp, inc, x_best, rhs, counters, dual, model, lo, hi)
+        return _LiveDQ(r, dag, h, batch, group, prog.alg_bytes_per_box(), est, cap, (plo, phi), (lb, lA, lbias), ibp,
+                       status, graphs, keep)
+
+    def _prepare(self, keys):
+        """One prepared many-instance launch per kernel group for these requests' batches."""
+        L = _lib.lib()
+        for h, _ in self._plans:
+            L.gear_crown_multi_plan_destroy(h)
+        self._plans = []
+        groups = {}
+        for k in keys:
+            groups.setdefault(self.live[k].group, []).append(k)
+        import ctypes
+        for gkey, ks in groups.items():
+            ks.sort(key=lambda k: -self.live[k].cost)        # expensive boxes first
+            args = (_lib.LowerArgs * len(ks))()
+            for j, k in enumerate(ks):
+                lv = self.live[k]
+                (plo, phi), (lb, lA, lbias) = lv.boxes, lv.outs
+                args[j] = _lib.LowerArgs(lv.dag.handle.value, plo.data_ptr(), phi.data_ptr(), lv.batch, None,
+                                         lb.data_ptr(), lA.data_ptr(), lbias.data_ptr(),
+                                         lv.ibp.data_ptr() if lv.ibp is not None else None)
+            nbytes = int(L.gear_crown_multi_workspace_bytes(args, len(args)))
+            if nbytes < 0:
+                _lib.check(-1, "gear_crown_multi_workspace_bytes")
+            ws = torch.empty(max(nbytes, 8), dtype=torch.uint8, device=self.device)
+            h = ctypes.c_void_p()
+            _lib.check(L.gear_crown_multi_prepare(args, len(args), ws.data_ptr(), ws.numel(), ctypes.byref(h)),
+                       "gear_crown_multi_prepare")
+            self._plans.append((h, ws))
+        self._plan_keys = tuple(keys)
+
+    def step(self, now: Optional[float] = None) -> int:
+        """Admit, run one round over the running requests, retire; returns the domains bounded."""
+        given = now is not None
+        now = now if given else self.clock()
+        self._admit(now)
+        self.max_live = max(self.max_live, len(self.live))
+        if not self.live:
+            return 0
+        keys = list(self.live)
+        if self.round_cap is not None and len(keys) > self.round_cap:
+            keys = sorted(keys, key=lambda k: (self.live[k].req.lo.shape[1], self.live[k].req.arrival))
+            keys = keys[:self.round_cap]
+        t0 = time.perf_counter()
+        if self._plan_keys != tuple(keys):
+            self._prepare(keys)
+        every = max(1, int(self.incumbent_every))
+        for k in keys:
+            lv = self.live[k]
+            lv.graphs["pop_propose" if lv.req.rounds % every == 0 else "pop"].replay()
+        t1 = time.perf_counter()
+        L = _lib.lib()
+        st = torch.cuda.current_stream(self.device).cuda_stream
+        for h, _ in self._plans:
+            _lib.check(L.gear_crown_multi_launch(h, st), "gear_crown_multi_launch")
+        self.t_bound += time.perf_counter() - t1
+        for k in keys:
+            self.live[k].graphs["step"].replay()
+        rows = torch.stack([self.live[k].status for k in keys]).cpu().tolist()
+        self.t_round += time.perf_counter() - t0
+        self.rounds += 1
+        t = now if given else self.clock()
+        bounded = 0
+        for k, row in zip(keys, rows):
+            lv = self.live[k]
+            r = lv.req
+            r.rounds += 1
+            prev = r.bounded
+            r.bounded = int(row[3])
+            bounded += r.bounded - prev
+            r.P = row[9]
+            r.gap = BaB._gap(row[9], row[8])
+        self.bounded += bounded
+        for k in list(self.live):
+            lv = self.live[k]
+            r = lv.req
+            status = None
+            if k in keys:
+                row = rows[keys.index(k)]
+                if r.gap <= self.rel_gap:
+                    status = "closed"
+                elif int(row[0]) == 0:
+                    status = "emptied"
+                elif int(row[0]) + lv.batch > lv.cap or int(row[7]):
+                    status = "memory"
+            if status is None and t - r.arrival > self.time_budget:
+                status = "budget"
+            if status:
+                r.status, r.finished = status, t
+                self.done[k] = r
+                del self.live[k]
+                lv.release()
+        if self._plan_keys is not None and any(k not in self.live for k in self._plan_keys):
+            self._plan_keys = None          # re-plan next round (its instances' buffers may be freed)
+            for h, _ in self._plans:
+                L.gear_crown_multi_plan_destroy(h)
+            self._plans = []
+        return bounded

@@ -164,6 +164,11 @@ int gear_queue_push(gear_queue* q, const double* lo, const double* hi, const dou
 int gear_queue_pop(gear_queue* q, double* lo_out, double* hi_out, void* stream);
 int gear_queue_size(const gear_queue* q, int64_t* open, void* stream);
 int gear_queue_counters(const gear_queue* q, int64_t* counters, double* dual, void* stream);
+/* Grow the queue to `capacity` slots (synchronous: waits for `stream`, copies the open domains into
+ * a new block, frees the old one). The queue's device pointers change: work captured into a CUDA
+ * graph that uses it must be captured again. gear_queue_capacity: the current capacity. */
+int gear_queue_reserve(gear_queue* q, int64_t capacity, void* stream);
+int64_t gear_queue_capacity(const gear_queue* q);
 int64_t gear_bab_step_workspace_bytes(const gear_dag* dag, int64_t batch);
 int gear_bab_step(gear_queue* q, const gear_dag* dag, const double* lo, const double* hi, const double* incumbent,
                   const double* rhs, double sb_coeff_thresh, double sb_min_width_ratio, int ibp_enhancement,

@@ -84,10 +84,11 @@ def test_graph_bab_reaches_the_gap():
     m = problems.make_instance("quad_exp_n10", 2)
     lo, hi = problems.root_box("quad_exp_n10")
     g = graph.trace(m, lo.repeat(2, 1))
-    b = GraphBaB(g, lo, hi, batch=2048, model=m.cuda(), device="cuda")
+    # a small first capacity: the queue grows during the run and the iterations are captured again
+    b = GraphBaB(g, lo, hi, batch=2048, model=m.cuda(), device="cuda", capacity=20000)
     P, D, gap = b.run(rel_gap=1e-4, time_limit=120)
     assert gap <= 1e-4 and math.isfinite(P) and D <= P
-    assert b.status["overflow"] == 0
+    assert b.status["overflow"] == 0 and b.regrown > 0
 
 
 def test_multi_graph_bab_equals_each_instance_alone():
@@ -102,13 +103,20 @@ def test_multi_graph_bab_equals_each_instance_alone():
              for m in insts]
     models = [m.cuda() for m in insts]
     me = MultiEngine(graphs, mode="auto", cta_threads=128)
-    mb = MultiGraphBaB(graphs, roots, models, batch=128, engine=me, chunk=2)
-    res = mb.run(rel_gap=-1.0, time_limit=600, max_rounds=6)
-    assert mb.rounds == 6 and mb.captures == 1 and mb.replays == 2
+    # small first queues (70 slots for batches of 32): they grow during the run
+    mb = MultiGraphBaB(graphs, roots, models, batch=32, engine=me, queue_slots=70)
+    res = mb.run(rel_gap=-1.0, time_limit=600, max_rounds=10)
+    assert mb.rounds == 10 and mb.prepares >= 1
+    assert mb.captures_regrown > 0                        # queues grew (their graphs captured again)
+    compared = 0
     for i, g in enumerate(graphs):
+        if res[i]["status"] != "running":
+            continue                                      # retired early (emptied its queue)
         var = me.variants[i]
         eng = CrownEngine(g, mode=var[0], cta_threads=var[1] or 128)
-        b = GraphBaB(g, roots[i][0], roots[i][1], batch=128, model=models[i], engine=eng, chunk=2)
-        P, D, _ = b.run(rel_gap=-1.0, max_iterations=6, time_limit=600)
-        assert b.status["iterations"] == 6
+        b = GraphBaB(g, roots[i][0], roots[i][1], batch=32, model=models[i], engine=eng, chunk=2)
+        P, D, _ = b.run(rel_gap=-1.0, max_iterations=10, time_limit=600)
+        assert b.status["iterations"] == 10
         assert res[i]["P"] == P and res[i]["D"] == D and res[i]["bounded"] == b.status["bounded"]
+        compared += 1
+    assert compared >= 3

@@ -1,6 +1,7 @@
 """Serving loop (continuous batching): requests submitted while others run are admitted at the
 next round, and every request's result -- incumbent, domains bounded, relative gap, rounds --
-is the same as its own branch and bound run alone with the same kernel variant."""
+is the same as its own branch and bound run alone with the same kernel variant. Both forms: the
+host-driven rounds (Server) and device queues with per-request CUDA graphs (DeviceServer)."""
 import math
 
 import pytest
@@ -9,7 +10,7 @@ import torch
 from gear_b200 import problems
 from gear_b200.bab import BaB
 from gear_b200.engine import CrownEngine
-from gear_b200.serve import Server
+from gear_b200.serve import DeviceServer, Server
 
 pytestmark = pytest.mark.gpu
 
@@ -19,11 +20,12 @@ def _req(k, n):
     return m, torch.full((1, n), -2.0, dtype=torch.float64), torch.full((1, n), 2.0, dtype=torch.float64)
 
 
-def test_serve_same_alone_and_in_mix():
+@pytest.mark.parametrize("cls", [Server, DeviceServer])
+def test_serve_same_alone_and_in_mix(cls):
     sizes = [(0, 6), (1, 10), (2, 14), (3, 8), (4, 12), (5, 20)]
     # the clock advances one unit per round: a request leaves after at most 25 rounds in the
     # system (closed, emptied or at its budget), so the rounds each took part in differ
-    srv = Server(batch=64, rel_gap=1e-4, time_budget=25.0, admission="small_first", incumbent_every=3,
+    srv = cls(batch=64, rel_gap=1e-4, time_budget=25.0, admission="small_first", incumbent_every=3,
                  round_cap=3)
     reqs = {}
     clock = 0.0
@@ -54,9 +56,10 @@ def test_serve_same_alone_and_in_mix():
         assert (g_alone == r.gap) or (math.isinf(g_alone) and math.isinf(r.gap))
 
 
-def test_serve_admission_waits_for_memory():
+@pytest.mark.parametrize("cls", [Server, DeviceServer])
+def test_serve_admission_waits_for_memory(cls):
     """A request that does not fit the HBM budget waits; it is admitted once memory frees up."""
-    srv = Server(batch=32, rel_gap=1e-4, time_budget=1e9, hbm_budget=torch.cuda.memory_allocated() + 1)
+    srv = cls(batch=32, rel_gap=1e-4, time_budget=1e9, hbm_budget=torch.cuda.memory_allocated() + 1)
     m, lo, hi = _req(9, 6)
     r = srv.submit("a", m, lo, hi, arrival=0.0)
     srv.step(now=0.0)
