@@ -491,6 +491,34 @@ def plain_gpu(dev, workload, lo, hi, fused_value, steps=3, warmup=1):
                     "box state in global memory between launches"}, out
 
 
+def constrained(dev, cases=((1024, 200, 20), (4096, 50, 16), (65536, 200, 20)), steps=5, warmup=2):
+    """Constrained concretisation (the reference's sort_out_constr_batches + constraints_solving,
+    concretize_func.py:312-850, as one device call gear_constrained_lower) on
+    problems.cut_rows(batch, n, rows): one objective row per box, rows that cut, skip or exclude
+    the box. Inputs resident on the device; CUDA-event time per call. The first two cases are the
+    ones the reference's PyTorch sweep was timed on, on CPU cores, by oracle/reference_cpu.py."""
+    import torch
+    from gear_b200 import problems
+    from gear_b200.concretize import constraints_solving
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = []
+    for batch, n, rows in cases:
+        xl, xu, obj, A, b = (t.to(dev) for t in problems.cut_rows(batch, n, rows))
+        for _ in range(warmup):
+            lb, inf = constraints_solving(xl, xu, obj, (A, b), return_infeasible=True)
+        torch.cuda.synchronize(dev)
+        e0.record()
+        for _ in range(steps):
+            constraints_solving(xl, xu, obj, (A, b))
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / steps
+        out.append({"batch": batch, "n": n, "rows": rows, "ms_per_call": ms, "boxes_per_s": batch / (ms / 1000.0),
+                    "infeasible": int(inf.sum()), "finite_bounds": int(torch.isfinite(lb).sum()),
+                    "input_bytes": int(8 * batch * (2 * n + n + rows * n + rows))})
+    return {"api": "gear_b200.concretize.constraints_solving (gear_constrained_lower)", "cases": out}
+
+
 def dense_nodes(dev, batch=8192, steps=3, warmup=1):
     """The dense-node configuration (dense_a_n2048: y = A x with A 1024 x 2048, objective
     sum alpha_j y_j^2 + beta_j y_j y_{j+1}), `batch` boxes: CROWN with the fold products of the
@@ -582,6 +610,8 @@ def main():
                     help="run the serving loop under Poisson arrivals (50 per second) for this long; 0 skips it")
     ap.add_argument("--dense-batch", type=int, default=8192,
                     help="boxes of the dense-node configuration (dense_a_n2048, tensor-core fold); 0 skips it")
+    ap.add_argument("--no-constrained", dest="constrained", action="store_false",
+                    help="skip the constrained-concretisation block")
     ap.add_argument("--no-plain", dest="plain", action="store_false",
                     help="skip the plain GPU form (one launch per step and per op) on the workload")
     ap.add_argument("--workload", default=WORKLOAD, help="benchmark workload (profiling of other shapes)")
@@ -745,6 +775,8 @@ def main():
                         "closed": [res["mixed_bab"]["closed"], pb["closed"]], "target": 10.0}
         if args.dense_batch > 0:
             res["dense_nodes"] = dense_nodes(dev, batch=args.dense_batch)
+        if args.constrained:
+            res["constrained"] = constrained(dev)
         if args.serve_seconds > 0:
             res["serve"] = serve(dev, seconds=args.serve_seconds)
         if world == 1 and not args.no_cpu_baseline:

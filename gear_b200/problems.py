@@ -197,3 +197,20 @@ def root_box(workload: str, n: int = None):
     n = spec["n"] if n is None else n
     L, U = (-2.0, 2.0) if workload == "quad_exp_n10" else (-1.0, 1.0)
     return torch.full((1, n), L, dtype=F64), torch.full((1, n), U, dtype=F64)
+
+
+def cut_rows(batch: int, n: int, rows: int, objectives: int = 1, seed: int = 7000, t_lo: float = -1.1,
+             t_hi: float = 0.6):
+    """A constrained-concretisation workload: boxes (batch, n) of half-widths U(0.05, 0.95) around
+    centres U(-2, 2), objectives (batch, objectives, n) ~ N(0, 1) and rows A x + b <= 0 (A (batch,
+    rows, n) ~ N(0, 1)) whose plane sits at t ~ U(t_lo, t_hi) half-ranges of the row over its box
+    (t < -1: the row never binds; t > 1: it excludes the box; between: it cuts). float64, seeded."""
+    g = _gen(seed)
+    c = torch.rand(batch, n, generator=g, dtype=F64) * 4 - 2
+    w = torch.rand(batch, n, generator=g, dtype=F64) * 0.9 + 0.05
+    xl, xu = c - w, c + w
+    obj = torch.randn(batch, objectives, n, generator=g, dtype=F64)
+    A = torch.randn(batch, rows, n, generator=g, dtype=F64)
+    t = torch.rand(batch, rows, generator=g, dtype=F64) * (t_hi - t_lo) + t_lo
+    b = -(A * c[:, None]).sum(-1) + t * (A.abs() * w[:, None]).sum(-1)
+    return xl, xu, obj, A, b

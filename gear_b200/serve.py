@@ -16,6 +16,7 @@ batch_branch_and_bound.py``); this loop is the batching layer above that search.
 from __future__ import annotations
 
 import math
+import pickle
 import time
 from dataclasses import dataclass
 from typing import Dict, List, Optional
@@ -37,12 +38,14 @@ def _compile_program(graph, cta_threads, simt_items_max):
     return prog
 
 
-def _compile_request(args):
-    """Pool job: trace a request's model and compile its program (stripped for the trip back)."""
+def _compile_request(blob):
+    """Pool job: trace a request's model and compile its program (stripped for the trip back).
+    Arguments and result travel as plain pickles (tensors by value): torch's process-sharing
+    reductions would hold a file descriptor per tensor in the server for as long as it lives."""
     from .program import stripped
-    model, lo, cta_threads, simt_items_max = args
+    model, lo, cta_threads, simt_items_max = pickle.loads(blob)
     g = _graph.trace(model, lo.repeat(2, 1))
-    return g, stripped(_compile_program(g, cta_threads, simt_items_max))
+    return pickle.dumps((g, stripped(_compile_program(g, cta_threads, simt_items_max))))
 
 
 def _warm(_):
@@ -149,8 +152,8 @@ class Server:
         hi = hi.reshape(1, -1).to(torch.float64).cpu()
         r = Request(key, model, lo, hi, rhs, self.clock() if arrival is None else arrival)
         if self.pool is not None:
-            r.compiled = self.pool.submit(_compile_request, (model.to(torch.float64).cpu(), lo, self.cta_threads,
-                                                             self.simt_items_max))
+            r.compiled = self.pool.submit(_compile_request, pickle.dumps(
+                (model.to(torch.float64).cpu(), lo, self.cta_threads, self.simt_items_max)))
         else:
             r.graph = _graph.trace(model.to(torch.float64).cpu(), lo.repeat(2, 1))
         self.waiting.append(r)
@@ -190,7 +193,7 @@ class Server:
                 if not r.compiled.done():
                     still.append(r)                  # its program is still being compiled
                     continue
-                r.graph, prog = r.compiled.result()
+                r.graph, prog = pickle.loads(r.compiled.result())
                 r.compiled = None
                 r.program = prog
             elif r.program is not None:

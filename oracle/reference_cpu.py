@@ -154,6 +154,33 @@ def time_compute_bounds(workload, batch, reps=3):
             "reference_boxes_per_s": batch / min(ref), "port_boxes_per_s": batch / min(port)}
 
 
+def time_constrained(batch, n, rows, reps=3):
+    """Seconds per reference constrained concretisation (sort_out_constr_batches +
+    constraints_solving, concretize_func.py:312-850, the PyTorch sweep, sign -1) of
+    problems.cut_rows(batch, n, rows): best of reps after one warm-up; and of the numpy
+    restatement oracle/concretize.py on the same inputs (one call: a per-box loop)."""
+    from auto_LiRPA import concretize_func as cf
+    from gear_b200 import problems
+    from oracle import concretize as oc
+    xl, xu, obj, A, b = problems.cut_rows(batch, n, rows)
+    cf.MAX_CONSTRAINT_ROWS = None
+
+    def ref():
+        cons, masks = cf.sort_out_constr_batches(xl, xu, (A, b))
+        return cf.constraints_solving(xl, xu, obj, cons, -1.0, sorted_out_batches=masks or {})
+    ref()
+    tr = []
+    for _ in range(reps):
+        t = time.perf_counter()
+        ref()
+        tr.append(time.perf_counter() - t)
+    args = (xl.numpy(), xu.numpy(), obj.numpy(), A.numpy(), b.numpy())
+    t = time.perf_counter()
+    oc.constrained_lower(*args)
+    tp = [time.perf_counter() - t]
+    return {"batch": batch, "n": n, "rows": rows, "reference_s": min(tr), "port_s": min(tp)}
+
+
 def reference_bab(inst, rel_gap=1e-4, batch=2048, time_limit=600.0):
     """Branch and bound to the relative gap on quad_exp_n10 instance `inst` with the reference's
     step functions; returns wall seconds, iterations, domains bounded and the final gap."""
@@ -226,6 +253,7 @@ def main():
     cores = os.cpu_count() or 1
     torch.set_num_threads(cores)
     rows = [time_compute_bounds("quad_exp_n10", 256), time_compute_bounds("dense_q_n200", 256)]
+    cons = [time_constrained(1024, 200, 20), time_constrained(4096, 50, 16)]
     babs = [reference_bab(i) for i in range(args.bab_instances)]
     lines = ["# The reference's own CPU path, timed on this build container's cores", "",
              f"Command: `python oracle/reference_cpu.py REFERENCE_ROOT` ({cores} cores, torch threads = {cores}, "
@@ -236,6 +264,12 @@ def main():
     for r in rows:
         lines.append(f"| {r['workload']} | {r['batch']} | {r['reference_s']:.3f} s | {r['reference_boxes_per_s']:.0f} | "
                      f"{r['port_s']:.3f} s | {r['port_boxes_per_s']:.0f} | {r['port_s'] / r['reference_s']:.2f} |")
+    lines += ["", "Constrained concretisation (sort_out_constr_batches + constraints_solving, sign -1, no row cap) "
+              "of `gear_b200.problems.cut_rows(batch, n, rows)`, one objective row per box:", "",
+              "| batch | n | rows | reference | boxes/s | numpy port | boxes/s |", "|---|---|---|---|---|---|---|"]
+    for r in cons:
+        lines.append(f"| {r['batch']} | {r['n']} | {r['rows']} | {r['reference_s']:.3f} s | "
+                     f"{r['batch'] / r['reference_s']:.0f} | {r['port_s']:.3f} s | {r['batch'] / r['port_s']:.0f} |")
     lines += ["", "Branch and bound to relative gap 1e-4 with the reference's step functions (batch 2048, "
               "quad_exp_n10 instances, CROWN bounds, incumbent from box midpoints):", "",
               "| instance | wall s | iterations | domains bounded | domains/s | final gap |", "|---|---|---|---|---|---|"]

@@ -70,3 +70,27 @@ def test_serve_admission_waits_for_memory(cls):
         if srv.idle():
             break
     assert r.status in ("closed", "emptied") and r.admitted == 1.0
+
+
+def test_serve_compile_pool_same_results():
+    """Requests traced and compiled in the spawned pool (compile_workers) give the same results as
+    ones compiled in the serving process, once their programs are ready."""
+    sizes = [(0, 6), (1, 10), (2, 14), (3, 25)]
+    out = {}
+    for workers in (0, 2):
+        srv = DeviceServer(batch=64, rel_gap=1e-4, time_budget=25.0, incumbent_every=3, round_cap=3,
+                           compile_workers=workers)
+        try:
+            reqs = [srv.submit(k, *_req(k, n), arrival=0.0) for k, n in sizes]
+            for r in reqs:
+                if r.compiled is not None:
+                    r.compiled.result(timeout=600)
+            clock = 0.0
+            while not srv.idle():
+                srv.step(now=clock)
+                clock += 1.0
+                assert srv.rounds < 100
+            out[workers] = {k: (r.P, r.bounded, r.gap, r.rounds, r.group) for k, r in srv.done.items()}
+        finally:
+            srv.close()
+    assert out[0] == out[2]
