@@ -397,8 +397,8 @@ def mixed_bab(dev, setup, batch=256, rel_gap=1e-4, time_limit=60.0, plain=False,
 
 
 def serve(dev, seconds=10.0, rate=50.0, budget=30.0, batch=2048, rel_gap=1e-4, seed=0, round_bytes=16 << 20,
-          max_live=128, admission="small_first", incumbent_every=4, round_cap=16, device_queues=False,
-          compile_workers=8):
+          max_live=128, admission="small_first", incumbent_every=4, round_cap=32, device_queues=True,
+          compile_workers=8, preempt=False):
     """The serving loop under Poisson arrivals (rate per second for `seconds`): instances of the
     quad-exp family with n log-uniform in [5, 2000] (two bilinear constraints), each to the
     relative gap or its time budget (from arrival). Continuous batching: requests are admitted as
@@ -419,7 +419,8 @@ def serve(dev, seconds=10.0, rate=50.0, budget=30.0, batch=2048, rel_gap=1e-4, s
     ns = [int(round(_m.exp(_m.log(5) + (_m.log(2000) - _m.log(5)) * float(torch.rand(1, generator=g)))))
           for _ in arrivals]
     srv = (DeviceServer if device_queues else Server)(device=str(dev), compile_workers=compile_workers, batch=batch, rel_gap=rel_gap, time_budget=budget, round_bytes=round_bytes,
-                 max_live=max_live, admission=admission, incumbent_every=incumbent_every, round_cap=round_cap)
+                 max_live=max_live, admission=admission, incumbent_every=incumbent_every, round_cap=round_cap,
+                 preempt=preempt)
     t0 = time.perf_counter()
     clock = lambda: time.perf_counter() - t0
     srv.clock = clock
@@ -446,13 +447,17 @@ def serve(dev, seconds=10.0, rate=50.0, budget=30.0, batch=2048, rel_gap=1e-4, s
             "arrival_seconds": seconds, "requests": len(arrivals), "closed": len(ttg),
             "budget_reached": sum(1 for r in done if r.status == "budget"),
             "emptied": sum(1 for r in done if r.status == "emptied"),
+            "preempted": sum(1 for r in done if r.status == "preempted"),
+            "closed_by_n": {f"{a}-{b}": [sum(1 for r in done if a <= r.lo.shape[1] <= b and r.status == "closed"),
+                                         sum(1 for r in done if a <= r.lo.shape[1] <= b)]
+                            for a, b in ((5, 10), (11, 15), (16, 20), (21, 50), (51, 2000))},
             "time_to_gap_s": {"p50": q(ttg, 0.5), "p99": q(ttg, 0.99)},
             "time_in_system_s": {"p50": q(tis, 0.5), "p99": q(tis, 0.99)},
             "subdomains_per_s": srv.bounded / wall, "rounds": srv.rounds, "max_concurrent": srv.max_live,
             "rel_gap": rel_gap, "budget_s": budget, "batch_per_instance_max": batch, "round_bytes": round_bytes,
             "max_live": max_live, "waited_out": sum(1 for r in done if r.admitted is None),
             "admission": admission, "incumbent_every": incumbent_every, "round_cap": round_cap,
-            "compile_workers": compile_workers,
+            "compile_workers": compile_workers, "preempt": preempt,
             "closed_n_max": max((r.lo.shape[1] for r in done if r.status == "closed"), default=None),
             "host_s": {"rounds": srv.t_round, "crown_launch_calls": srv.t_bound}, "wall_s": wall,
             "form": "device queues, per-request CUDA graphs (DeviceServer)" if device_queues else

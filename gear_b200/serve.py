@@ -67,7 +67,7 @@ class Request:
     P: float = math.inf
     rounds: int = 0
     bounded: int = 0
-    status: str = "waiting"            # waiting, running, closed, emptied, budget
+    status: str = "waiting"            # waiting, running, closed, emptied, budget, memory, preempted
     group: tuple = ()                  # kernel group: (mode, threads, global working set, smem class)
     compiled: object = None            # future of (graph, program) from the compile pool, or None
     program: object = None             # the compiled program once known
@@ -101,13 +101,18 @@ class Server:
     (the quickest to close). incumbent_every: each instance evaluates its model at the popped
     midpoints on every k-th of its rounds only (BaB(incumbent_every=k)). round_cap: a round
     runs at most this many live instances, the narrowest boxes first (then by arrival); the
-    others keep their state and wait for a later round (their budget keeps running)."""
+    others keep their state and wait for a later round (their budget keeps running). preempt: when
+    max_live instances run and an arrived request is narrower (fewer inputs) than the widest of
+    them, that one leaves with status "preempted" to make room (the narrow requests are the ones
+    that can close within their budget; a wide one would otherwise hold its slot until its
+    budget runs out while narrow arrivals wait out theirs)."""
 
     def __init__(self, device="cuda", batch: int = 256, rel_gap: float = 1e-4, time_budget: float = 30.0,
                  hbm_budget: Optional[int] = None, cta_threads: int = 256, simt_items_max: int = SIMT_PACK_ITEMS,
                  ibp_enhancement: bool = True, clock=time.perf_counter, round_bytes: Optional[int] = None,
                  min_batch: int = 16, max_live: Optional[int] = None, admission: str = "fifo",
-                 incumbent_every: int = 1, round_cap: Optional[int] = None, compile_workers: int = 0):
+                 incumbent_every: int = 1, round_cap: Optional[int] = None, compile_workers: int = 0,
+                 preempt: bool = False):
         if not torch.cuda.is_available():
             raise _lib.GearError("gear_b200 needs a CUDA device (no CPU fallback)")
         self.device = torch.device(device)
@@ -122,6 +127,8 @@ class Server:
         self.admission = admission
         self.incumbent_every = incumbent_every
         self.round_cap = round_cap
+        self.preempt = preempt
+        self.preempted = 0
         self.t_bound = 0.0                 # host seconds in the CROWN launches / the rest of a round
         self.t_round = 0.0
         if hbm_budget is None:
@@ -186,9 +193,18 @@ class Server:
                 r.status, r.finished = "budget", now     # its budget ran out before a slot freed up
                 self.done[r.key] = r
                 continue
-            if r.arrival > now or (self.live_cap is not None and len(self.live) >= self.live_cap):
+            if r.arrival > now:
                 still.append(r)
                 continue
+            if self.live_cap is not None and len(self.live) >= self.live_cap:
+                widest = max(self.live, key=lambda k: (self.live[k].req.lo.shape[1], self.live[k].req.arrival)) \
+                    if self.preempt and self.live else None
+                if widest is None or self.live[widest].req.lo.shape[1] <= r.lo.shape[1] or \
+                        (r.compiled is not None and not r.compiled.done()):
+                    still.append(r)
+                    continue
+                self._retire(widest, "preempted", now)
+                self.preempted += 1
             if r.compiled is not None:
                 if not r.compiled.done():
                     still.append(r)                  # its program is still being compiled
@@ -215,6 +231,15 @@ class Server:
             r.group = group
             self.live[r.key] = self._make_live(r, prog, dag, group, batch, est)
         self.waiting = sorted(still, key=lambda r: r.arrival)
+
+    def _retire(self, k, status, t):
+        """Move a live request to done with this status (and free its device state)."""
+        lv = self.live.pop(k)
+        lv.req.status, lv.req.finished = status, t
+        self.done[k] = lv.req
+        release = getattr(lv, "release", None)
+        if release is not None:
+            release()
 
     def _make_live(self, r, prog, dag, group, batch, est):
         """The running state of an admitted request (a host-driven BaB over its device queue)."""
@@ -301,9 +326,7 @@ class Server:
             if status is None and t - r.arrival > self.time_budget:
                 status = "budget"
             if status:
-                r.status, r.finished = status, t
-                self.done[k] = r
-                del self.live[k]
+                self._retire(k, status, t)
         return B
 
     def idle(self) -> bool:
@@ -513,10 +536,7 @@ class DeviceServer(Server):
             if status is None and t - r.arrival > self.time_budget:
                 status = "budget"
             if status:
-                r.status, r.finished = status, t
-                self.done[k] = r
-                del self.live[k]
-                lv.release()
+                self._retire(k, status, t)
         if self._plan_keys is not None and any(k not in self.live for k in self._plan_keys):
             self._plan_keys = None          # re-plan next round (its instances' buffers may be freed)
             for h, _ in self._plans:

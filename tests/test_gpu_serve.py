@@ -94,3 +94,23 @@ def test_serve_compile_pool_same_results():
         finally:
             srv.close()
     assert out[0] == out[2]
+
+
+@pytest.mark.parametrize("cls", [Server, DeviceServer])
+def test_serve_preempts_the_widest(cls):
+    """With max_live running and preempt on, a narrower arrival replaces the widest live request
+    (status "preempted"); without preempt it waits."""
+    for preempt in (False, True):
+        srv = cls(batch=32, rel_gap=1e-12, time_budget=1e9, max_live=2, preempt=preempt)
+        srv.submit("w30", *_req(30, 30), arrival=0.0)
+        srv.submit("w20", *_req(20, 20), arrival=0.0)
+        srv.step(now=0.0)
+        assert set(srv.live) == {"w30", "w20"}
+        narrow = srv.submit("n6", *_req(6, 6), arrival=1.0)
+        srv.step(now=1.0)
+        if preempt:
+            assert srv.done["w30"].status == "preempted" and srv.preempted == 1
+            assert set(srv.live) == {"w20", "n6"} and narrow.admitted == 1.0
+        else:
+            assert "w30" in srv.live and narrow.status == "waiting" and srv.preempted == 0
+        srv.close()
