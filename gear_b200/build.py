@@ -8,7 +8,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(CSRC, "libgear_b200.so")
 SOURCES = ["gear_capi.cu"]
 DEPS = ["gear_capi.cu", "crown_kernel.cuh", "crown_simt.cuh", "gear_program.h", "bab_kernels.cuh",
-        "concretize_kernels.cuh", "dual_kernels.cuh", "fold_tc.cuh", "bab_queue.cuh"]
+        "concretize_kernels.cuh", "dual_kernels.cuh", "fold_tc.cuh", "split_tc.cuh", "bab_queue.cuh"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-fmad=false",
               "-std=c++17", "-shared", "-Xcompiler", "-fPIC"]
 

@@ -66,6 +66,15 @@ struct Work {
   // folds on the CUDA cores instead)
   const double* fold_ext;
   const int* fold_fail;
+  // the final pass's product through a dense node on the input on the tensor cores (OF_SPLIT op,
+  // tensor-core programs): the kernel writes that op's A rows densely, (B * S, split_k) doubles,
+  // and per row the pass's bias sum, charge sum and interval fallback, (B * S, 3), and per box
+  // its open flag; the GEMM and the concretisation run after it (split_tail_kernel). Null: the
+  // kernel takes the product itself.
+  double* split_v = nullptr;
+  double* split_rows = nullptr;
+  int* split_open = nullptr;
+  int split_k = 0;
 };
 
 // ------------------------------------------------------------------ small helpers
@@ -939,7 +948,9 @@ __device__ __forceinline__ void gemv_row(const double* V, const int32_t* vcols, 
 // IDX: also skip the loads of identity source / target lists and row pointers (OpFlag). Used
 // by the instances whose working set is in global memory; in the shared-memory instances the
 // extra live flags cost more in register spills than the loads they save (measured).
-template <int NT, bool WHOLE = true, bool IDX = false>
+// SPLIT: the tensor-core programs' instance, which can hand the final pass's product through a
+// dense node on the input (OF_SPLIT op) to the tensor cores (Work.split_v).
+template <int NT, bool WHOLE = true, bool IDX = false, bool SPLIT = false>
 __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops, const Work& wk, int op_lo_ = 0,
                          int op_hi_ = 1 << 30, int phase_ = 3) {
   // WHOLE: every phase and every op (compile-time constants for the fused kernels)
@@ -1209,6 +1220,15 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
               ctx.row(side, R_ERR)[s] += sm_ * fbias;
             }
           }
+          if (SPLIT && (oflags & OF_SPLIT) && wk.split_v) {
+            // the tensor cores take this row's product: its A row, dense over v's outputs
+            double* dst = wk.split_v + ((size_t)bx.b * S + s) * wk.split_k;
+            for (int j = eoff; j < wk.split_k; j += estep) dst[j] = 0.0;
+            if (block_rows) __syncthreads();
+            else __syncwarp();
+            for (int e = e0 + eoff; e < e1; e += estep) dst[vcols[e]] = V[e];
+            continue;
+          }
           if (e0 == e1) {
             if (zero_u) for (int j = eoff; j < urow; j += estep) Ur[j] = 0.0;
             continue;
@@ -1246,6 +1266,30 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
 #ifdef GEAR_STEP_PROFILE
   if (tid == 0) t_op = clock64();
 #endif
+  if (SPLIT && wk.split_v && pr[P_FINAL] != 0 && nop > 0 && (sops[(nop - 1) * OP_REC + O_SINGLE] & OF_SPLIT)) {
+    // the input's A comes from the tensor cores: hand each row's bias sum, charge sum and
+    // interval fallback (backward_bound.py:826) and the box's open flag to split_tail_kernel
+    for (int s = tid; s < S; s += NT) {
+      double fb = 0;
+      if (pr[P_INIT] == 0) {
+        fb = bx.lo[tnd[N_CUR] + s];
+      } else {
+        const int wt = tnd[N_W];
+        const double* Cb = wk.C + ((size_t)bx.b * S + s) * wt;
+        for (int c = 0; c < wt; ++c) {
+          const double cv = Cb[c];
+          fb += cv > 0 ? cv * bx.lo[tnd[N_CUR] + c] : (cv < 0 ? cv * bx.hi[tnd[N_CUR] + c] : 0.0);
+        }
+      }
+      double* r = wk.split_rows + ((size_t)bx.b * S + s) * 3;
+      r[0] = ctx.row(0, R_VAL)[s];
+      r[1] = ctx.row(0, R_ERR)[s];
+      r[2] = fb;
+    }
+    if (tid == 0) wk.split_open[bx.b] = bx.open ? 1 : 0;
+    __syncthreads();
+    return;
+  }
 
   // ---- concretisation at the input and outputs
   const bool fold = pr[P_NFOLD] != 0;
@@ -1489,7 +1533,7 @@ __device__ __forceinline__ void cta_step(const DevProgram& P, Box& bx, double* t
       break;
     }
     case ST_PASS: case ST_FINAL:
-      if (WHOLE) run_pass<NT, true, IDX>(bx, a, work, sops, wk);
+      if (WHOLE) run_pass<NT, true, IDX, FX>(bx, a, work, sops, wk);
       else run_pass<NT, false, IDX>(bx, a, work, sops, wk, op_lo, op_hi, phase);
       break;
     case ST_COMPARE: compare_node<NT>(bx, a, tmp_lo, tmp_hi, st[3] != 0); break;

@@ -9,17 +9,17 @@
 // products on low-precision units, in its fixed-point form):
 //
 //   every row of W and every box row of x0 / eps is scaled by a power of two 2^e with
-//   max |.| < 2^e and cut into DIGITS truncated base-128 digits, d_1..d_5 in [-127, 127]
-//   (|v| 2^-e = sum_i d_i 128^-i + rest, 0 <= rest < 128^-5, sign carried by every digit);
+//   max |.| < 2^e and cut into DIGITS (6) truncated base-128 digits, d_1..d_6 in [-127, 127]
+//   (|v| 2^-e = sum_i d_i 128^-i + rest, 0 <= rest < 128^-6, sign carried by every digit);
 //   the digit planes are int8 matrices and every digit product d_i e_j is formed exactly by
 //   tcgen05.mma.kind::i8 with int32 accumulation in TMEM. Products of equal level i + j share
-//   one accumulator (one scale 128^-(i+j)); levels 2..DIGITS+1 are kept (15 of the 25 digit
+//   one accumulator (one scale 128^-(i+j)); levels 2..DIGITS+1 are kept (21 of the 36 digit
 //   pairs), their int32 sums are combined in float64 and scaled by 2^(e_row + e_box).
 //
 // Rigorous enclosure. Per input k the dropped terms are the residual products and the digit
 // pairs beyond level DIGITS+1; with W^ = |W| 2^-e, X^ = |x| 2^-f (both < 1):
-//   |exact - kept| < 128^-5 (W^_k + X^_k) + 128^-6 sum_{i>=2} |d_i,k|,
-// and the float64 combination of the 5 level sums errs by at most 5 u sum_k X^_k. Summed over
+//   |exact - kept| < 128^-6 (W^_k + X^_k) + 128^-7 sum_{i>=2} |d_i,k|,
+// and the float64 combination of the 6 level sums errs by at most 5 u sum_k X^_k. Summed over
 // k, with the row and box sums taken in upward rounding, this gives E_c (centre) and E_r
 // (radius) in absolute terms. The radius handed to the CROWN kernel is r^ + E_r + E_c (upward
 // rounding), so the interval [c^ - r', c^ + r'] contains W x0 -/+ |W| eps: every bound built on
@@ -39,7 +39,7 @@
 namespace gear {
 namespace foldtc {
 
-constexpr int DIGITS = 5;                 // base-128 digits per operand (35 bits)
+constexpr int DIGITS = 6;                 // base-128 digits per operand (42 bits)
 constexpr int LEVELS = DIGITS;            // i + j = 2 .. DIGITS + 1
 constexpr int BM = 128;                   // boxes per tile (TMEM lanes)
 constexpr int BN = 64;                    // outputs per tile (TMEM columns per level)
@@ -50,7 +50,9 @@ constexpr int PLANE_A = BM * BK;          // bytes of one box digit plane per st
 constexpr int PLANE_B = BN * BK;          // bytes of one weight digit plane per stage
 constexpr int STAGE_BYTES = DIGITS * (PLANE_A + PLANE_B);
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;   // + 1 KB for aligning the ring
-constexpr uint32_t TMEM_COLS = 512;       // LEVELS * BN = 320 columns, allocated as a power of two
+constexpr uint32_t TMEM_COLS = 512;       // LEVELS * BN = 384 columns, allocated as a power of two
+static_assert(LEVELS * BN <= (int)TMEM_COLS, "level accumulators exceed the TMEM allocation");
+static_assert(SMEM_BYTES + 64 <= 232448, "the stage ring exceeds the opt-in shared memory of a CTA");
 constexpr int CORE_SBO = (BK / 16) * 128; // bytes between 8-row groups of a plane
 constexpr int CORE_LBO = 128;             // bytes between the two 16-byte K chunks of an MMA step
 // instruction descriptor: D int32, A and B signed int8, both K-major, N = BN, M = BM
@@ -88,6 +90,10 @@ struct BatchDigits {
   int64_t fold_w;
   int64_t B;
   int* status;           // set to 1 when a bounded wait expired
+  // 0: the fold (two products per tile). 1: one product, the rows of xc against W^T of a dense
+  // node (the final pass's A_v W, split_tc.cuh): fold[n] = the product, fold[w + n] its
+  // enclosure radius E_c (0 for an all-zero row, whose product is exact)
+  int gemv = 0;
 };
 
 // ------------------------------------------------------------------ digit split
@@ -221,6 +227,48 @@ __global__ void __launch_bounds__(NT) box_digits_kernel(const double* __restrict
   }
 }
 
+// One row m of V (M x K, row-major) -> signed digit planes and the row statistics (norm_c, ec;
+// open when an entry is not finite). Grid: m_pad rows.
+__global__ void __launch_bounds__(NT) row_digits_kernel(const double* __restrict__ V, int64_t M, int K, int k_pad,
+                                                        int8_t* xc, int64_t plane, BoxStat* st) {
+  __shared__ double redd[NT / 32];
+  __shared__ int redi[NT / 32];
+  const int64_t m = blockIdx.x;
+  const bool row = m < M;
+  double mc = 0;
+  int bad = 0;
+  if (row)
+    for (int k = threadIdx.x; k < K; k += NT) {
+      const double c = V[m * K + k];
+      bad |= !isfinite(c);
+      mc = fmax(mc, fabs(c));
+    }
+  mc = block_reduce(mc, [](double a, double c) { return fmax(a, c); }, redd);
+  bad = block_reduce(bad, [](int a, int c) { return a | c; }, redi);
+  const int ec = bad ? 0 : scale_exp(mc);
+  double sc = 0;
+  for (int k = threadIdx.x; k < k_pad; k += NT) {
+    const double c = (row && !bad && k < K) ? V[m * K + k] : 0.0;
+    int dc[DIGITS];
+    split_digits(c, ec, true, dc);
+#pragma unroll
+    for (int i = 0; i < DIGITS; ++i) xc[i * plane + m * k_pad + k] = (int8_t)dc[i];
+    sc = __dadd_ru(sc, ldexp(fabs(c), -ec));
+  }
+  sc = block_reduce(sc, [](double a, double c) { return __dadd_ru(a, c); }, redd);
+  if (threadIdx.x == 0 && row) {
+    BoxStat s;
+    s.norm_c = sc;
+    s.norm_r = 0;
+    s.xm_max = 0;
+    s.ec = ec;
+    s.er = 0;
+    s.open = bad;
+    s.pad = 0;
+    st[m] = s;
+  }
+}
+
 // ------------------------------------------------------------------ tcgen05 helpers
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -285,15 +333,17 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t (&v)[16]) {
 
 // |exact - kept| of one fold product over K inputs, relative to 2^(e_row + e_box), rounded up
 __device__ __forceinline__ double split_error(double wnorm, double xnorm, double wdelta) {
-  const double t1 = __dmul_ru(__dadd_ru(wnorm, xnorm), 0x1p-35);   // 128^-5 (sum W^ + sum X^)
-  const double t2 = __dmul_ru(wdelta, 0x1p-42);                     // 128^-6 sum |d_i>=2|
-  const double t3 = __dmul_ru(xnorm, 6.0 * 0x1p-53);                // float64 combination of the levels
+  constexpr double R_D = 1.0 / (double)(1ull << (7 * DIGITS));     // 128^-DIGITS, exact
+  const double t1 = __dmul_ru(__dadd_ru(wnorm, xnorm), R_D);        // 128^-D (sum W^ + sum X^)
+  const double t2 = __dmul_ru(wdelta, R_D / 128.0);                 // 128^-(D+1) sum |d_i>=2|
+  const double t3 = __dmul_ru(xnorm, (LEVELS + 1) * 0x1p-53);       // float64 combination of the levels
   return __dadd_ru(__dadd_ru(t1, t2), t3);
 }
 
 // ------------------------------------------------------------------ the GEMM
 // Grid: (n_pad / BN, b_pad / BM). Two products per tile: op 0 = signed W digits x centre digits
-// (c), op 1 = |W| digits x radius digits (r, then t from the row and box statistics).
+// (c), op 1 = |W| digits x radius digits (r, then t from the row and box statistics); with
+// bt.gemv only op 0, and its enclosure radius.
 __global__ void __launch_bounds__(NT, 1) fold_tc_kernel(NodeDigits nd, BatchDigits bt) {
   extern __shared__ uint8_t dyn_smem[];
   __shared__ __align__(8) uint64_t mbar[STAGES];
@@ -304,7 +354,7 @@ __global__ void __launch_bounds__(NT, 1) fold_tc_kernel(NodeDigits nd, BatchDigi
   const int n0 = blockIdx.x * BN;
   const int64_t m0 = (int64_t)blockIdx.y * BM;
   const int KB = nd.k_pad / BK;
-  const int T = 2 * KB;
+  const int T = bt.gemv ? KB : 2 * KB;
 
   if (tid == 0) {
     for (int s = 0; s < STAGES; ++s)
@@ -404,6 +454,8 @@ __global__ void __launch_bounds__(NT, 1) fold_tc_kernel(NodeDigits nd, BatchDigi
           const int en = nd.we[n];
           if (op == 0) {
             out[n] = ldexp(acc[c], en + bs.ec);
+            if (bt.gemv)
+              out[nd.w + n] = bs.norm_c == 0 ? 0.0 : ldexp(split_error(nd.wnorm[n], bs.norm_c, nd.wdelta[n]), en + bs.ec);
           } else {
             const double wn = nd.wnorm[n], wdl = nd.wdelta[n];
             const double e_c = ldexp(split_error(wn, bs.norm_c, wdl), en + bs.ec);

@@ -18,6 +18,7 @@
 #include "concretize_kernels.cuh"
 #include "dual_kernels.cuh"
 #include "fold_tc.cuh"
+#include "split_tc.cuh"
 #include "bab_queue.cuh"
 
 namespace {
@@ -57,6 +58,12 @@ struct gear_dag {
   void* tc_dev = nullptr;
   std::vector<gear::foldtc::NodeDigits> tc_nodes;
   int tc_k_pad = 0;
+  // the final pass's product through a dense node on the input on the tensor cores (OF_SPLIT
+  // op): digit planes of that node's W^T (n x w), in a device block of their own
+  bool split = false;
+  void* split_dev = nullptr;
+  gear::foldtc::NodeDigits split_nd{};
+  int split_k = 0;        // w: the node's outputs (the product's inner dimension)
 };
 
 namespace {
@@ -83,6 +90,80 @@ TcLayout tc_layout(const gear_dag* d, int64_t batch, int64_t base) {
   return L;
 }
 
+// Workspace of the tensor-core product of the final pass (after the fold's): the dense A rows
+// (M = B S rows of split_k), per row bias / charge / fallback, per box open flags, row
+// statistics, digit planes (m_pad x k_pad), the product with its radius (M x 2 n), a status flag.
+struct SplitLayout {
+  int64_t v, rows, open, stats, xc, prod, flag, total, m_pad, plane;
+};
+SplitLayout split_layout(const gear_dag* d, int64_t batch, int64_t base) {
+  using namespace gear::foldtc;
+  SplitLayout L{};
+  const int64_t M = batch * d->hdr[gear::H_S], n = d->hdr[gear::H_N];
+  L.m_pad = align_up(M, BM);
+  L.plane = L.m_pad * d->split_nd.k_pad;
+  int64_t o = align_up(base, kAlign);
+  L.v = o;     o = align_up(o + M * d->split_k * (int64_t)sizeof(double), kAlign);
+  L.rows = o;  o = align_up(o + M * 3 * (int64_t)sizeof(double), kAlign);
+  L.open = o;  o = align_up(o + batch * (int64_t)sizeof(int), kAlign);
+  L.stats = o; o = align_up(o + L.m_pad * (int64_t)sizeof(BoxStat), kAlign);
+  L.xc = o;    o = align_up(o + DIGITS * L.plane, kAlign);
+  L.prod = o;  o = align_up(o + M * 2 * n * (int64_t)sizeof(double), kAlign);
+  L.flag = o;  o = align_up(o + (int64_t)sizeof(int), kAlign);
+  L.total = o;
+  return L;
+}
+
+// The OF_SPLIT op of the final pass, if any: digit planes of its node's W^T (n rows of w).
+int split_prepare(gear_dag* d, const int32_t* nodes, const int32_t* ops) {
+  using namespace gear;
+  using namespace gear::foldtc;
+  if (!ops) return GEAR_OK;
+  const int nsteps = d->hdr[H_NSTEPS];
+  int fpass = -1;
+  for (int si = 0; si < nsteps; ++si)
+    if (d->steps[(size_t)si * STEP_REC] == ST_FINAL) fpass = d->steps[(size_t)si * STEP_REC + 1];
+  if (fpass < 0 || d->passes.empty()) return GEAR_OK;
+  const int32_t* pr = d->passes.data() + (size_t)fpass * PASS_REC;
+  if (pr[P_NOP] < 1 || pr[P_SIDES] != 1 || pr[P_XDENSE] == 0) return GEAR_OK;
+  const int32_t* op = ops + (size_t)(pr[P_OP0] + pr[P_NOP] - 1) * OP_REC;
+  if (!(op[O_SINGLE] & OF_SPLIT)) return GEAR_OK;
+  const int32_t* nd = nodes + (int64_t)op[O_V] * NODE_REC;
+  const int w = nd[N_W], n = nd[N_WIN];
+  if (nd[N_WT_OFF] < 0 || n != d->hdr[H_N] || w < 2 * BK) return GEAR_OK;
+  NodeDigits dg{};
+  dg.w = n;
+  dg.n_pad = (int)align_up(n, BN);
+  dg.k_pad = (int)align_up(w, BK);
+  if ((int64_t)DIGITS * dg.k_pad * 127 * 127 >= (int64_t)1 << 31) return GEAR_OK;
+  dg.plane = (int64_t)dg.n_pad * dg.k_pad;
+  dg.fold_off = 0;
+  const int64_t bytes = align_up(2 * DIGITS * dg.plane + (int64_t)dg.n_pad * (sizeof(int) + 2 * sizeof(double)) + 64,
+                                 kAlign);
+  cudaError_t e = cudaMalloc(&d->split_dev, bytes);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(final-pass product digits)");
+  int8_t* wd = (int8_t*)d->split_dev;
+  int8_t* wa = wd + DIGITS * dg.plane;
+  double* wnorm = (double*)align_up((int64_t)(wa + DIGITS * dg.plane), 8);
+  double* wdelta = wnorm + dg.n_pad;
+  int* we = (int*)(wdelta + dg.n_pad);
+  dg.wd = wd;
+  dg.wa = wa;
+  dg.we = we;
+  dg.wnorm = wnorm;
+  dg.wdelta = wdelta;
+  // W^T is (n x w) row-major in the program (the forward products' copy): its rows are the
+  // product's outputs, its columns the inner dimension
+  w_digits_kernel<<<dg.n_pad, NT>>>(d->P.dp + nd[N_WT_OFF], n, w, dg, wd, wa, we, wnorm, wdelta);
+  e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "final-pass product digits");
+  d->split_nd = dg;
+  d->split_k = w;
+  d->split = true;
+  return GEAR_OK;
+}
+
 // Digit planes of every dense node on the input (fold step of a box-per-CTA program), built once.
 int tc_prepare(gear_dag* d, const int32_t* nodes) {
   using namespace gear;
@@ -101,8 +182,8 @@ int tc_prepare(gear_dag* d, const int32_t* nodes) {
     p.n_pad = (int)align_up(p.w, BN);
     p.k_pad = (int)align_up(p.K, BK);
     p.woff = nd[N_W_OFF];
-    // int32 level sums: at most DIGITS - 1 pairs x k_pad x 127^2 must stay below 2^31
-    if ((int64_t)(DIGITS - 1) * p.k_pad * 127 * 127 >= (int64_t)1 << 31)
+    // int32 level sums: at most DIGITS pairs x k_pad x 127^2 must stay below 2^31
+    if ((int64_t)DIGITS * p.k_pad * 127 * 127 >= (int64_t)1 << 31)
       return fail(GEAR_E_INVALID, "gear_dag_create: %s", "tensor-core fold: input width beyond the int32 accumulator bound");
     if (d->tc_k_pad && d->tc_k_pad != p.k_pad)
       return fail(GEAR_E_INVALID, "gear_dag_create: %s", "tensor-core fold: dense nodes on the input of different widths");
@@ -344,8 +425,10 @@ extern "C" int gear_dag_create(const int32_t* header, int64_t header_len, const 
       return fail(GEAR_E_INVALID, "gear_dag_create: %s", "the tensor-core fold is for box-per-CTA programs");
     }
     int st = tc_prepare(d, nodes);
+    if (st == GEAR_OK) st = split_prepare(d, nodes, ops);
     if (st != GEAR_OK) {
       if (d->tc_dev) cudaFree(d->tc_dev);
+      if (d->split_dev) cudaFree(d->split_dev);
       cudaFree(d->dev);
       delete d;
       return st;
@@ -359,6 +442,7 @@ extern "C" int gear_dag_destroy(gear_dag* dag) {
   if (!dag) return GEAR_OK;
   if (dag->dev) cudaFree(dag->dev);
   if (dag->tc_dev) cudaFree(dag->tc_dev);
+  if (dag->split_dev) cudaFree(dag->split_dev);
   delete dag;
   return GEAR_OK;
 }
@@ -395,7 +479,8 @@ extern "C" int64_t gear_crown_workspace_bytes(const gear_dag* dag, int64_t batch
   if (!dag || batch < 0) return -1;
   const int64_t slots = slots_for(dag, batch) * dag->slot_doubles * (int64_t)sizeof(double);
   if (dag->tc_nodes.empty() || batch == 0) return slots;
-  return tc_layout(dag, batch, slots).total;
+  const int64_t tc = tc_layout(dag, batch, slots).total;
+  return dag->split ? split_layout(dag, batch, tc).total : tc;
 }
 
 static int crown_lower_impl(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
@@ -449,10 +534,54 @@ static int crown_lower_impl(const gear_dag* dag, const double* x_L, const double
     if (pre < 0) return pre;
     wk.fold_ext = (const double*)((char*)workspace + L.fold);
     wk.fold_fail = (const int*)((char*)workspace + L.flag);
+    if (dag->split && lA) {
+      const SplitLayout SL = split_layout(dag, batch, L.total);
+      char* ws = (char*)workspace;
+      wk.split_v = (double*)(ws + SL.v);
+      wk.split_rows = (double*)(ws + SL.rows);
+      wk.split_open = (int*)(ws + SL.open);
+      wk.split_k = dag->split_k;
+    }
   }
-  const int st = launch_crown(dag, wk, slots_for(dag, batch), (cudaStream_t)stream);
+  int st = launch_crown(dag, wk, slots_for(dag, batch), (cudaStream_t)stream);
   g_launches += pre;
-  return st;
+  if (st != GEAR_OK || !wk.split_v) return st;
+  // the final pass's product on the tensor cores, then its concretisation
+  using namespace gear::foldtc;
+  const SplitLayout SL = split_layout(dag, batch, tc_layout(dag, batch, slots_for(dag, batch) * dag->slot_doubles *
+                                                                            (int64_t)sizeof(double)).total);
+  char* ws = (char*)workspace;
+  cudaStream_t cs = (cudaStream_t)stream;
+  const int64_t M = batch * dag->hdr[gear::H_S];
+  const int n = dag->hdr[gear::H_N];
+  int* flag = (int*)(ws + SL.flag);
+  cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(int), cs);
+  if (e != cudaSuccess) return cuda_fail(e, "final-pass product status");
+  BoxStat* rst = (BoxStat*)(ws + SL.stats);
+  int8_t* xc = (int8_t*)(ws + SL.xc);
+  row_digits_kernel<<<(unsigned)SL.m_pad, NT, 0, cs>>>(wk.split_v, M, dag->split_k, dag->split_nd.k_pad, xc, SL.plane,
+                                                       rst);
+  BatchDigits bt;
+  bt.xc = xc;
+  bt.xr = xc;                 // unused: one product
+  bt.plane = SL.plane;
+  bt.st = rst;
+  bt.fold = (double*)(ws + SL.prod);
+  bt.fold_w = 2 * (int64_t)n;
+  bt.B = M;
+  bt.status = flag;
+  bt.gemv = 1;
+  dim3 grid((unsigned)(dag->split_nd.n_pad / BN), (unsigned)(SL.m_pad / BM));
+  fold_tc_kernel<<<grid, NT, SMEM_BYTES, cs>>>(dag->split_nd, bt);
+  int64_t tail = (M + 7) / 8;
+  const int64_t tail_max = (int64_t)dag->num_sms * 8;
+  if (tail > tail_max) tail = tail_max;
+  gear::split_tail_kernel<256><<<(unsigned)(tail < 1 ? 1 : tail), 256, 0, cs>>>(wk, dag->hdr[gear::H_S], n,
+                                                                             (const double*)(ws + SL.prod), rst, flag);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "final-pass product launch");
+  g_launches += 3;
+  return GEAR_OK;
 }
 
 extern "C" int gear_crown_fold_vectors(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,

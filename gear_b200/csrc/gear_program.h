@@ -35,8 +35,9 @@ enum OpField {
 };
 // bits of an op record's O_SINGLE field: every target pulls one source; the source list, the
 // target list, the target row pointers or v's row pointers are the identity (the kernel then
-// computes the index instead of loading it)
-enum OpFlag { OF_SINGLE = 1, OF_SRC_ID = 2, OF_TGT_ID = 4, OF_TPTR_ID = 8, OF_VRP_ID = 16 };
+// computes the index instead of loading it). OF_SPLIT: the final pass's product through a dense
+// node on the input, handed to the tensor cores when the launch provides the buffers for it.
+enum OpFlag { OF_SINGLE = 1, OF_SRC_ID = 2, OF_TGT_ID = 4, OF_TPTR_ID = 8, OF_VRP_ID = 16, OF_SPLIT = 32 };
 // buffer offset marker: the input's A of a final pass accumulates in the lA output (row s at s * n)
 constexpr int ROOT_IN_LA = -2;
 // rows with at most this many entries are handled by one thread, longer rows by a warp

@@ -62,7 +62,7 @@ OP_REC = 32
  O_TPTR, O_UK, O_TMAXROW, O_SHORT, O_NSHORT, O_LONG, O_NLONG, O_SINGLE) = range(32)
 ROW_THREAD_MAX = 16  # rows with at most this much work run on one thread, longer rows on a warp
 # bits of the op record's O_SINGLE field (OpFlag in gear_program.h)
-OF_SINGLE, OF_SRC_ID, OF_TGT_ID, OF_TPTR_ID, OF_VRP_ID = 1, 2, 4, 8, 16
+OF_SINGLE, OF_SRC_ID, OF_TGT_ID, OF_TPTR_ID, OF_VRP_ID, OF_SPLIT = 1, 2, 4, 8, 16, 32
 ROOT_IN_LA = -2     # buffer marker: the input's A of a final pass accumulates in the lA output
 
 PLANES_PER_ELEM = {"mul": 6, "sqr": 4, "exp": 4, "log": 4, "sin": 4, "cos": 4, "pow": 4}
@@ -145,6 +145,7 @@ class Program:
             raise ProgramError(f"unknown tie rule {tie_rule!r}")
         self.tie_rule = tie_rule
         self.fold_tc = bool(fold_tc) and mode == "cta"
+        self.split_op = -1          # node whose final-pass product runs on the tensor cores (_mark_split)
         if mode not in MODES:
             raise ProgramError(f"unknown execution mode {mode!r}")
         if cta_threads not in (64, 128, 256):
@@ -682,6 +683,8 @@ class Program:
                 self.op_recs.append(r)
             if last_use.get(v, -2) == i and v != 0 and bufoff.get(v, 0) >= 0:
                 release(v)
+        if self.fold_tc and pi.final and xdense and pi.sides == 1:
+            self._mark_split(op_begin)
         smem = top
         x_nnz = 0 if fold else nnz.get(0, 0)
         rec = np.full(PASS_REC, -1, dtype=np.int32)
@@ -718,6 +721,28 @@ class Program:
         pi.bufoff = bufoff
         pi.fold = fold
         pi.nnz = nnz
+
+    # smallest dense node (outputs) whose final-pass product goes to the tensor cores
+    SPLIT_MIN_WIDTH = 128
+
+    def _mark_split(self, op_begin):
+        """Flag (OF_SPLIT) the final pass's product through a dense node on the input for the
+        tensor cores: the pass's last op, the only one into the input, a Linear/MatMul step of
+        at least SPLIT_MIN_WIDTH outputs whose transposed weights the program holds. The kernel
+        then hands that product (A_v W over the whole batch) to a tcgen05 GEMM and the
+        concretisation to a kernel after it (gear_capi.cu)."""
+        ops = self.op_recs[op_begin:]
+        into_x = [r for r in ops if r[O_U] == 0]
+        if len(into_x) != 1 or ops[-1] is not into_x[0]:
+            return
+        r = into_x[0]
+        v = int(r[O_V])
+        nd = self.g[v]
+        if (r[O_DENSE] != 1 or r[O_FOLD] != 0 or r[O_UMERGE] != 0 or r[O_UK] > 1 or
+                nd.kind not in ("linear", "matmul") or v not in self.fold_off or nd.width < self.SPLIT_MIN_WIDTH):
+            return
+        r[O_SINGLE] = int(r[O_SINGLE]) | OF_SPLIT
+        self.split_op = v
 
     def _moves(self, n, slot, rowptr, cols, v, p):
         """Pull lists: for each target entry of input p, the source entries of v.
@@ -786,7 +811,7 @@ class Program:
 
 
 # ===================================================================== compile pools
-_KEEP = ("S", "n", "t", "mode", "cta_threads", "tie_rule", "fold_tc", "x_in_la", "return_a", "dense_c", "arena_w", "plane_w", "fold_w", "maxw",
+_KEEP = ("S", "n", "t", "mode", "cta_threads", "tie_rule", "fold_tc", "split_op", "x_in_la", "return_a", "dense_c", "arena_w", "plane_w", "fold_w", "maxw",
          "max_S", "max_smem", "smem_total", "pass_global", "simt_buf", "simt_rows", "sin_off", "work", "header",
          "node_arr", "step_arr", "pass_arr", "op_arr", "int_pool", "dbl_pool")
 

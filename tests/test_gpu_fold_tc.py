@@ -98,3 +98,44 @@ def test_tensor_core_fold_bounds_sound_on_sampled_points(workload):
         assert torch.all(lb[b] <= (y + slack).min(0).values)
         plane = pts @ lA[b].T + lbias[b]
         assert torch.all(plane <= y + slack + 1e-9 * torch.clamp(plane.abs(), min=1.0))
+
+
+@pytest.mark.parametrize("spec", [None, "two_rows"])
+def test_final_pass_product_on_tensor_cores(spec):
+    """dense_a_n2048's final pass ends with the product through its 1024 x 2048 node (A_v W): with the
+    tensor-core fold that product runs as one tcgen05 GEMM over the batch (split_tc.cuh). Its lA rows
+    agree with the float64 CUDA-core product to 1e-9 of the row's scale, lb and lbias to 1e-6
+    relative, a box with an infinite coordinate falls back to the same interval bound, and the
+    launch sequence is box digits, fold GEMM, CROWN kernel, row digits, product GEMM, tail."""
+    wl = "dense_a_n2048"
+    m = problems.make_instance(wl, 0)
+    lo, hi = _boxes(wl, 62, 8)
+    hi[5, 7] = float("inf")                          # an open box
+    g = graph.trace(m, lo[:2])
+    B = lo.shape[0]
+    xL, xU = lo.cuda(), hi.cuda()
+    kw = {}
+    C = None
+    if spec == "two_rows":
+        kw = dict(spec_rows=2, dense_c=True)
+        C = torch.tensor([[[1.0], [-1.0]]], dtype=torch.float64, device="cuda").expand(B, 2, 1).contiguous()
+    tc = CrownEngine(g, mode="cta", cta_threads=256, tie_rule="exact", fold_tc=True, **kw)
+    cc = CrownEngine(g, mode="cta", cta_threads=256, tie_rule="exact", **kw)
+    assert tc.prog.split_op >= 0 and cc.prog.split_op == -1
+    a = tc.lower(xL, xU, C)
+    launches = _lib.lib().gear_last_launch_count()
+    b = cc.lower(xL, xU, C)
+    torch.cuda.synchronize()
+    assert launches == 2 + len(tc.prog.fold_off) + 3
+    la, lb_ = a[0].cpu().numpy(), b[0].cpu().numpy()
+    fin = np.isfinite(lb_)
+    assert np.array_equal(fin, np.isfinite(la))
+    assert np.all(np.abs(la - lb_)[fin] <= 1e-6 * np.maximum(1.0, np.abs(lb_[fin])))
+    assert np.array_equal(la[5], lb_[5])             # the open box: the same interval fallback
+    Aa, Ab = a[1].cpu().numpy(), b[1].cpu().numpy()
+    scale = np.abs(Ab).max(axis=2, keepdims=True)
+    assert np.all(np.abs(Aa - Ab) <= 1e-9 * np.maximum(scale, 1e-300))
+    ba, bb = a[2].cpu().numpy(), b[2].cpu().numpy()
+    fb = np.isfinite(bb)
+    assert np.array_equal(fb, np.isfinite(ba))
+    assert np.all(np.abs(ba - bb)[fb] <= 1e-6 * np.maximum(1.0, np.abs(bb[fb])))

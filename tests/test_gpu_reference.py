@@ -9,10 +9,13 @@ relative change of the reference's own lb when its boxes grow by one ulp.
 * tie_rule "exact" on the GPU against the exact-tie reference run: every row, every fixture,
   every kernel variant, within 1e-5 relative (measured ~1e-11).
 * tie_rule "reference" (the default) against the plain reference run: within 1e-5 on every
-  row the reference itself determines to 1e-5 (lb_ulp_dev <= 1e-5). On the other rows the
-  reference's choice between two McCormick planes with equal box minima follows rounding noise
-  in its intermediate bounds (a one-ulp change of the box moves those rows by up to 4%), so
-  there the GPU bound is only required to be sound.
+  row the reference itself determines to 1e-5 (lb_ulp_dev <= 1e-5), for the float64 CUDA-core
+  variants. On the other rows the reference's choice between two McCormick planes with equal
+  box minima follows rounding noise in its intermediate bounds (a one-ulp change of the box
+  moves those rows by up to 4%), so there the GPU bound is only required to be sound. The
+  tensor-core fold moves intermediate bounds by up to its enclosure radius (~1e-10 relative),
+  far beyond the one-ulp perturbation that makes a row "determined", so its variant is held to
+  the exact-tie comparison (every row) and to soundness.
 * Soundness: 10^4 seeded points per box, 32 boxes each of quad_exp_n10, dense_q_n200 and
   dense_a_n2048, default tie rule: lb <= min f over the points, and lA x + lbias <= f(x) at
   every point (both up to 1e-9 relative for the rounding of the sampled forward pass)."""
@@ -55,7 +58,7 @@ def test_exact_ties_match_reference_every_row(case, mode, threads, tc):
 
 
 @pytest.mark.parametrize("case", cases())
-@pytest.mark.parametrize("mode,threads,tc", VARIANTS)
+@pytest.mark.parametrize("mode,threads,tc", [v for v in VARIANTS if not v[2]])
 def test_default_matches_reference_on_determined_rows(case, mode, threads, tc):
     m, g, d, _ = load(case)
     lb, lA, lbias = _run(g, d, mode, threads, tc, "reference")
