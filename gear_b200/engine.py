@@ -132,6 +132,24 @@ class CrownEngine:
             return self._dags[next(iter(self._dags))].name
         return None if v is None else self._dag(*v).name
 
+    def kernel_name(self, batch: int) -> Optional[str]:
+        """The CROWN kernel instance this batch size launches (crown_megakernel<threads, global
+        working set, tensor-core fold> or crown_simt_kernel)."""
+        v = self.variant(batch)
+        if v is None:
+            return None
+        if v == "simt":
+            return "crown_simt_kernel"
+        if self.mode == "fixed":
+            prog = self._fixed.prog
+        elif self.mode == "auto":
+            prog = self._dag(*self._choice[self._bucket(batch)]).prog
+        else:
+            prog = self._dags[next(iter(self._dags))].prog
+        gws = int(prog.pass_global > 0)
+        fx = int(int(prog.header[23]) != 0)
+        return f"crown_megakernel<{v[3:]}, {gws}, {fx}>"
+
     def freeze(self, x_L: torch.Tensor, x_U: torch.Tensor, C: Optional[torch.Tensor] = None):
         """Time the variants once on these boxes and use the fastest for every later batch size
         (a caller whose batches vary, like a branch-and-bound loop, pays the timing once)."""
