@@ -86,6 +86,13 @@ __device__ __forceinline__ double widen(double bound, double err, double sign) {
   return (isinf(err) && err > 0) ? sign * INFINITY : out;
 }
 __device__ __forceinline__ double finite_abs(double v) { return isfinite(v) ? fabs(v) : 0.0; }
+// whether tot = fl(old + add) rounded (TwoSum's error is nonzero) or is not finite: on an
+// unbounded entry only such a merge costs (_merge_charge, backward_bound.py:740-752)
+__device__ __forceinline__ bool merge_rounded(double old, double add, double tot) {
+  const double bv = tot - old;
+  const double e = (old - (tot - bv)) + (add - bv);
+  return !isfinite(tot) || e != 0.0;
+}
 __device__ __forceinline__ double gamma_k(double k) { return (k + 1.0) * UNIT * (1.0 + 1e-6); }
 // NaN-propagating min / max (torch.minimum / np.minimum semantics)
 __device__ __forceinline__ double pmax(double a, double b) { return (isnan(a) || a > b) ? a : (isnan(b) ? b : (a > b ? a : b)); }
@@ -108,6 +115,34 @@ __device__ void relax_sqr(double l, double u, double* p) {
   double lk = 2 * mid;
   double lb = -mid * lk + mid * mid;
   p[0] = lk; p[1] = lb; p[2] = uk; p[3] = ub;
+}
+
+// _stop_undefined_interval (backward_bound.py:249-292) for one element whose relaxation is
+// undefined (a non-finite input interval, log of an interval reaching 0): a coefficient that
+// selects an undefined side takes the node's own interval [lo_v, hi_v] as a constant plane (a
+// non-finite constant still discards the row). The square is convex with a tangent below
+// (require_finite_relaxation_bounds(convex_tangent_lower=True), operators/base.py:318-340): only
+// its upper side is undefined, its lower tangent is built on the substitute interval (the finite
+// endpoint, or 0 -/+ 1 where unbounded), unless the node's interval lies above the hull's lower
+// end, where the lower side stops too (backward_bound.py:384-392).
+__device__ __forceinline__ void undefined_stop(int kind, double l, double u, double lo_v, double hi_v, double* p) {
+  bool stop_lower = true;
+  if (kind == NK_SQR) {
+    const bool fl = isfinite(l), fu = isfinite(u);
+    const double lf = fl ? l : 0.0, uf = fu ? u : 0.0;
+    double q[4];
+    relax_sqr(fl ? l : fmin(uf, 0.0) - 1.0, fu ? u : fmax(lf, 0.0) + 1.0, q);
+    const double hull = u < 0 ? u * u : (l > 0 ? l * l : 0.0);
+    stop_lower = lo_v > hull;
+    p[0] = q[0];
+    p[1] = q[1];
+  }
+  if (stop_lower) {
+    p[0] = 0.0;
+    p[1] = lo_v;
+  }
+  p[2] = 0.0;
+  p[3] = hi_v;
 }
 
 __device__ void relax_exp(double l, double u, double* p) {
@@ -766,6 +801,15 @@ __device__ void relax_node(const Box& bx, int v) {
   int kind = nd[N_KIND], w = nd[N_W];
   double* pl = bx.planes + nd[N_PLANE];
   const double* T = P->dp + P->hdr[H_SINOFF];
+  // the undefined-side stop needs the node's own interval to be NaN-free and not inverted on
+  // every element (_stop_undefined_interval's precondition)
+  int ivbad = 0;
+  if (kind != NK_MUL)
+    for (int j = threadIdx.x; j < w; j += NT) {
+      const double lo_v = bx.lo[nd[N_CUR] + j], hi_v = bx.hi[nd[N_CUR] + j];
+      ivbad |= isnan(lo_v) || isnan(hi_v) || lo_v > hi_v;
+    }
+  const bool stop_ok = !__syncthreads_or(ivbad);
   for (int j = threadIdx.x; j < w; j += NT) {
     if (kind == NK_MUL) {
       const int32_t* a = node_rec(P, nd[N_IN0]);
@@ -792,9 +836,10 @@ __device__ void relax_node(const Box& bx, int v) {
       }
       bool bad = !(isfinite(l) && isfinite(u));
       if (kind == NK_LOG) bad = bad || !(l > 0);
-      if (kind == NK_POW) bad = bad || !(u >= 0 || (int)P->dp[nd[N_CVEC] + 1] != POW_FRAC);
-      if (bad) {
-        p[0] = p[1] = p[2] = p[3] = NAN;
+      const bool off = kind == NK_POW && !(u >= 0 || (int)P->dp[nd[N_CVEC] + 1] != POW_FRAC);
+      if (bad || off) {
+        if (stop_ok && !off) undefined_stop(kind, l, u, bx.lo[nd[N_CUR] + j], bx.hi[nd[N_CUR] + j], p);
+        else p[0] = p[1] = p[2] = p[3] = NAN;
       } else if (kind == NK_SQR) relax_sqr(l, u, p);
       else if (kind == NK_EXP) relax_exp(l, u, p);
       else if (kind == NK_LOG) relax_log(l, u, p);
@@ -1082,7 +1127,9 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
               double cv = cvec[c];
               if (inex[c] && a != 0.0) {
                 double m = m0[map0[c]];
-                sc += isinf(m) ? INFINITY : UNIT * (fabs(a * cv) * m);
+                // on an unbounded input only a product that rounded costs (the exact error of a
+                // cv, one FMA; _affine_backward_terms, backward_bound.py:611-640)
+                sc += isinf(m) ? (__fma_rn(a, cv, -(a * cv)) != 0.0 ? INFINITY : 0.0) : UNIT * (fabs(a * cv) * m);
               }
             } else if (kind == NK_LINEAR) {
               // bias of a folded Linear: A_v . b
@@ -1094,7 +1141,9 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
               double my = m1 ? m1[map1[c]] : fabs(cvec[c]);
               double e_ = rounding_error(mx + my, 2);
               double fa = finite_abs(a);
-              sc += fa > 0 ? (isinf(e_) ? INFINITY : fa * e_) : 0.0;
+              // an unbounded output entry adds nothing (its magnitude counts as 0, as in the
+              // deferred charge of _enclose_affine_backward, backward_bound.py:780-787)
+              sc += fa > 0 ? (isinf(e_) ? 0.0 : fa * e_) : 0.0;
               if (kind == NK_ADDC || kind == NK_SUBC || kind == NK_RSUBC) {
                 double cv = kind == NK_SUBC ? -cvec[c] : cvec[c];
                 sb += a * cv;
@@ -1156,11 +1205,13 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
             acc += na;
           }
           int ti = (IDX && (oflags & OF_TGT_ID)) ? k : tgt[k];
-          U[ti] += acc;
+          const double old = U[ti];
+          const double tot = old + acc;
+          U[ti] = tot;
           if (uk >= 2 && acc != 0.0) {
             int col = u_la ? ti - s * n : ucols[ti];
             double m = mu[col];
-            pmerge += isinf(m) ? INFINITY : fabs(acc) * m;
+            pmerge += isinf(m) ? (merge_rounded(old, acc, tot) ? INFINITY : 0.0) : fabs(acc) * m;
           }
         }
         if (uk >= 2) {

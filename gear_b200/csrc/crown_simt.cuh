@@ -142,6 +142,13 @@ __device__ void simt_relax_node(const SBox& bx, int v) {
   SView pl = bx.planes + nd[N_PLANE];
   const double* T = P->dp + P->hdr[H_SINOFF];
   const int32_t* a = node_rec(P, nd[N_IN0]);
+  // the undefined-side stop needs the node's own interval NaN-free and not inverted everywhere
+  bool stop_ok = true;
+  if (kind != NK_MUL)
+    for (int j = 0; j < w; ++j) {
+      const double lo_v = bx.lo[nd[N_CUR] + j], hi_v = bx.hi[nd[N_CUR] + j];
+      if (isnan(lo_v) || isnan(hi_v) || lo_v > hi_v) stop_ok = false;
+    }
   for (int j = 0; j < w; ++j) {
     double q[6];
     if (kind == NK_MUL) {
@@ -166,9 +173,10 @@ __device__ void simt_relax_node(const SBox& bx, int v) {
       }
       bool bad = !(isfinite(l) && isfinite(u));
       if (kind == NK_LOG) bad = bad || !(l > 0);
-      if (kind == NK_POW) bad = bad || !(u >= 0 || (int)P->dp[nd[N_CVEC] + 1] != POW_FRAC);
-      if (bad) {
-        q[0] = q[1] = q[2] = q[3] = NAN;
+      const bool off = kind == NK_POW && !(u >= 0 || (int)P->dp[nd[N_CVEC] + 1] != POW_FRAC);
+      if (bad || off) {
+        if (stop_ok && !off) undefined_stop(kind, l, u, bx.lo[nd[N_CUR] + j], bx.hi[nd[N_CUR] + j], q);
+        else q[0] = q[1] = q[2] = q[3] = NAN;
       } else if (kind == NK_SQR) relax_sqr(l, u, q);
       else if (kind == NK_EXP) relax_exp(l, u, q);
       else if (kind == NK_LOG) relax_log(l, u, q);
@@ -272,7 +280,7 @@ __device__ void simt_run_pass(const SBox& bx, int pid, const Work& wk, bool live
               double cv = __ldg(cvec + c);
               if (__ldg(inex + c) && a != 0.0) {
                 double m = m0[__ldg(map0 + c)];
-                sc += isinf(m) ? INFINITY : UNIT * (fabs(a * cv) * m);
+                sc += isinf(m) ? (__fma_rn(a, cv, -(a * cv)) != 0.0 ? INFINITY : 0.0) : UNIT * (fabs(a * cv) * m);
               }
             } else if (kind == NK_LINEAR) {
               double bb = __ldg(bvec + c);
@@ -283,7 +291,7 @@ __device__ void simt_run_pass(const SBox& bx, int pid, const Work& wk, bool live
               double my = two ? m1[__ldg(map1 + c)] : fabs(__ldg(cvec + c));
               double e_ = rounding_error(mx + my, 2);
               double fa = finite_abs(a);
-              sc += fa > 0 ? (isinf(e_) ? INFINITY : fa * e_) : 0.0;
+              sc += fa > 0 ? (isinf(e_) ? 0.0 : fa * e_) : 0.0;
               if (kind == NK_ADDC || kind == NK_SUBC || kind == NK_RSUBC) {
                 double cv = kind == NK_SUBC ? -__ldg(cvec + c) : __ldg(cvec + c);
                 sb += a * cv;
@@ -397,10 +405,12 @@ __device__ void simt_run_pass(const SBox& bx, int pid, const Work& wk, bool live
             acc += na;
           }
           int ti = __ldg(tgt + k);
-          U[ti] += acc;
+          const double old = U[ti];
+          const double tot = old + acc;
+          U[ti] = tot;
           if (uk >= 2 && acc != 0.0) {
             double m = mu[__ldg(ucols + ti)];
-            pmerge += isinf(m) ? INFINITY : fabs(acc) * m;
+            pmerge += isinf(m) ? (merge_rounded(old, acc, tot) ? INFINITY : 0.0) : fabs(acc) * m;
           }
         }
         if (uk >= 2) rerr[s] += gmerge * pmerge;

@@ -76,6 +76,27 @@ def gamma(k):
     return (k + 1) * U * (1 + 1e-6)
 
 
+def two_product_error(a, b):
+    """a * b - fl(a * b) exactly (Dekker's TwoProduct with Veltkamp's split); +inf where the product
+    is not finite or a split could overflow."""
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    with np.errstate(all="ignore"):
+        p = a * b
+        f = 2.0 ** 27 + 1.0
+
+        def split(x):
+            t = f * x
+            h = t - (t - x)
+            return h, x - h
+        ah, al = split(a)
+        bh, bl = split(b)
+        e = ((ah * bh - p) + ah * bl + al * bh) + al * bl
+    lim = np.finfo(np.float64).max / 2.0 ** 28
+    ok = np.isfinite(p) & (np.abs(a) < lim) & (np.abs(b) < lim)
+    return np.where(ok, e, np.inf)
+
+
 def abs_dot(absA, m):
     """<|A|, m> per row with 0 * inf = 0 and inf where |A| > 0 meets m = inf."""
     mf = np.where(np.isinf(m), 0.0, m)
@@ -645,6 +666,7 @@ class CrownOracle:
             bad = ~(np.isfinite(l) & np.isfinite(u))
             if k == "log":
                 bad = bad | ~(l > 0)
+            off = np.zeros_like(bad)
             if k == "pow":
                 # BoundPow.bound_backward raises the input node's stored upper bound to
                 # lower + 1e-8 before relaxing (s_shaped.py:791, :801); the change persists
@@ -675,9 +697,45 @@ class CrownOracle:
             else:
                 raise NotImplementedError(k)
             p = tuple(np.where(bad, 0.0, q) for q in p)
+            if bad.any():
+                p, bad = self._stop_undefined(v, k, l, u, p, bad, off)
             res = ("unary", p, bad)
         self.plane_cache[v] = res
         return res
+
+    def _stop_undefined(self, v, k, l, u, p, bad, off):
+        """_stop_undefined_interval (backward_bound.py:249-292) on the elements whose relaxation is
+        undefined (a non-finite input interval, log of an interval reaching 0): a coefficient that
+        selects an undefined side uses the node's own interval (_node_interval: its stored bounds,
+        else interval arithmetic from its inputs) as a constant plane, and only a non-finite
+        constant still discards the row. The square is convex with a tangent below
+        (require_finite_relaxation_bounds(convex_tangent_lower=True), operators/base.py:318-340):
+        only its upper side is undefined and the lower tangent is built on the substitute interval
+        (the finite endpoint, or 0 -/+ 1 when both are unbounded), unless the node's interval lies
+        above the hull's lower end (backward_bound.py:384-392), where the lower side stops too.
+        Off-domain pow elements (a fractional power entirely below 0) keep discarding their rows.
+        No element stops when some element's interval is NaN or inverted. Returns (planes, the
+        elements that still discard every row using them)."""
+        lo_v, hi_v = self.bounds[v] if v in self.bounds else self._interval(v, {})
+        if np.any(np.isnan(lo_v) | np.isnan(hi_v) | (lo_v > hi_v)):
+            return p, bad
+        lw, lb, uw, ub = p
+        stop = bad & ~off
+        no_lower, no_upper = stop.copy(), stop.copy()
+        if k == "sqr":
+            fl, fu = np.isfinite(l), np.isfinite(u)
+            lf, uf = np.where(fl, l, 0.0), np.where(fu, u, 0.0)
+            sl = np.where(fl, l, np.minimum(uf, 0.0) - 1.0)
+            su = np.where(fu, u, np.maximum(lf, 0.0) + 1.0)
+            tk, tb, _, _ = relax_sqr(sl, su)
+            with np.errstate(invalid="ignore"):
+                hull = np.where(u < 0, u * u, np.where(l > 0, l * l, 0.0))
+            no_lower = stop & (lo_v > hull)
+            tangent = stop & ~no_lower
+            lw, lb = np.where(tangent, tk, lw), np.where(tangent, tb, lb)
+        lw, lb = np.where(no_lower, 0.0, lw), np.where(no_lower, lo_v, lb)
+        uw, ub = np.where(no_upper, 0.0, uw), np.where(no_upper, hi_v, ub)
+        return (lw, lb, uw, ub), bad & off
 
     # -------------------------------------------------------------- backward
     def backward(self, t, C, lower=True, upper=True):
@@ -741,8 +799,19 @@ class CrownOracle:
                     old = A[p][side]
                     if K.get(p, 0) >= 2:
                         # merge rounding: the K_p additions into A_p err by at most
-                        # gamma(K_p) sum_i |contribution_i| (charged per contribution)
-                        err[side] += gamma(K[p]) * abs_dot(np.abs(new), self.magnitude(p)[None])
+                        # gamma(K_p) sum_i |contribution_i| (charged per contribution) on the
+                        # finite magnitudes; on an unbounded entry only an addition that rounded
+                        # costs (+inf), by TwoSum (_merge_charge, backward_bound.py:740-752)
+                        m = self.magnitude(p)
+                        unb = np.isinf(m)
+                        err[side] += gamma(K[p]) * abs_dot(np.abs(new), np.where(unb, 0.0, m)[None])
+                        if old is not None and unb.any():
+                            with np.errstate(all="ignore"):
+                                tot_ = old + new
+                                bv = tot_ - old
+                                e2 = (old - (tot_ - bv)) + (new - bv)
+                            e2 = np.where(np.isfinite(tot_), e2, np.inf)
+                            err[side] += np.where(((e2 != 0) & unb[None]).any(-1), np.inf, 0.0)
                     A[p][side] = new if old is None else old + new
         # concretisation at the input
         xL, xU = self.xL, self.xU
@@ -813,7 +882,13 @@ class CrownOracle:
                 outs[0][side] = scatter(newA, a["map0"], g[n.inputs[0]].width)
                 m_in = self.magnitude(n.inputs[0])[:, a["map0"]]
                 exact = (c == 0) | (np.abs(np.frexp(c)[0]) == 0.5)
-                err[side] += U * abs_dot(np.abs(np.where(exact, 0.0, newA)), m_in[None])
+                # on unbounded inputs only a product that rounded costs (+inf): the exact error of
+                # A * c by TwoProduct (_affine_backward_terms, backward_bound.py:611-640)
+                unb = np.isinf(m_in)
+                m_fin = np.where(unb, 0.0, m_in)
+                e = U * abs_dot(np.abs(np.where(exact, 0.0, newA)), m_fin[None])
+                rounded = (two_product_error(Am, np.broadcast_to(c, Am.shape)) != 0) & unb[None]
+                err[side] += np.where(rounded.any(-1), np.inf, e)
             elif k in ("add", "sub", "addc", "subc", "rsubc"):
                 mx = self.magnitude(n.inputs[0])[:, a["map0"]]
                 if k in ("add", "sub"):
@@ -829,8 +904,12 @@ class CrownOracle:
                     bias[side] += cb
                     bias_mag[side] += np.abs(Am) @ np.abs(cval)
                     my = np.abs(a["c"])[None, :]
-                # Add/Sub output rounding (_affine_output_error, interval_bound.py:71-77)
-                e = rounding_error(mx + my, 2)
+                # Add/Sub output rounding (_affine_output_error, interval_bound.py:71-77); an
+                # unbounded output entry adds nothing (its magnitude counts as 0, as in the
+                # deferred charge of _enclose_affine_backward, backward_bound.py:780-787)
+                with np.errstate(invalid="ignore"):
+                    e = rounding_error(mx + my, 2)
+                e = np.where(np.isinf(e), 0.0, e)
                 err[side] += abs_dot(finite_abs(Am), e[None])
             elif k == "neg":
                 outs[0][side] = -Am

@@ -121,6 +121,7 @@ def main(ref_root):
     cases.append(("sin_wide", 0, 12))
     cases.append(("pow_ops", 0, 12))
     cases.append(("pow_ops", 1, 12))
+    cases.append(("undef_ops", 0, 16))
     only = set(sys.argv[2:])
     if only:
         cases = [c for c in cases if c[0] in only]

@@ -1,6 +1,8 @@
 """Small test-only models that exercise operators the benchmark workloads do not
 (cos, neg, sub of two nodes, reverse-sub, nn.Linear with bias, slices, scalar gathers,
-division by a constant, concatenation of several rows)."""
+division by a constant, concatenation of several rows), and relaxations that are undefined on
+some boxes (log of an interval reaching 0, and sin / exp / square of the resulting unbounded
+interval)."""
 import torch
 
 F64 = torch.float64
@@ -82,4 +84,28 @@ class PowOps(torch.nn.Module):
         return torch.cat([t3 + t4, t15 - t05, (x[:, 5] ** 5).unsqueeze(1)], 1)
 
 
-MODELS = {"mixed_ops": (MixedOps, 6), "sin_wide": (SinWide, 5), "direct_ops": (DirectOps, 6), "pow_ops": (PowOps, 6)}
+class UndefOps(torch.nn.Module):
+    """log(x + 0.6) on x in [-1, 1]: its relaxation is undefined on boxes whose interval reaches
+    0 (the log's interval is then unbounded below), and so are those of sin, exp and the square of
+    that log. Rows: -c log(.) (upper side used), sin(log(.)), exp(log(.)) plus a bilinear, the
+    square of the log, and +c log(.) (lower side used)."""
+
+    def __init__(self, seed=13):
+        super().__init__()
+        g = torch.Generator().manual_seed(seed)
+        self.register_buffer("c", torch.rand(3, generator=g, dtype=F64) + 0.5)
+        self.register_buffer("d", torch.randn(3, generator=g, dtype=F64))
+        self.box = (-1.0, 1.0)
+
+    def forward(self, x):
+        L = torch.log(x[:, 0:3] + 0.6)
+        f0 = (-self.c * L).sum(1, keepdim=True) + (x[:, 3] * x[:, 4]).unsqueeze(1)
+        f1 = (self.d * torch.sin(L)).sum(1, keepdim=True) + x[:, 5:6]
+        f2 = torch.exp(L).sum(1, keepdim=True) - (x[:, 0] * x[:, 1]).unsqueeze(1)
+        f3 = (L ** 2).sum(1, keepdim=True)
+        f4 = (self.c * L).sum(1, keepdim=True)
+        return torch.cat([f0, f1, f2, f3, f4], 1)
+
+
+MODELS = {"mixed_ops": (MixedOps, 6), "sin_wide": (SinWide, 5), "direct_ops": (DirectOps, 6), "pow_ops": (PowOps, 6),
+          "undef_ops": (UndefOps, 6)}

@@ -15,6 +15,7 @@ import torch
 
 from gear_b200 import _lib, graph, problems
 from gear_b200.bab import BaB, GraphBaB
+from gear_b200.engine import CrownEngine
 
 pytestmark = pytest.mark.gpu
 
@@ -78,6 +79,24 @@ def test_graph_bab_runs_the_search_bab_runs(inst):
     assert b.status["bounded"] == a.stats.bounded
     assert Pa == Pb and Da == Db
     assert b.status["open"] == len(a.queue)
+
+
+def test_graph_bab_tensor_core_program():
+    """A tensor-core program (dense_a_n2048: the fold and the final pass's product on tcgen05) in
+    the device-queue step (gear_bab_step) runs the same search as the host-driven loop."""
+    m = problems.make_instance("dense_a_n2048", 0)
+    lo, hi = problems.root_box("dense_a_n2048")
+    g = graph.trace(m, lo.repeat(2, 1))
+    md = m.cuda()
+    eng = CrownEngine(g, mode="cta", cta_threads=256, fold_tc=True)
+    assert eng.prog.split_op >= 0
+    a = BaB(g, lo, hi, batch=64, model=md, device="cuda", engine=eng)
+    Pa, Da, _ = a.run(rel_gap=-1.0, max_iterations=6, time_limit=600)
+    b = GraphBaB(g, lo, hi, batch=64, model=md, device="cuda", engine=eng, chunk=2)
+    Pb, Db, _ = b.run(rel_gap=-1.0, max_iterations=6, time_limit=600)
+    assert b.status["iterations"] == a.stats.iterations == 6
+    assert b.status["bounded"] == a.stats.bounded
+    assert Pa == Pb and Da == Db
 
 
 def test_graph_bab_reaches_the_gap():
