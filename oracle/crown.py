@@ -605,6 +605,7 @@ class CrownOracle:
         check the restatement against recorded reference intermediates)."""
         self.tie_tol = tie_tol
         self.inject = inject or {}
+        self.cuts = None
         self.g = graph
         self.sin = SinRelax()
         self.consumers = graph.consumers()
@@ -830,11 +831,25 @@ class CrownOracle:
             # added to one error term (bias sums over visits + n terms, the box dot over n terms)
             f_bias = (max(nvisit, 1) + nin + 16) * EPS * 4
             f_box = (nin + 16) * EPS * 4
-            base = np.einsum("sbx,bx->sb", Ax, x0)
-            dev = np.einsum("sbx,bx->sb", np.abs(Ax), eps)
-            bmag = np.einsum("sbx,bx->sb", finite_abs(Ax), maxabs)
-            val = bias[side] + base
-            errt = err[side] + bias_mag[side] * f_bias + bmag * f_box + dev
+            if self.cuts is not None:
+                # concretisation over box ∩ cut rows (PerturbationLpNorm(constraints=...):
+                # constraints_solving, concretize_func.py:431-850, with its own rounding and the
+                # box bound as floor); an upper bound is minus the lower bound of -A
+                from .concretize import constrained_lower
+                cA, cb, cmax = self.cuts
+                with np.errstate(all="ignore"):
+                    obj = np.ascontiguousarray((Ax if side == 0 else -Ax).transpose(1, 0, 2))
+                    v = constrained_lower(xL, xU, obj, cA, cb, cmax).T
+                base = v if side == 0 else -v
+                dev = np.zeros_like(base)
+                val = bias[side] + base
+                errt = err[side] + bias_mag[side] * f_bias
+            else:
+                base = np.einsum("sbx,bx->sb", Ax, x0)
+                dev = np.einsum("sbx,bx->sb", np.abs(Ax), eps)
+                bmag = np.einsum("sbx,bx->sb", finite_abs(Ax), maxabs)
+                val = bias[side] + base
+                errt = err[side] + bias_mag[side] * f_bias + bmag * f_box + dev
             with np.errstate(invalid="ignore"):
                 tot = val + sign * (errt + (np.abs(val) + errt) * (17 * EPS * 4))
             bad = undef[side] | np.isnan(tot) | (tot == -sign * np.inf)
@@ -959,9 +974,14 @@ class CrownOracle:
         return outs
 
     # -------------------------------------------------------------- driver
-    def compute_bounds(self, xL, xU, C=None, bound_upper=False):
-        """lb (B, S), ub or None, A = (lA (B, S, n), lbias (B, S))."""
+    def compute_bounds(self, xL, xU, C=None, bound_upper=False, constraints=None, max_rows=0):
+        """lb (B, S), ub or None, A = (lA (B, S, n), lbias (B, S)). constraints = (A (B, K, n),
+        b (B, K)): rows A x + b <= 0 that every concretisation, intermediate passes included,
+        intersects with the box (PerturbationLpNorm(constraints=...)); max_rows caps the rows a
+        box sweeps (MAX_CONSTRAINT_ROWS)."""
         g = self.g
+        self.cuts = None if constraints is None else (np.asarray(constraints[0], np.float64),
+                                                      np.asarray(constraints[1], np.float64), int(max_rows))
         self.xL = np.asarray(xL, dtype=np.float64).reshape(xL.shape[0], -1)
         self.xU = np.asarray(xU, dtype=np.float64).reshape(xU.shape[0], -1)
         B = self.xL.shape[0]
