@@ -120,6 +120,10 @@ def lib():
         L.gear_crown_lower_plain.restype = i32
         L.gear_crown_lower_plain_ibp.argtypes = [vp, vp, vp, i64, vp, vp, vp, vp, vp, vp, i64, vp]
         L.gear_crown_lower_plain_ibp.restype = i32
+        L.gear_crown_cuts_workspace_bytes.argtypes = [vp, i64, i32]
+        L.gear_crown_cuts_workspace_bytes.restype = i64
+        L.gear_crown_lower_cuts.argtypes = [vp, vp, vp, i64, vp, vp, vp, i32, i32, vp, vp, vp, vp, vp, i64, vp]
+        L.gear_crown_lower_cuts.restype = i32
         L.gear_crown_multi_workspace_bytes.argtypes = [ctypes.POINTER(LowerArgs), i32]
         L.gear_crown_multi_workspace_bytes.restype = i64
         L.gear_crown_lower_multi.argtypes = [ctypes.POINTER(LowerArgs), i32, vp, i64, vp]
@@ -156,4 +160,5 @@ EXPORTED = ("gear_dag_create", "gear_dag_destroy", "gear_crown_workspace_bytes",
             "gear_crown_lower_plain_ibp", "gear_queue_create", "gear_queue_destroy", "gear_queue_push",
             "gear_queue_pop", "gear_queue_size", "gear_queue_counters", "gear_bab_step_workspace_bytes",
             "gear_bab_step", "gear_bab_step_bounded", "gear_crown_multi_prepare", "gear_crown_multi_launch",
-            "gear_crown_multi_plan_destroy", "gear_queue_reserve", "gear_queue_capacity")
+            "gear_crown_multi_plan_destroy", "gear_queue_reserve", "gear_queue_capacity",
+            "gear_crown_cuts_workspace_bytes", "gear_crown_lower_cuts")

@@ -170,13 +170,18 @@ class BaB:
                  engine_mode: str = "auto", cta_threads: int = 128,
                  sb_min_width_ratio: float = 1e-3, model: Optional[torch.nn.Module] = None,
                  constrained: bool = False, max_constraint_rows: int = 16, clip: bool = False,
-                 clip_iterations: int = 1, ibp_enhancement: bool = True, incumbent_every: int = 1):
+                 clip_iterations: int = 1, ibp_enhancement: bool = True, incumbent_every: int = 1,
+                 cuts_everywhere: bool = True):
         """constrained: the reference's complete clipping mode's constrained concretisation
         (batch_branch_and_bound.py:422-428): every child keeps its parent's planes
         lA_j x + lbias_j <= thr_j as cut rows, and the objective row of its CROWN bound is
         concretised over the box intersected with them (concretize_func.py:415-850, at most
         max_constraint_rows rows per box, the f3 setting's concretize_max_constraint_rows);
-        a box that the cuts exclude is pruned.
+        a box that the cuts exclude is pruned. cuts_everywhere (the reference's behaviour): the
+        cut rows enter every concretisation of the CROWN call, the intermediate passes'
+        included (PerturbationLpNorm(constraints=...), gear_crown_lower_cuts, the plain form's
+        launch sequence); False: the fused kernel bounds the box and only the objective row is
+        concretised again over box ∩ rows (looser, one fused launch).
         clip: domain clipping of the children with their parent's planes (clip.py:237-470,
         clip_iterations rounds); children that become empty are dropped.
         ibp_enhancement: every bound is the larger of CROWN's and the plain IBP bound of the
@@ -219,6 +224,12 @@ class BaB:
         self.clip_iterations = clip_iterations
         self.constrained = constrained
         self.max_constraint_rows = max_constraint_rows
+        self.cut_engine = None
+        if constrained and cuts_everywhere:
+            from .engine import CutEngine
+            self.cut_engine = CutEngine(graph, cta_threads=cta_threads,
+                                        tie_rule=getattr(self.engine, "tie_rule", "reference"),
+                                        max_rows=max_constraint_rows)
         self.queue = DomainQueue(self.n, self.S, 4 * batch, self.device, cuts=constrained)
         key = torch.full((1, self.S), -math.inf, dtype=torch.float64, device=self.device)
         cutA = torch.zeros(1, self.S * self.n, dtype=torch.float64, device=self.device) if constrained else None
@@ -393,7 +404,11 @@ class BaB:
         B = lo.shape[0]
         self.propose_incumbent((lo + hi) / 2)
         lb_ibp = torch.empty(B, self.S, dtype=torch.float64, device=self.device) if self.ibp_enhancement else None
-        lb, lA, lbias = self.engine.lower(lo, hi, lb_ibp=lb_ibp)
+        if self.cut_engine is not None:
+            lb, lA, lbias = self.cut_engine.lower(lo, hi, popped[4].reshape(B, self.S, self.n), popped[5],
+                                                  lb_ibp=lb_ibp)
+        else:
+            lb, lA, lbias = self.engine.lower(lo, hi, lb_ibp=lb_ibp)
         st = self.prune_branch(popped, lb, lA, lbias)
         K, inc = torch.cat([st["nk"].to(torch.float64), self._inc_dev]).tolist()   # the iteration's host read
         self.sync_incumbent(inc)

@@ -13,6 +13,11 @@ Mirrors ``auto_LiRPA``'s ``BoundedModule`` / ``BoundedTensor`` / ``PerturbationL
                                                'lbias': (B, S), 'ubias': None,
                                                'unstable_idx': None}
 
+A perturbation carrying linear rows, ``PerturbationLpNorm(x_L=lo, x_U=hi, constraints=(A, b))``
+with A (B, K, n) and b (B, K) meaning A x + b <= 0 (perturbations.py:129-199), makes every
+concretisation of the call, the intermediate passes' included, the constrained one
+(``engine.CutEngine``, C ABI ``gear_crown_lower_cuts``).
+
 Everything runs in float64 on the GPU through ``libgear_b200.so``; there is no CPU path.
 Only ``method='CROWN'`` (alias ``'backward'``) and ``'ibp'`` are accepted, with
 ``bound_upper=False`` for CROWN; other methods raise ``NotImplementedError`` as the
@@ -28,12 +33,10 @@ from . import graph as _graph
 from .engine import CrownEngine
 
 # The reference's GEAR configuration turns these on (exp_configs/NLP_solver/f3.yaml); the
-# engine always behaves as if the first three were set. For 'undefined_relaxation_interval' it
-# applies the coarser row rule only: a row that touches an element whose relaxation is undefined
-# (a non-finite input interval, log of a non-positive interval, an overflowing exp) is discarded
-# and falls back to the output interval, where the reference first tries to stop just the
-# coefficients selecting the undefined side (backward_bound.py:249-292). Both are sound; they
-# differ only on boxes with such elements.
+# engine always behaves as if they were set: an element whose relaxation is undefined (a
+# non-finite input interval, log of an interval reaching 0) stops at the node's own interval on
+# its undefined sides (backward_bound.py:249-292), and only a row with a non-finite contribution
+# is discarded to the output interval (backward_bound.py:826).
 HOT_PATH_BOUND_OPTS = {'fp_enclosure': {'affine_backward': True}, 'compare_crown_with_ibp_intermediate': True,
                        'undefined_relaxation_rows': True, 'undefined_relaxation_interval': True}
 
@@ -107,6 +110,18 @@ class BoundedModule:
             self._engines[key] = eng
         return eng
 
+    def _cut_engine(self, spec_rows: int, dense_c: bool):
+        key = ("cuts", spec_rows, dense_c)
+        eng = self._engines.get(key)
+        if eng is None:
+            from .engine import CutEngine
+            with torch.cuda.device(self.device):
+                eng = CutEngine(self.graph, spec_rows=spec_rows, dense_c=dense_c,
+                                cta_threads=int(self.bound_opts.get("gear_cta_threads", 128)),
+                                tie_rule=self.bound_opts.get("gear_tie_rule", "reference"))
+            self._engines[key] = eng
+        return eng
+
     # "auto" fold placement: dense nodes on the input with at least this many weights in all run
     # their fold products on the tensor cores (measured on B200: 30% off a dense_a_n2048 call with
     # 2 M weights, 4% on dense_q_n200's 50 k, where the fold is a small share of the kernel)
@@ -141,8 +156,7 @@ class BoundedModule:
         ptb = getattr(xt, "ptb", None)
         if ptb is None:
             raise ValueError("the input must be a BoundedTensor with a PerturbationLpNorm")
-        if getattr(ptb, "constraints", None) is not None:
-            raise NotImplementedError("constrained concretisation is not on the GPU path yet")
+        cons = getattr(ptb, "constraints", None)
         lo, hi = ptb.bounds(xt)
         B = lo.shape[0]
         lo = lo.reshape(B, -1).to(self.device, torch.float64)
@@ -156,14 +170,22 @@ class BoundedModule:
             raise NotImplementedError("the final pass computes lower bounds (bound_upper=False)")
         w = self.final_node_width()
         if C is None or self._is_identity(C.to(self.device)):
-            eng = self._engine(w, False)
+            eng = self._engine(w, False) if cons is None else None
             Cd = None
         else:
             C = C.to(self.device, torch.float64)
-            eng = self._engine(int(C.shape[1]), True)
+            eng = self._engine(int(C.shape[1]), True) if cons is None else None
             Cd = C
         want_A = bool(return_A)
-        lb, lA, lbias = eng.lower(lo, hi, Cd, return_A=want_A)
+        if cons is not None:
+            # every concretisation over box ∩ rows A x + b <= 0 (PerturbationLpNorm(constraints=
+            # (A, b)), perturbations.py:129-199; rows in standard form, (B, K, n) and (B, K))
+            ceng = self._cut_engine(int(C.shape[1]) if Cd is not None else w, Cd is not None)
+            cA, cb = cons
+            lb, lA, lbias = ceng.lower(lo, hi, cA.to(self.device, torch.float64), cb.to(self.device, torch.float64),
+                                       Cd, max_rows=int(self.bound_opts.get("concretize_max_constraint_rows", 0)))
+        else:
+            lb, lA, lbias = eng.lower(lo, hi, Cd, return_A=want_A)
         if not return_A:
             return lb, None
         A = {self.output_name[0]: {self.input_name[0]: {

@@ -75,6 +75,14 @@ struct Work {
   double* split_rows = nullptr;
   int* split_open = nullptr;
   int split_k = 0;
+  // concretisation over the box intersected with cut rows (the plain form's launches only):
+  // phase bit 4 of a pass writes its input A rows densely, (B, cut_h, n) with cut_h = sides * S
+  // (the upper side negated: its bound is minus the lower bound of -A); the constrained sweep
+  // turns them into lower bounds cut_v (B, cut_h), which the concretisation phase then takes in
+  // place of the box terms A x0 -/+ |A| eps and their rounding
+  double* cut_obj = nullptr;
+  const double* cut_v = nullptr;
+  int cut_h = 0;
 };
 
 // ------------------------------------------------------------------ small helpers
@@ -1313,6 +1321,34 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
     }
 #endif
   }
+  if (!WHOLE && (phase & 4)) {
+    // the pass's input A rows, dense and signed, for the constrained sweep (absent entries are
+    // zeros of the row's sign, as in the dense product -A of the reference)
+    const int H = wk.cut_h;
+    double* obj = wk.cut_obj + (size_t)bx.b * H * n;
+    for (int side = 0; side < sides; ++side) {
+      const double z = side == 0 ? 0.0 : -0.0;
+      for (int k = tid; k < S * n; k += NT) obj[(size_t)side * S * n + k] = z;
+    }
+    __syncthreads();
+    if (pr[P_NFOLD] == 0 && pr[P_XNNZ] > 0) {
+      const int32_t* xrp = P->ip + pr[P_XRP];
+      const int32_t* xcols = P->ip + pr[P_XCOLS];
+      for (int side = 0; side < sides; ++side) {
+        const double* V = ctx.vals(side, pr[P_XBUF]);
+        const double sg = side == 0 ? 1.0 : -1.0;
+        for (int s = warp; s < S; s += NWARP) {
+          const int e0 = xrp[s], e1 = xrp[s + 1];
+          for (int e = e0 + lane; e < e1; e += 32) {
+            const int c = xcols[e];
+            const double a = xdense ? V[(size_t)s * n + c] : V[e];
+            obj[((size_t)side * S + s) * n + c] = sg * a;
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
   if (!(phase & 2)) return;
 #ifdef GEAR_STEP_PROFILE
   if (tid == 0) t_op = clock64();
@@ -1347,7 +1383,19 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
   const int xnnz = pr[P_XNNZ];
   const int32_t* xrp = (!fold && xnnz > 0) ? P->ip + pr[P_XRP] : nullptr;
   const int32_t* xcols = (!fold && xnnz > 0) ? P->ip + pr[P_XCOLS] : nullptr;
-  if (xrp) {
+  if (!WHOLE && wk.cut_v) {
+    // concretisation over box ∩ cut rows: the sweep's lower bound of each signed row (its own
+    // rounding included) replaces the box terms; the root term of lbias is that bound
+    const double* cv = wk.cut_v + (size_t)bx.b * wk.cut_h;
+    for (int side = 0; side < sides; ++side) {
+      for (int s = tid; s < S; s += NT) {
+        const double v = cv[side * S + s];
+        const double base = side == 0 ? v : -v;
+        ctx.row(side, R_VAL)[s] += base;
+        if (ctx.nrows > R_ROOT) ctx.row(side, R_ROOT)[s] = base;
+      }
+    }
+  } else if (xrp) {
     const RowSplit rs = row_split<NT>(pr[P_XMAXROW]);
     for (int side = 0; side < sides; ++side) {
       const double* V = ctx.vals(side, pr[P_XBUF]);

@@ -5,6 +5,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <new>
@@ -709,9 +710,17 @@ extern "C" int64_t gear_crown_plain_workspace_bytes(const gear_dag* dag, int64_t
   return batch * dag->slot_doubles * (int64_t)sizeof(double);
 }
 
+// cut rows for gear_crown_lower_cuts: the constrained sweep's state and buffers (null: plain form)
+struct CutRun {
+  gear::cc::Work w;     // the sweep over the boxes and their rows (obj / lb / H set per pass)
+  double* obj;          // (B, sides * S, n) dense signed input rows of the running pass
+  double* v;            // (B, sides * S) their lower bounds over box ∩ rows
+  int warps;            // warps per CTA of the sweep
+  size_t smem;          // its dynamic shared memory
+};
 static int plain_impl(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch, const double* C,
                       double* lb, double* lA, double* lbias, double* lb_ibp, void* workspace, int64_t workspace_bytes,
-                      void* stream);
+                      void* stream, CutRun* cut = nullptr);
 
 extern "C" int gear_crown_lower_plain(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
                                       const double* C, double* lb, double* lA, double* lbias, void* workspace,
@@ -728,15 +737,15 @@ extern "C" int gear_crown_lower_plain_ibp(const gear_dag* dag, const double* x_L
 
 static int plain_impl(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch, const double* C,
                       double* lb, double* lA, double* lbias, double* lb_ibp, void* workspace, int64_t workspace_bytes,
-                      void* stream) {
-  g_launches = 0;
+                      void* stream, CutRun* cut) {
+  if (!cut) g_launches = 0;
   if (!dag || batch < 0) return fail(GEAR_E_INVALID, "gear_crown_lower_plain: %s", "bad arguments");
   if (!plain_ok(dag))
     return fail(GEAR_E_INVALID, "gear_crown_lower_plain: %s",
                 "needs a box-per-CTA program compiled with its pass working set in global memory");
   if (batch == 0) return GEAR_OK;
   if (!x_L || !x_U || !lb || !lA) return fail(GEAR_E_INVALID, "gear_crown_lower_plain: %s", "bad arguments");
-  if (!workspace || workspace_bytes < gear_crown_plain_workspace_bytes(dag, batch))
+  if (!cut && (!workspace || workspace_bytes < gear_crown_plain_workspace_bytes(dag, batch)))
     return fail(GEAR_E_WORKSPACE, "gear_crown_lower_plain: %s", "workspace too small");
   gear::Work wk;
   wk.xL = x_L;
@@ -781,12 +790,33 @@ static int plain_impl(const gear_dag* dag, const double* x_L, const double* x_U,
       const int nop = dag->passes[(size_t)a * gear::PASS_REC + gear::P_NOP];
       e = go(si, 0, 0, 1);
       for (int oi = 0; oi < nop && e == cudaSuccess; ++oi) e = go(si, oi, oi + 1, 0);
+      if (cut && e == cudaSuccess) {
+        // dense signed input rows -> the constrained sweep -> the concretisation reads its bounds
+        const int32_t* pr = dag->passes.data() + (size_t)a * gear::PASS_REC;
+        const int H = pr[gear::P_SIDES] * pr[gear::P_S];
+        wk.cut_obj = cut->obj;
+        wk.cut_h = H;
+        wk.cut_v = nullptr;
+        e = go(si, 0, 0, 4);
+        if (e == cudaSuccess) {
+          cut->w.obj = cut->obj;
+          cut->w.lb = cut->v;
+          cut->w.H = H;
+          const int64_t items = batch * H;
+          gear::cc::concretize_sweep_kernel<<<(unsigned)((items + cut->warps - 1) / cut->warps), 32 * cut->warps,
+                                              cut->smem, st>>>(cut->w);
+          ++launches;
+          e = cudaGetLastError();
+        }
+        wk.cut_v = cut->v;
+      }
       if (e == cudaSuccess) e = go(si, 0, 0, 2);
+      wk.cut_v = nullptr;
     } else {
       e = go(si, 0, 0, 0);
     }
   }
-  g_launches = launches;
+  g_launches += launches;
   return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "crown_plain_kernel launch");
 }
 
@@ -1672,6 +1702,104 @@ extern "C" int gear_constrained_lower(const double* x_L, const double* x_U, int6
   g_launches = launches + 1;
   e = cudaGetLastError();
   return e == cudaSuccess ? GEAR_OK : cuda_fail(e, "gear_constrained_lower");
+}
+
+// ------------------------------------------------------------------ CROWN under cut rows
+namespace {
+struct CutsLayout {
+  size_t plain, cc, obj, v, total;
+  CcLayout c;
+};
+int cuts_rows_max(const gear_dag* d) {
+  int h = 1;
+  for (int p = 0; p < d->hdr[gear::H_NPASSES]; ++p) {
+    const int32_t* pr = d->passes.data() + (size_t)p * gear::PASS_REC;
+    h = std::max(h, pr[gear::P_SIDES] * pr[gear::P_S]);
+  }
+  return h;
+}
+bool cuts_ok(const gear_dag* d) {
+  if (!plain_ok(d)) return false;
+  for (int p = 0; p < d->hdr[gear::H_NPASSES]; ++p)
+    if (d->passes[(size_t)p * gear::PASS_REC + gear::P_NFOLD] != 0) return false;
+  return true;
+}
+CutsLayout cuts_layout(const gear_dag* d, int64_t batch, int K) {
+  CutsLayout L;
+  size_t o = 0;
+  auto take = [&](size_t bytes) { size_t at = o; o += (bytes + 255) / 256 * 256; return at; };
+  const int H = cuts_rows_max(d), n = d->hdr[gear::H_N];
+  L.plain = take((size_t)batch * d->slot_doubles * sizeof(double));
+  L.c = cc_layout(batch, K);
+  L.cc = take(L.c.total);
+  L.obj = take((size_t)batch * H * n * sizeof(double));
+  L.v = take((size_t)batch * H * sizeof(double));
+  L.total = o;
+  return L;
+}
+}  // namespace
+
+extern "C" int64_t gear_crown_cuts_workspace_bytes(const gear_dag* dag, int64_t batch, int K) {
+  if (!cuts_ok(dag) || batch < 0 || K < 0) return -1;
+  return (int64_t)cuts_layout(dag, batch, K).total;
+}
+
+extern "C" int gear_crown_lower_cuts(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
+                                     const double* C, const double* cut_A, const double* cut_b, int K, int max_rows,
+                                     double* lb, double* lA, double* lbias, double* lb_ibp, void* workspace,
+                                     int64_t workspace_bytes, void* stream) {
+  g_launches = 0;
+  if (!dag || batch < 0 || K < 0 || max_rows < 0)
+    return fail(GEAR_E_INVALID, "gear_crown_lower_cuts: %s", "bad arguments");
+  if (!cuts_ok(dag))
+    return fail(GEAR_E_INVALID, "gear_crown_lower_cuts: %s",
+                "needs a box-per-CTA program compiled for cut rows (working set in global memory, no folded passes)");
+  if (batch == 0) return GEAR_OK;
+  if (!x_L || !x_U || !lb || !lA || (K > 0 && (!cut_A || !cut_b)))
+    return fail(GEAR_E_INVALID, "gear_crown_lower_cuts: %s", "bad arguments");
+  const int n = dag->hdr[gear::H_N];
+  const CutsLayout L = cuts_layout(dag, batch, K);
+  if (!workspace || workspace_bytes < (int64_t)L.total)
+    return fail(GEAR_E_WORKSPACE, "gear_crown_lower_cuts: %s", "workspace smaller than gear_crown_cuts_workspace_bytes");
+  const size_t per = gear::cc::sweep_smem_per_warp(n, K);
+  if (per > (size_t)(227 << 10))
+    return fail(GEAR_E_INVALID, "gear_crown_lower_cuts: %s", "too many variables or rows for one warp's shared memory");
+  int warps = (int)((size_t)(160 << 10) / per);
+  warps = std::max(1, std::min(warps, 4));
+  cudaStream_t st = (cudaStream_t)stream;
+  char* ws = (char*)workspace;
+  char* cc = ws + L.cc;
+  CutRun cut;
+  cut.w.xL = x_L; cut.w.xU = x_U; cut.w.A = cut_A; cut.w.b = cut_b;
+  cut.w.d = (double*)(cc + L.c.d);
+  cut.w.score = (double*)(cc + L.c.score);
+  cut.w.infeasible = (int*)(cc + L.c.infeasible);
+  cut.w.uncovered = (int*)(cc + L.c.uncovered);
+  cut.w.nkeep = (int*)(cc + L.c.nkeep);
+  cut.w.glob = (int*)(cc + L.c.glob);
+  cut.w.infeasible_out = nullptr;
+  cut.w.B = batch; cut.w.X = n; cut.w.K = K; cut.w.max_rows = max_rows;
+  cut.w.obj = nullptr; cut.w.lb = nullptr; cut.w.H = 1;
+  cut.obj = (double*)(ws + L.obj);
+  cut.v = (double*)(ws + L.v);
+  cut.warps = warps;
+  cut.smem = per * warps;
+  // the per-box counters and flags start at zero on every call
+  cudaError_t e = cudaMemsetAsync(cc + L.c.infeasible, 0, L.c.total - L.c.infeasible, st);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+  e = cudaFuncSetAttribute(gear::cc::concretize_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cut.smem);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute");
+  if (K > 0) {
+    // rows: infeasibility / cover tests, centred offsets and worst-case values, once per call
+    const int64_t rows = batch * K;
+    gear::cc::concretize_rows_kernel<<<(unsigned)((rows + 7) / 8), 256, 0, st>>>(cut.w);
+    gear::cc::concretize_boxes_kernel<<<(unsigned)((batch + 255) / 256), 256, 0, st>>>(cut.w);
+    g_launches = 2;
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "gear_crown_lower_cuts rows");
+  }
+  return plain_impl(dag, x_L, x_U, batch, C, lb, lA, lbias, lb_ibp, ws + L.plain, (int64_t)(L.total - L.plain),
+                    stream, &cut);
 }
 
 #ifdef GEAR_STEP_PROFILE

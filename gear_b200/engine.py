@@ -517,6 +517,72 @@ class PlainEngine:
         return out
 
 
+class CutEngine:
+    """CROWN bounds with every concretisation over the box intersected with cut rows
+    (gear_crown_lower_cuts; the reference's compute_bounds with PerturbationLpNorm(x_L, x_U,
+    constraints=(A, b)), auto_LiRPA/bound_general.py:1275): each intermediate pass and the final
+    pass bound their rows by the constrained dual sweep (concretize_func.py:431-850). Runs the
+    plain form's launch sequence on a program compiled for cut rows (no folded passes, pass
+    working set in global memory), plus a dense-row launch and a sweep per pass."""
+
+    def __init__(self, graph: Graph, spec_rows: Optional[int] = None, dense_c: bool = False, cta_threads: int = 128,
+                 tie_rule: str = "reference", max_rows: int = 0):
+        if not torch.cuda.is_available():
+            raise _lib.GearError("gear_b200 needs a CUDA device (no CPU fallback)")
+        self.dag = _Dag.from_program(Program(graph, spec_rows=spec_rows, dense_c=dense_c, mode="cta",
+                                             cta_threads=cta_threads, smem_limit=0, tie_rule=tie_rule, cuts=True))
+        self.prog = self.dag.prog
+        self.n, self.S = self.prog.n, self.prog.S
+        self.max_rows = int(max_rows)
+        self._ws = None
+        self.launches = 0
+
+    def lower(self, x_L: torch.Tensor, x_U: torch.Tensor, cut_A: Optional[torch.Tensor], cut_b: Optional[torch.Tensor],
+              C: Optional[torch.Tensor] = None, out=None, lb_ibp: Optional[torch.Tensor] = None,
+              max_rows: Optional[int] = None):
+        """lb (B, S), lA (B, S, n), lbias (B, S) under the rows cut_A (B, K, n) x + cut_b (B, K) <= 0
+        (K may be 0 or cut_A None: the box bound with the sweep's rounding)."""
+        B = x_L.shape[0]
+        dev = x_L.device
+        if dev.type != "cuda":
+            raise _lib.GearError("inputs must be CUDA tensors")
+        x_L = x_L.reshape(B, self.n).to(torch.float64).contiguous()
+        x_U = x_U.reshape(B, self.n).to(torch.float64).contiguous()
+        if cut_A is None:
+            K = 0
+            cA = cb = None
+        else:
+            cA = cut_A.reshape(B, -1, self.n).to(dev, torch.float64).contiguous()
+            K = int(cA.shape[1])
+            cb = cut_b.reshape(B, K).to(dev, torch.float64).contiguous()
+        if C is not None:
+            C = C.to(dev, torch.float64).contiguous()
+        if out is None:
+            out = (torch.empty(B, self.S, dtype=torch.float64, device=dev),
+                   torch.empty(B, self.S, self.n, dtype=torch.float64, device=dev),
+                   torch.empty(B, self.S, dtype=torch.float64, device=dev))
+        if B == 0:
+            return out
+        lb, lA, lbias = out
+        L = _lib.lib()
+        nbytes = int(L.gear_crown_cuts_workspace_bytes(self.dag.handle, B, K))
+        if nbytes < 0:
+            raise _lib.GearError("gear_crown_cuts_workspace_bytes: program not compiled for cut rows")
+        if self._ws is None or self._ws.numel() < nbytes or self._ws.device != dev:
+            self._ws = None
+            self._ws = torch.empty(max(nbytes, 8), dtype=torch.uint8, device=dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        mr = self.max_rows if max_rows is None else int(max_rows)
+        _lib.check(L.gear_crown_lower_cuts(self.dag.handle, x_L.data_ptr(), x_U.data_ptr(), B,
+                                           C.data_ptr() if C is not None else None,
+                                           cA.data_ptr() if K else None, cb.data_ptr() if K else None, K, mr,
+                                           lb.data_ptr(), lA.data_ptr(), lbias.data_ptr(),
+                                           lb_ibp.data_ptr() if lb_ibp is not None else None,
+                                           self._ws.data_ptr(), self._ws.numel(), stream), "gear_crown_lower_cuts")
+        self.launches = int(L.gear_last_launch_count())
+        return out
+
+
 class PlainMultiEngine:
     """The plain GPU form of many instances (the denominator of the uneven batch): each instance
     bounded alone by its own PlainEngine, one instance after another, one kernel launch per

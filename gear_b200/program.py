@@ -127,7 +127,8 @@ class Program:
 
     def __init__(self, graph: Graph, spec_rows: Optional[int] = None, dense_c: bool = False,
                  return_a: bool = True, smem_limit: int = 232448, mode: str = "cta",
-                 cta_threads: int = 128, tie_rule: str = "reference", fold_tc: bool = False):
+                 cta_threads: int = 128, tie_rule: str = "reference", fold_tc: bool = False,
+                 cuts: bool = False):
         """mode: "cta" runs one box per CTA with the pass working set in shared memory, and the
         final pass accumulates the input's A directly in the lA output; "simt" runs one box per
         thread with every per-box array box-interleaved in global scratch, and writes lA from the
@@ -140,11 +141,16 @@ class Program:
         bounds), "exact" picks plane 1, the exact-arithmetic outcome.
         fold_tc: compute the fold vectors of the dense nodes on the input (W x0, |W| eps) for the
         whole batch on the tensor cores before the CROWN kernel (int8 digit slicing with a rigorous
-        error term; box-per-CTA programs with such nodes only, otherwise ignored)."""
+        error term; box-per-CTA programs with such nodes only, otherwise ignored).
+        cuts: compile for concretisation over the box intersected with cut rows
+        (gear_crown_lower_cuts): no pass folds its input rows into per-box vectors (the
+        constrained sweep needs every input A row), and with smem_limit=0 the program runs in
+        the plain form's launch sequence."""
         if tie_rule not in TIE_RULES:
             raise ProgramError(f"unknown tie rule {tie_rule!r}")
         self.tie_rule = tie_rule
-        self.fold_tc = bool(fold_tc) and mode == "cta"
+        self.cuts = bool(cuts)
+        self.fold_tc = bool(fold_tc) and mode == "cta" and not self.cuts
         self.split_op = -1          # node whose final-pass product runs on the tensor cores (_mark_split)
         if mode not in MODES:
             raise ProgramError(f"unknown execution mode {mode!r}")
@@ -531,7 +537,7 @@ class Program:
         # fold decision: root contributions only from linear/matmul-on-input ops with
         # at most one entry per row, in a non-final pass
         contributors = [v for v in pi.order if 0 in g[v].inputs and v in pats]
-        fold = (not pi.final and len(contributors) == 1 and
+        fold = (not pi.final and not self.cuts and len(contributors) == 1 and
                 all(g[v].kind in ("linear", "matmul") and v in self.fold_off and
                     np.diff(rowptr[v]).max(initial=0) <= 1 for v in contributors))
         # liveness-based buffer allocation (doubles per side)
@@ -811,7 +817,7 @@ class Program:
 
 
 # ===================================================================== compile pools
-_KEEP = ("S", "n", "t", "mode", "cta_threads", "tie_rule", "fold_tc", "split_op", "x_in_la", "return_a", "dense_c", "arena_w", "plane_w", "fold_w", "maxw",
+_KEEP = ("S", "n", "t", "mode", "cta_threads", "tie_rule", "cuts", "fold_tc", "split_op", "x_in_la", "return_a", "dense_c", "arena_w", "plane_w", "fold_w", "maxw",
          "max_S", "max_smem", "smem_total", "pass_global", "simt_buf", "simt_rows", "sin_off", "work", "header",
          "node_arr", "step_arr", "pass_arr", "op_arr", "int_pool", "dbl_pool")
 

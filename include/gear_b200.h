@@ -304,6 +304,29 @@ int gear_crown_lower_plain_ibp(const gear_dag* dag, const double* x_L, const dou
                                const double* C, double* lb, double* lA, double* lbias, double* lb_ibp,
                                void* workspace, int64_t workspace_bytes, void* stream);
 
+/* ---------------------------------------------------------------- CROWN under cut rows
+ * Replaces BoundedModule.compute_bounds(x=(BoundedTensor(x0, PerturbationLpNorm(x_L, x_U,
+ * constraints=(A, b))),), C, method='CROWN') (solver/auto_LiRPA/bound_general.py:1275 with
+ * perturbations.py:129 carrying the rows), as the input-split BaB's constrained mode calls it
+ * (complete_verifier/input_split/batch_branch_and_bound.py:422-428): EVERY concretisation of the
+ * call -- each intermediate pass (both sides) and the final pass -- bounds its rows over the box
+ * [x_L, x_U] intersected with the box's rows cut_A (batch, K, n) x + cut_b (batch, K) <= 0, by the
+ * sequential dual sweep of gear_constrained_lower (constraints_solving, concretize_func.py:431-850;
+ * an upper bound is minus the sweep's lower bound of -A), in place of the box terms. lb, lA, lbias
+ * (and lb_ibp when non-NULL, as gear_crown_lower_plain_ibp) as gear_crown_lower. A box its rows
+ * exclude gets bounds that only say so through the concretisations (+inf lower rows are discarded
+ * to the interval fallback); callers that prune on infeasibility test it with
+ * gear_constrained_lower. The DAG must be compiled for cut rows (gear_b200/program.py
+ * Program(..., cuts=True, smem_limit=0): box per CTA, pass working set in global memory, no
+ * folded passes). Runs in the plain form's launch sequence (one launch per step / op) plus, per
+ * pass, one launch writing the dense rows and one sweep. K may be 0 (the reference's box bound
+ * with its rounding). n and K are bounded by one warp's shared memory (n <= ~2000). */
+int64_t gear_crown_cuts_workspace_bytes(const gear_dag* dag, int64_t batch, int K);
+int gear_crown_lower_cuts(const gear_dag* dag, const double* x_L, const double* x_U, int64_t batch,
+                          const double* C, const double* cut_A, const double* cut_b, int K, int max_rows,
+                          double* lb, double* lA, double* lbias, double* lb_ibp, void* workspace,
+                          int64_t workspace_bytes, void* stream);
+
 /* ---------------------------------------------------------------- many instances, one launch
  * One instance of a multi-instance CROWN call: the arguments gear_crown_lower takes for one
  * DAG (same shapes and meaning; batch may be 0). The reference bounds each instance with its own

@@ -77,3 +77,6 @@ def test_multi_and_plain_sizes_reject_bad_arguments(lib):
     lib.gear_crown_plain_workspace_bytes.restype = ctypes.c_int64
     lib.gear_crown_plain_workspace_bytes.argtypes = [ctypes.c_void_p, ctypes.c_int64]
     assert lib.gear_crown_plain_workspace_bytes(None, 1) == -1
+    lib.gear_crown_cuts_workspace_bytes.restype = ctypes.c_int64
+    lib.gear_crown_cuts_workspace_bytes.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32]
+    assert lib.gear_crown_cuts_workspace_bytes(None, 1, 4) == -1

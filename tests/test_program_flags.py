@@ -57,3 +57,18 @@ def test_pass_working_set_moves_to_global_memory():
     assert b.smem_total < a.smem_total
     for f in ("node_arr", "step_arr", "pass_arr", "op_arr", "int_pool", "dbl_pool"):
         assert np.array_equal(getattr(a, f), getattr(b, f))
+
+
+def test_cut_programs_fold_no_pass():
+    """Program(cuts=True): the constrained sweep needs every input A row, so no pass folds its
+    rows into the per-box fold vectors (dense_q_n200 folds its Linear-on-input passes otherwise);
+    the fold vectors themselves stay for the IBP steps."""
+    from gear_b200.program import P_NFOLD
+    m = problems.make_instance("dense_q_n200", 0)
+    lo, hi = problems.make_boxes("dense_q_n200", 2, 0)
+    g = graph.trace(m, lo)
+    plain = Program(g, mode="cta", smem_limit=0)
+    cut = Program(g, mode="cta", smem_limit=0, cuts=True)
+    assert any(int(r[P_NFOLD]) for r in plain.pass_arr.reshape(-1, PASS_REC))
+    assert not any(int(r[P_NFOLD]) for r in cut.pass_arr.reshape(-1, PASS_REC))
+    assert cut.fold_w == plain.fold_w > 0 and cut.pass_global > 0
