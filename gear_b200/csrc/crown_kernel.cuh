@@ -1229,16 +1229,88 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
       }
     };
 
+    // an entry-wise op (OF_FUSED, every row short): one sweep over the row's entries takes each
+    // entry's bias terms and its move (u's entry e <- v's entry e), in the order and with the
+    // arithmetic of row_body's two sweeps, so the results are the same bits; u's row needs no
+    // clearing (a fresh row holds exactly the moved entries)
+    auto fused_row = [&](int s) {
+      const bool vid = (oflags & OF_VRP_ID) != 0;
+      const int e0 = vid ? s : vrp[s], e1 = vid ? s + 1 : vrp[s + 1];
+      if (e0 == e1) return;
+      for (int side = 0; side < sides; ++side) {
+        const double* V = ctx.vals(side, op[O_VBUF]);
+        double* U = ctx.vals(side, op[O_UBUF]);
+        double sb = 0, sm_ = 0, sc = 0, pmerge = 0;
+        int und_ = 0;
+        for (int e = e0; e < e1; ++e) {
+          const double a = V[e];
+          const int c = __ldg(vcols + e);
+          double na;
+          if (relax || kind == NK_MUL) {
+            const double* p = pl + ppe * c;
+            double bt;
+            na = elem_coef(kind, slot, side, a, p, 0.0, &bt);
+            if (need_a) {   // slot 0: the node's bias terms
+              double bt2, nb = 0.0;
+              if (kind == NK_MUL) nb = elem_coef(kind, 1, side, a, p, 0.0, &bt2);
+              if (a != 0.0 && (!isfinite(bt) || !isfinite(na) || !isfinite(nb))) und_ = 1;
+              if (isfinite(bt)) { sb += bt; sm_ += fabs(bt); }
+            }
+          } else if (kind == NK_MULC) {
+            const double cv = __ldg(cvec + c);
+            na = a * cv;
+            if (need_a && inex[c] && a != 0.0) {
+              const double m = m0[map0[c]];
+              sc += isinf(m) ? (__fma_rn(a, cv, -(a * cv)) != 0.0 ? INFINITY : 0.0) : UNIT * (fabs(a * cv) * m);
+            }
+          } else {
+            double bt;
+            na = elem_coef(kind, slot, side, a, nullptr, cvec ? __ldg(cvec + c) : 0.0, &bt);
+            if (need_a) {
+              const double mx = m0[map0[c]];
+              const double my = m1 ? m1[map1[c]] : fabs(cvec[c]);
+              const double e_ = rounding_error(mx + my, 2);
+              const double fa = finite_abs(a);
+              sc += fa > 0 ? (isinf(e_) ? 0.0 : fa * e_) : 0.0;
+              if (kind == NK_ADDC || kind == NK_SUBC || kind == NK_RSUBC) {
+                const double cv = kind == NK_SUBC ? -cvec[c] : cvec[c];
+                sb += a * cv;
+                sm_ += fabs(a) * fabs(cv);
+              }
+            }
+          }
+          const double acc = 0.0 + (isfinite(na) ? na : 0.0);
+          const double old = zero_u ? 0.0 : U[e];
+          const double tot = old + acc;
+          U[e] = tot;
+          if (uk >= 2 && acc != 0.0) {
+            const double m = mu[ucols[e]];
+            pmerge += isinf(m) ? (merge_rounded(old, acc, tot) ? INFINITY : 0.0) : fabs(acc) * m;
+          }
+        }
+        if (need_a) {
+          double* val = ctx.row(side, R_VAL);
+          val[s] = und_ ? NAN : val[s] + sb;
+          ctx.row(side, R_ERR)[s] += sm_ * fbias + sc;
+        }
+        if (uk >= 2) ctx.row(side, R_ERR)[s] += gmerge * pmerge;
+      }
+    };
+
     if (!dense) {
       const int32_t* shortr = P->ip + op[O_SHORT];
       const int32_t* longr = P->ip + op[O_LONG];
       const int nshort = op[O_NSHORT], nlong = op[O_NLONG];
+      if (IDX && (oflags & OF_FUSED)) {
+        for (int i = tid; i < nshort; i += NT) fused_row(shortr[i]);
+      } else {
       for (int i = tid; i < nshort; i += NT) row_body(shortr[i], 0, 1, 0);
       if (2 * nlong <= NWARP) {
         // few long rows (single rows of a chain): the whole CTA on each, instead of idle warps
         for (int i = 0; i < nlong; ++i) row_body(longr[i], tid, NT, 2);
       } else {
         for (int i = warp; i < nlong; i += NWARP) row_body(longr[i], lane, 32, 1);
+      }
       }
     } else {
       // ---- GEMV: A_u[s, :] (+)= sum_e A_v[e] W[c_e, :]; charges gamma_w <|A_v||W|, m_u> and merges

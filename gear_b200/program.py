@@ -62,7 +62,7 @@ OP_REC = 32
  O_TPTR, O_UK, O_TMAXROW, O_SHORT, O_NSHORT, O_LONG, O_NLONG, O_SINGLE) = range(32)
 ROW_THREAD_MAX = 16  # rows with at most this much work run on one thread, longer rows on a warp
 # bits of the op record's O_SINGLE field (OpFlag in gear_program.h)
-OF_SINGLE, OF_SRC_ID, OF_TGT_ID, OF_TPTR_ID, OF_VRP_ID, OF_SPLIT = 1, 2, 4, 8, 16, 32
+OF_SINGLE, OF_SRC_ID, OF_TGT_ID, OF_TPTR_ID, OF_VRP_ID, OF_SPLIT, OF_FUSED = 1, 2, 4, 8, 16, 32, 64
 ROOT_IN_LA = -2     # buffer marker: the input's A of a final pass accumulates in the lA output
 
 PLANES_PER_ELEM = {"mul": 6, "sqr": 4, "exp": 4, "log": 4, "sin": 4, "cos": 4, "pow": 4}
@@ -686,6 +686,16 @@ class Program:
                 r[O_NSHORT] = len(short)
                 r[O_LONG] = P.add_int(long_)
                 r[O_NLONG] = len(long_)
+                # entry-wise op: entry e of v's row s moves to entry e of u's row s (one source per
+                # target, identity sources and targets, the moves of row s are v's entries of row
+                # s, and a fresh u row has exactly those entries): the kernel then takes each
+                # entry's bias terms and its move in one sweep, without clearing u's row first
+                f = int(r[O_SINGLE])
+                if (r[O_DENSE] == 0 and len(long_) == 0 and not (p == 0 and xdense) and
+                        (f & (OF_SINGLE | OF_SRC_ID | OF_TGT_ID)) == (OF_SINGLE | OF_SRC_ID | OF_TGT_ID) and
+                        np.array_equal(tptr, rowptr[v]) and
+                        (r[O_UMERGE] == 1 or np.array_equal(rowptr[p], rowptr[v]))):
+                    r[O_SINGLE] = f | OF_FUSED
                 self.op_recs.append(r)
             if last_use.get(v, -2) == i and v != 0 and bufoff.get(v, 0) >= 0:
                 release(v)
