@@ -1301,7 +1301,7 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
       const int32_t* shortr = P->ip + op[O_SHORT];
       const int32_t* longr = P->ip + op[O_LONG];
       const int nshort = op[O_NSHORT], nlong = op[O_NLONG];
-      if (IDX && (oflags & OF_FUSED)) {
+      if (oflags & OF_FUSED) {
         for (int i = tid; i < nshort; i += NT) fused_row(shortr[i]);
       } else {
       for (int i = tid; i < nshort; i += NT) row_body(shortr[i], 0, 1, 0);
