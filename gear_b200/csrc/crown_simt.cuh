@@ -257,6 +257,73 @@ __device__ void simt_run_pass(const SBox& bx, int pid, const Work& wk, bool live
     for (int side = 0; side < sides; ++side) {
       SView V = vals(side, op[O_VBUF]);
       SView rval = row(side, R_VAL), rerr = row(side, R_ERR);
+      if (op[O_SINGLE] & OF_FUSED) {
+        // an entry-wise op: each entry's bias terms and its move (u's entry e <- v's entry e) in
+        // one sweep, in the order and with the arithmetic of the sweeps below (same bits); u needs
+        // no clearing (its entries are exactly the moved ones)
+        SView U = vals(side, op[O_UBUF]);
+        const int32_t* ucols = P->ip + op[O_UCOLS];
+        SView mu = bx.mag + und[N_CUR];
+        for (int s = 0; s < S; ++s) {
+          const int e0 = __ldg(vrp + s), e1 = __ldg(vrp + s + 1);
+          if (e0 == e1) continue;
+          double sb = 0, sm_ = 0, sc = 0, pmerge = 0;
+          int und_ = 0;
+          for (int e = e0; e < e1; ++e) {
+            const double a = V[e];
+            const int c = __ldg(vcols + e);
+            double na;
+            if (relax || kind == NK_MUL) {
+              double p[6];
+              for (int k = 0; k < ppe; ++k) p[k] = pl[ppe * c + k];
+              double bt;
+              na = elem_coef(kind, slot, side, a, p, 0.0, &bt);
+              if (need_a) {   // slot 0: the node's bias terms
+                double bt2, nb = 0.0;
+                if (kind == NK_MUL) nb = elem_coef(kind, 1, side, a, p, 0.0, &bt2);
+                if (a != 0.0 && (!isfinite(bt) || !isfinite(na) || !isfinite(nb))) und_ = 1;
+                if (isfinite(bt)) { sb += bt; sm_ += fabs(bt); }
+              }
+            } else if (kind == NK_MULC) {
+              const double cv = __ldg(cvec + c);
+              na = a * cv;
+              if (need_a && __ldg(inex + c) && a != 0.0) {
+                const double m = m0[__ldg(map0 + c)];
+                sc += isinf(m) ? (__fma_rn(a, cv, -(a * cv)) != 0.0 ? INFINITY : 0.0) : UNIT * (fabs(a * cv) * m);
+              }
+            } else {
+              double bt;
+              na = elem_coef(kind, slot, side, a, nullptr, cvec ? __ldg(cvec + c) : 0.0, &bt);
+              if (need_a) {
+                const double mx = m0[__ldg(map0 + c)];
+                const double my = two ? m1[__ldg(map1 + c)] : fabs(__ldg(cvec + c));
+                const double e_ = rounding_error(mx + my, 2);
+                const double fa = finite_abs(a);
+                sc += fa > 0 ? (isinf(e_) ? 0.0 : fa * e_) : 0.0;
+                if (kind == NK_ADDC || kind == NK_SUBC || kind == NK_RSUBC) {
+                  const double cv = kind == NK_SUBC ? -__ldg(cvec + c) : __ldg(cvec + c);
+                  sb += a * cv;
+                  sm_ += fabs(a) * fabs(cv);
+                }
+              }
+            }
+            const double acc = 0.0 + (isfinite(na) ? na : 0.0);
+            const double old = zero_u ? 0.0 : U[e];
+            const double tot = old + acc;
+            U[e] = tot;
+            if (uk >= 2 && acc != 0.0) {
+              const double m = mu[__ldg(ucols + e)];
+              pmerge += isinf(m) ? (merge_rounded(old, acc, tot) ? INFINITY : 0.0) : fabs(acc) * m;
+            }
+          }
+          if (need_a) {
+            rval[s] = und_ ? NAN : rval[s] + sb;
+            rerr[s] += sm_ * fbias + sc;
+          }
+          if (uk >= 2) rerr[s] += gmerge * pmerge;
+        }
+        continue;
+      }
       // ---- bias, bias magnitude, charges and undefined flags (v's rows)
       if (need_a) {
         for (int s = 0; s < S; ++s) {
