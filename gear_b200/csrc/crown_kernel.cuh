@@ -1233,13 +1233,19 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
     // entry's bias terms and its move (u's entry e <- v's entry e), in the order and with the
     // arithmetic of row_body's two sweeps, so the results are the same bits; u's row needs no
     // clearing (a fresh row holds exactly the moved entries)
+    // OF_FUSED_T: entry e moves to u's entry tgt[e] of the same row; a fresh u row is cleared first
     auto fused_row = [&](int s) {
       const bool vid = (oflags & OF_VRP_ID) != 0;
+      const bool tmap = (oflags & OF_FUSED_T) != 0;
       const int e0 = vid ? s : vrp[s], e1 = vid ? s + 1 : vrp[s + 1];
-      if (e0 == e1) return;
+      if (e0 == e1 && !(tmap && zero_u)) return;
+      const int32_t* tgt = P->ip + op[O_TGT];
       for (int side = 0; side < sides; ++side) {
         const double* V = ctx.vals(side, op[O_VBUF]);
         double* U = ctx.vals(side, op[O_UBUF]);
+        // a u row the op opens is cleared even where v's row is empty (as row_body does)
+        if (tmap && zero_u) for (int j = urp[s]; j < urp[s + 1]; ++j) U[j] = 0.0;
+        if (e0 == e1) continue;
         double sb = 0, sm_ = 0, sc = 0, pmerge = 0;
         int und_ = 0;
         for (int e = e0; e < e1; ++e) {
@@ -1280,11 +1286,12 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
             }
           }
           const double acc = 0.0 + (isfinite(na) ? na : 0.0);
-          const double old = zero_u ? 0.0 : U[e];
+          const int ti = tmap ? __ldg(tgt + e) : e;
+          const double old = zero_u ? 0.0 : U[ti];
           const double tot = old + acc;
-          U[e] = tot;
+          U[ti] = tot;
           if (uk >= 2 && acc != 0.0) {
-            const double m = mu[ucols[e]];
+            const double m = mu[ucols[ti]];
             pmerge += isinf(m) ? (merge_rounded(old, acc, tot) ? INFINITY : 0.0) : fabs(acc) * m;
           }
         }
@@ -1301,7 +1308,7 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
       const int32_t* shortr = P->ip + op[O_SHORT];
       const int32_t* longr = P->ip + op[O_LONG];
       const int nshort = op[O_NSHORT], nlong = op[O_NLONG];
-      if (oflags & OF_FUSED) {
+      if (oflags & (OF_FUSED | OF_FUSED_T)) {
         for (int i = tid; i < nshort; i += NT) fused_row(shortr[i]);
       } else {
       for (int i = tid; i < nshort; i += NT) row_body(shortr[i], 0, 1, 0);

@@ -257,13 +257,19 @@ __device__ void simt_run_pass(const SBox& bx, int pid, const Work& wk, bool live
     for (int side = 0; side < sides; ++side) {
       SView V = vals(side, op[O_VBUF]);
       SView rval = row(side, R_VAL), rerr = row(side, R_ERR);
-      if (op[O_SINGLE] & OF_FUSED) {
-        // an entry-wise op: each entry's bias terms and its move (u's entry e <- v's entry e) in
-        // one sweep, in the order and with the arithmetic of the sweeps below (same bits); u needs
-        // no clearing (its entries are exactly the moved ones)
+      if (op[O_SINGLE] & (OF_FUSED | OF_FUSED_T)) {
+        // an entry-wise op: each entry's bias terms and its move (u's entry e <- v's entry e, or
+        // tgt[e] with OF_FUSED_T) in one sweep, in the order and with the arithmetic of the sweeps
+        // below (same bits); with OF_FUSED u needs no clearing (its entries are the moved ones)
         SView U = vals(side, op[O_UBUF]);
         const int32_t* ucols = P->ip + op[O_UCOLS];
+        const int32_t* tgt = P->ip + op[O_TGT];
+        const bool tmap = (op[O_SINGLE] & OF_FUSED_T) != 0;
         SView mu = bx.mag + und[N_CUR];
+        if (tmap && zero_u) {
+          const int nnz_u = op[O_UNNZ];
+          for (int k = 0; k < nnz_u; ++k) U[k] = 0.0;
+        }
         for (int s = 0; s < S; ++s) {
           const int e0 = __ldg(vrp + s), e1 = __ldg(vrp + s + 1);
           if (e0 == e1) continue;
@@ -308,11 +314,12 @@ __device__ void simt_run_pass(const SBox& bx, int pid, const Work& wk, bool live
               }
             }
             const double acc = 0.0 + (isfinite(na) ? na : 0.0);
-            const double old = zero_u ? 0.0 : U[e];
+            const int ti = tmap ? __ldg(tgt + e) : e;
+            const double old = zero_u ? 0.0 : U[ti];
             const double tot = old + acc;
-            U[e] = tot;
+            U[ti] = tot;
             if (uk >= 2 && acc != 0.0) {
-              const double m = mu[__ldg(ucols + e)];
+              const double m = mu[__ldg(ucols + ti)];
               pmerge += isinf(m) ? (merge_rounded(old, acc, tot) ? INFINITY : 0.0) : fabs(acc) * m;
             }
           }

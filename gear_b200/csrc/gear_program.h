@@ -37,9 +37,14 @@ enum OpField {
 // target list, the target row pointers or v's row pointers are the identity (the kernel then
 // computes the index instead of loading it). OF_SPLIT: the final pass's product through a dense
 // node on the input, handed to the tensor cores when the launch provides the buffers for it.
-enum OpFlag { OF_SINGLE = 1, OF_SRC_ID = 2, OF_TGT_ID = 4, OF_TPTR_ID = 8, OF_VRP_ID = 16, OF_SPLIT = 32, OF_FUSED = 64 };
+enum OpFlag {
+  OF_SINGLE = 1, OF_SRC_ID = 2, OF_TGT_ID = 4, OF_TPTR_ID = 8, OF_VRP_ID = 16, OF_SPLIT = 32, OF_FUSED = 64,
+  OF_FUSED_T = 128
+};
 // OF_FUSED: an entry-wise op (entry e of v's row s moves to entry e of u's row s, which a fresh u
-// row holds exactly, all rows short): bias terms and moves in one sweep over the row's entries
+// row holds exactly, all rows short): bias terms and moves in one sweep over the row's entries.
+// OF_FUSED_T: the same sweep with entry e moving to u's entry tgt[e] of the same row (a fresh u row
+// is cleared first).
 // buffer offset marker: the input's A of a final pass accumulates in the lA output (row s at s * n)
 constexpr int ROOT_IN_LA = -2;
 // rows with at most this many entries are handled by one thread, longer rows by a warp

@@ -62,7 +62,7 @@ OP_REC = 32
  O_TPTR, O_UK, O_TMAXROW, O_SHORT, O_NSHORT, O_LONG, O_NLONG, O_SINGLE) = range(32)
 ROW_THREAD_MAX = 16  # rows with at most this much work run on one thread, longer rows on a warp
 # bits of the op record's O_SINGLE field (OpFlag in gear_program.h)
-OF_SINGLE, OF_SRC_ID, OF_TGT_ID, OF_TPTR_ID, OF_VRP_ID, OF_SPLIT, OF_FUSED = 1, 2, 4, 8, 16, 32, 64
+OF_SINGLE, OF_SRC_ID, OF_TGT_ID, OF_TPTR_ID, OF_VRP_ID, OF_SPLIT, OF_FUSED, OF_FUSED_T = 1, 2, 4, 8, 16, 32, 64, 128
 ROOT_IN_LA = -2     # buffer marker: the input's A of a final pass accumulates in the lA output
 
 PLANES_PER_ELEM = {"mul": 6, "sqr": 4, "exp": 4, "log": 4, "sin": 4, "cos": 4, "pow": 4}
@@ -690,12 +690,15 @@ class Program:
                 # target, identity sources and targets, the moves of row s are v's entries of row
                 # s, and a fresh u row has exactly those entries): the kernel then takes each
                 # entry's bias terms and its move in one sweep, without clearing u's row first
+                # OF_FUSED_T: the same sweep with each entry's target read from the op's target list
+                # (u's row holds more entries: it is cleared first when the op opens it)
                 f = int(r[O_SINGLE])
                 if (r[O_DENSE] == 0 and len(long_) == 0 and not (p == 0 and xdense) and
-                        (f & (OF_SINGLE | OF_SRC_ID | OF_TGT_ID)) == (OF_SINGLE | OF_SRC_ID | OF_TGT_ID) and
-                        np.array_equal(tptr, rowptr[v]) and
-                        (r[O_UMERGE] == 1 or np.array_equal(rowptr[p], rowptr[v]))):
-                    r[O_SINGLE] = f | OF_FUSED
+                        (f & (OF_SINGLE | OF_SRC_ID)) == (OF_SINGLE | OF_SRC_ID) and np.array_equal(tptr, rowptr[v])):
+                    if (f & OF_TGT_ID) and (r[O_UMERGE] == 1 or np.array_equal(rowptr[p], rowptr[v])):
+                        r[O_SINGLE] = f | OF_FUSED
+                    else:
+                        r[O_SINGLE] = f | OF_FUSED_T
                 self.op_recs.append(r)
             if last_use.get(v, -2) == i and v != 0 and bufoff.get(v, 0) >= 0:
                 release(v)

@@ -79,7 +79,7 @@ def test_fused_flag_marks_entrywise_ops():
     ops whose moves are entry-wise: one identity source and target per entry, row s's moves are
     v's entries of row s, and a fresh u row holds exactly those entries; every row short. The
     elementwise chains of the mixed family get it on most ops."""
-    from gear_b200.program import OF_FUSED, O_URP, O_UMERGE, O_NLONG, O_U, O_UBUF, ROOT_IN_LA
+    from gear_b200.program import OF_FUSED, OF_FUSED_T, O_URP, O_UMERGE, O_NLONG, O_U, O_UBUF, ROOT_IN_LA
     m = problems.mixed_instance(70)
     prog = Program(graph.trace(m, torch.zeros(2, m.n, dtype=torch.float64)), mode="cta", cta_threads=256)
     ops = prog.op_arr.reshape(-1, OP_REC)
@@ -90,14 +90,23 @@ def test_fused_flag_marks_entrywise_ops():
         S = int(pr[P_S])
         for o in ops[int(pr[P_OP0]):int(pr[P_OP0]) + int(pr[P_NOP])]:
             f = int(o[O_SINGLE])
-            if not f & OF_FUSED:
+            if not f & (OF_FUSED | OF_FUSED_T):
                 continue
             fused += 1
-            assert f & (OF_SINGLE | OF_SRC_ID | OF_TGT_ID) == (OF_SINGLE | OF_SRC_ID | OF_TGT_ID)
+            assert not (f & OF_FUSED and f & OF_FUSED_T)
+            assert f & (OF_SINGLE | OF_SRC_ID) == (OF_SINGLE | OF_SRC_ID)
             assert o[O_DENSE] == 0 and o[O_NLONG] == 0 and o[O_UBUF] != ROOT_IN_LA
             vrp = ip[o[O_VRP]:o[O_VRP] + S + 1]
             tptr = ip[o[O_TPTR]:o[O_TPTR] + S + 1]
             urp = ip[o[O_URP]:o[O_URP] + S + 1]
             assert np.array_equal(tptr, vrp)
-            assert o[O_UMERGE] == 1 or np.array_equal(urp, vrp)
-    assert fused > len(ops) // 2
+            if f & OF_FUSED:
+                assert f & OF_TGT_ID
+                assert o[O_UMERGE] == 1 or np.array_equal(urp, vrp)
+            else:
+                # every target of row s lies in u's row s
+                tgt = ip[o[O_TGT]:o[O_TGT] + int(o[O_NTGT])]
+                rows_u = np.repeat(np.arange(S), np.diff(urp))
+                rows_v = np.repeat(np.arange(S), np.diff(vrp))
+                assert np.array_equal(rows_u[tgt], rows_v)
+    assert fused > len(ops) * 3 // 4
