@@ -581,7 +581,7 @@ def dense_nodes(dev, batch=8192, steps=3, warmup=1):
         del eng, out
     a, b = lbs["tensor_core_fold_exact_ties"], lbs["cuda_core_fold_exact_ties"]
     res["error_vs_fp64"] = {"max_rel_lb": float(((a - b).abs() / torch.clamp(b.abs(), min=1.0)).max()),
-                            "tie_rule": "exact (both)", "tolerance_north_star": 1e-5}
+                            "tie_rule": "exact (both)", "tolerance": 1e-5}
     a, b = lbs["tensor_core_fold"], lbs["cuda_core_fold"]
     res["default_rule_difference"] = {"max_rel_lb": float(((a - b).abs() / torch.clamp(b.abs(), min=1.0)).max())}
     res["speedup_tensor_core_fold"] = res["cuda_core_fold"]["ms_per_call"] / res["tensor_core_fold"]["ms_per_call"]

@@ -7,7 +7,7 @@ decided in exact arithmetic (lb_exact, lA_exact, lbias_exact), plus lb_ulp_dev, 
 relative change of the reference's own lb when its boxes grow by one ulp.
 
 * tie_rule "exact" on the GPU against the exact-tie reference run: every row, every fixture,
-  every kernel variant, within 1e-5 relative (measured ~1e-11).
+  every kernel variant, within 1e-5 relative (the parity tolerance; measured ~1e-11).
 * tie_rule "reference" (the default) against the plain reference run: within 1e-5 on every
   row the reference itself determines to 1e-5 (lb_ulp_dev <= 1e-5), for the float64 CUDA-core
   variants. On the other rows the reference's choice between two McCormick planes with equal
