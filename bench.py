@@ -127,7 +127,8 @@ def cpu_baseline(per_core=16, cores=None, workload=WORKLOAD):
     boxes = sum(r[1] for r in res)
     return {"value": boxes / slowest, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"{boxes} {workload} sub-boxes ({per_core} per process on {cores} spawned processes, "
-                      f"float64 numpy oracle, 1 thread each; slowest process {slowest:.2f} s)"}
+                      f"float64 numpy oracle, 1 thread each; slowest process {slowest:.2f} s)",
+            "sample_boxes": boxes, "sample_s": slowest}
 
 
 def run_reference(args):
@@ -135,17 +136,25 @@ def run_reference(args):
     if rank != 0:
         return
     per_core = max(4, args.cpu_per_core)
-    vals = []
+    vals, secs = [], []
     for i in range(args.warmup + args.steps):
         r = cpu_baseline(per_core=per_core, workload=args.workload)
         if i >= args.warmup:
             vals.append(r["value"])
+            secs.append(r["sample_s"])
     v = statistics.median(vals)
     r["value"] = v
+    from gear_b200 import graph, problems
+    m = problems.make_instance(args.workload, 0)
+    lo, _ = problems.make_boxes(args.workload, 2, 0)
+    g = graph.trace(m, lo)
+    # the GPU arm's workload and shapes; each step bounds a sample of its boxes on the host cores
+    config = {"workload": args.workload, "batch": args.batch, "n": int(lo.shape[1]), "spec_rows": int(g[g.output].width),
+              "parallelism": f"replicas{args.gpus}", "sample_per_step": r["sample"]}
     out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * 1 / v,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.median(secs),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-           "data": "synthetic", "config": {"workload": args.workload, "batch": r["sample"]},
+           "data": "synthetic", "config": config,
            "cpu_baseline": r, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 
