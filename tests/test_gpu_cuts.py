@@ -141,3 +141,20 @@ def test_bab_with_cuts_everywhere_closes_like_final_row_form():
     assert res[True].cut_engine is not None and res[False].cut_engine is None
     a, b_ = res[True].incumbent, res[False].incumbent
     assert abs(a - b_) <= 1e-4 * max(1.0, abs(a), abs(b_))
+
+
+@pytest.mark.parametrize("case", cut_cases()[:2])
+def test_dense_specification_rows_match_oracle(case):
+    """A dense specification C (B, S', w) with cut rows: the engine compiled for C (dense_c) against
+    the oracle's compute_bounds(C, constraints) with exact ties, every row to 1e-9."""
+    m, g, d, _ = load_cuts(case)
+    B = d["x_L"].shape[0]
+    w = g[g.output].width
+    rng = np.random.default_rng(17)
+    C = rng.standard_normal((B, 2, w))
+    (lb, lA, lbias), _ = _gpu(g, d["x_L"], d["x_U"], d["A"], d["b"], C=C)
+    olb, _, olA, olbias = CrownOracle(g, tie_tol=EXACT_TIE_TOL).compute_bounds(
+        d["x_L"], d["x_U"], C, constraints=(d["A"], d["b"]))
+    assert _rel(lb, olb).max() < TOL
+    assert _rel(lbias, olbias).max() < TOL
+    assert np.abs(lA - olA).max() <= TOL * max(1.0, np.abs(olA).max())
