@@ -1160,10 +1160,34 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
             }
           }
           if (mode != 0) {
-            sb = row_sum(sb, mode);
-            sm_ = row_sum(sm_, mode);
-            sc = row_sum(sc, mode);
-            und_ = row_sum((double)und_, mode) != 0.0;
+            // the four sums of the row: warp sums, then (whole-CTA rows) one exchange through the
+            // reduction slots, each value summed over the warps in warp order as row_sum does
+            sb = warp_sum(sb);
+            sm_ = warp_sum(sm_);
+            sc = warp_sum(sc);
+            double ud = warp_sum((double)und_);
+            if (mode == 2) {
+              if (lane == 0) {
+                ctx.red[warp] = sb;
+                ctx.red[NWARP + warp] = sm_;
+                ctx.red[2 * NWARP + warp] = sc;
+                ctx.red[3 * NWARP + warp] = ud;
+              }
+              __syncthreads();
+              double t0 = 0.0, t1 = 0.0, t2 = 0.0, t3 = 0.0;
+              for (int w_ = 0; w_ < NWARP; ++w_) {
+                t0 += ctx.red[w_];
+                t1 += ctx.red[NWARP + w_];
+                t2 += ctx.red[2 * NWARP + w_];
+                t3 += ctx.red[3 * NWARP + w_];
+              }
+              __syncthreads();
+              sb = t0;
+              sm_ = t1;
+              sc = t2;
+              ud = t3;
+            }
+            und_ = ud != 0.0;
           }
           if (lead) {
             double* val = ctx.row(side, R_VAL);
