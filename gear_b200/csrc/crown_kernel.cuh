@@ -19,7 +19,9 @@
 //   concretise   concretize_bounds.py:160-321, concretize_func.py:553-569,
 //                fp_enclosure.py:34-98.
 // Compiled with -fmad=false: the elementwise formulas round like the reference's eager
-// float64 arithmetic (no contraction), which keeps the relaxation choices stable.
+// float64 arithmetic (no contraction), which keeps the relaxation choices stable. The dot
+// products of the GEMV steps, the fold vectors and the box concretisation accumulate with explicit
+// fused multiply-adds (as a BLAS product does); their rounding charges bound any such order.
 #pragma once
 #include <cuda_runtime.h>
 #include <math.h>
@@ -785,16 +787,16 @@ __device__ void fold_node(const Box& bx, int v, double* stage) {
 #pragma unroll
       for (int q = 0; q < FOLD_UNROLL; ++q) {
         const double aw = fabs(wv[q]);
-        c += xc[i + q] * wv[q];
-        r += xr[i + q] * aw;
-        t += xm[i + q] * aw;
+        c = __fma_rn(xc[i + q], wv[q], c);
+        r = __fma_rn(xr[i + q], aw, r);
+        t = __fma_rn(xm[i + q], aw, t);
       }
     }
     for (; i < win; ++i) {
       const double wv = __ldg(col + (int64_t)i * w), aw = fabs(wv);
-      c += xc[i] * wv;
-      r += xr[i] * aw;
-      t += xm[i] * aw;
+      c = __fma_rn(xc[i], wv, c);
+      r = __fma_rn(xr[i], aw, r);
+      t = __fma_rn(xm[i], aw, t);
     }
     f[j] = c;
     f[w + j] = r;
@@ -972,8 +974,8 @@ __device__ __forceinline__ void gemv_row(const double* V, const int32_t* vcols, 
           if (e + r >= e1) break;
 #pragma unroll
           for (int q = 0; q < JB; ++q) {
-            acc[q] += aq[r] * wq[r][q];
-            ab[q] += fabs(aq[r]) * fabs(wq[r][q]);
+            acc[q] = __fma_rn(aq[r], wq[r][q], acc[q]);
+            ab[q] = __fma_rn(fabs(aq[r]), fabs(wq[r][q]), ab[q]);
           }
         }
       }
@@ -1528,9 +1530,9 @@ __device__ void run_pass(const Box& bx, int pid, double* sm, int32_t* stage_ops,
           for (int q = 0; q < XB; ++q) {
             if (!ok[q]) continue;
             const double a = aq[q], l = lq[q], h = hq[q];
-            bs += a * ((h + l) / 2.0);
-            dv += fabs(a) * ((h - l) / 2.0);
-            be += finite_abs(a) * finite_abs(fmax(fabs(l), fabs(h)));
+            bs = __fma_rn(a, (h + l) / 2.0, bs);
+            dv = __fma_rn(fabs(a), (h - l) / 2.0, dv);
+            be = __fma_rn(finite_abs(a), finite_abs(fmax(fabs(l), fabs(h))), be);
           }
         }
         if (rs.warp) { bs = warp_sum(bs); dv = warp_sum(dv); be = warp_sum(be); }
