@@ -313,7 +313,8 @@ int gear_crown_lower_plain_ibp(const gear_dag* dag, const double* x_L, const dou
  * [x_L, x_U] intersected with the box's rows cut_A (batch, K, n) x + cut_b (batch, K) <= 0, by the
  * sequential dual sweep of gear_constrained_lower (constraints_solving, concretize_func.py:431-850;
  * an upper bound is minus the sweep's lower bound of -A), in place of the box terms. lb, lA, lbias
- * (and lb_ibp when non-NULL, as gear_crown_lower_plain_ibp) as gear_crown_lower. A box its rows
+ * (and lb_ibp when non-NULL, as gear_crown_lower_plain_ibp) as gear_crown_lower; lA is required.
+ * C (batch, S, w) or NULL (identity) as gear_crown_lower. A box its rows
  * exclude gets bounds that only say so through the concretisations (+inf lower rows are discarded
  * to the interval fallback); callers that prune on infeasibility test it with
  * gear_constrained_lower. The DAG must be compiled for cut rows (gear_b200/program.py
