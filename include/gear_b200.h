@@ -31,6 +31,8 @@
  *   gear_dual_lower_bound <- dual_lower_bound / certify_infeasible    complete_verifier/nlp_solver/rigorous_dual.py:1-238
  *   gear_constrained_lower <- sort_out_constr_batches + constraints_solving(sign=-1)
  *                        (+ drop_redundant_constraints, _solve_dual_var)  solver/auto_LiRPA/concretize_func.py:168-850
+ *   gear_crown_lower_cuts <- compute_bounds with PerturbationLpNorm(x_L, x_U, constraints=(A, b))
+ *                        bound_general.py:1275, perturbations.py:129-199, concretize_func.py:431-850
  */
 #ifndef GEAR_B200_H
 #define GEAR_B200_H
